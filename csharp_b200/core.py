@@ -1,0 +1,273 @@
+"""Host-side mirror of the reference's aligner and block-handler API over the C ABI.
+
+Names follow the reference (DSC-SPIDAL/csharp, SalsaTPL/):
+
+* :class:`ScoringMatrix`       Salsa.CoreTPL/Bio/Algorithms/ScoringMatrix.cs (``Load``, ``Scores``)
+* :class:`SmithWatermanGotoh`  Salsa.CoreTPL/Bio/Algorithms/SmithWaterman/SmithWatermanGotoh.cs
+  (``Align`` returning a :class:`PairwiseAlignment`, Alignment.cs)
+* :class:`Range`, :class:`Block`, :func:`range_partition`, :func:`block_partition`
+  Salsa.CoreTPL/Range.cs, Block.cs, RangePartitioner.cs, BlockPartitioner.cs
+* :class:`Engine`              the block handler ``ComputeBlock`` of the three applications and the
+  whole-job driver, on one CUDA device
+"""
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import lib as L
+
+PROTEIN, NUCLEIC = L.SW_PROTEIN, L.SW_NUCLEIC
+PERCENT_IDENTITY, KIMURA2, JUKES_CANTOR = L.SW_DIST_PERCENT_IDENTITY, L.SW_DIST_KIMURA2, L.SW_DIST_JUKES_CANTOR
+SWG_MPI, SWG_MS, NW = L.SW_MODE_SWG_MPI, L.SW_MODE_SWG_MS, L.SW_MODE_NW
+
+
+class ScoringMatrix:
+    """A substitution table indexed by residue bytes (``Scores[c1, c2]``)."""
+
+    BUILTIN = ("EDNAFULL", "BLOSUM62", "IDENTITY", "MATCH")
+
+    def __init__(self, name, scores: np.ndarray):
+        self.Name = name
+        self.Scores = np.ascontiguousarray(scores, dtype=np.int16).reshape(128, 128)
+
+    @staticmethod
+    def Load(name: str) -> "ScoringMatrix":
+        """A built-in matrix by the reference's resource name."""
+        out = np.zeros((128, 128), dtype=np.int16)
+        L.check(L.load().sw_builtin_scoring_matrix(name.encode(), L.ptr(out)))
+        return ScoringMatrix(name, out)
+
+    @staticmethod
+    def Parse(text, name="custom") -> "ScoringMatrix":
+        """ScoringMatrix.Load's parser over matrix text in the reference's format."""
+        if isinstance(text, str):
+            text = text.encode()
+        out = np.zeros((128, 128), dtype=np.int16)
+        L.check(L.load().sw_parse_scoring_matrix(text, len(text), L.ptr(out)))
+        return ScoringMatrix(name, out)
+
+    def GetScore(self, a, b):
+        return int(self.Scores[ord(a) if isinstance(a, str) else a, ord(b) if isinstance(b, str) else b])
+
+
+@dataclass
+class PairwiseAlignment:
+    """The PairwiseAlignment fields the distance path reads (Alignment.cs:29-195)."""
+    Score: float
+    Start1: int
+    Start2: int
+    End1: int
+    End2: int
+    Identity: int
+    Similarity: int
+    Gaps: int
+    Length: int
+    Distance: int
+
+    @property
+    def PercentIdentity(self):
+        return np.float32(self.Identity) / np.float32(self.Length) if self.Length else np.float32("nan")
+
+    @property
+    def PercentSimilarity(self):
+        return np.float32(self.Similarity) / np.float32(self.Length) if self.Length else np.float32("nan")
+
+
+@dataclass
+class Range:
+    """Inclusive index range (Range.cs:9-89)."""
+    StartIndex: int
+    EndIndex: int
+
+    @property
+    def Length(self):
+        return self.EndIndex - self.StartIndex + 1
+
+    def Contains(self, i):
+        return self.StartIndex <= i <= self.EndIndex
+
+
+@dataclass
+class Block:
+    """A rectangle of the pair matrix (Block.cs:9-61)."""
+    RowRange: Range
+    ColumnRange: Range
+    RowBlockNumber: int = 0
+    ColumnBlockNumber: int = 0
+
+    def Transpose(self):
+        return Block(self.ColumnRange, self.RowRange, self.ColumnBlockNumber, self.RowBlockNumber)
+
+
+def range_partition(length, parts, start=0):
+    """RangePartitioner.Partition (RangePartitioner.cs:17-55)."""
+    if parts < 1:
+        raise ValueError("Partitioning requires numPartitions to be greater than zero.")
+    s = np.zeros(parts, dtype=np.int32)
+    e = np.zeros(parts, dtype=np.int32)
+    L.check(L.load().sw_partition_ranges(start, length, parts, L.ptr(s), L.ptr(e)))
+    return [Range(int(a), int(b)) for a, b in zip(s, e)]
+
+
+def block_partition(rows, cols, row_blocks, col_blocks):
+    """BlockPartitioner.Partition (BlockPartitioner.cs:10-28)."""
+    rr, cc = range_partition(rows, row_blocks), range_partition(cols, col_blocks)
+    return [[Block(r, c, i, j) for j, c in enumerate(cc)] for i, r in enumerate(rr)]
+
+
+def block_is_computed(r, c):
+    """Does rank r compute block (r, c) under the SWG-MPI checkerboard (Program.cs:628-639)?"""
+    return bool(L.load().sw_block_is_computed(r, c))
+
+
+def pack_sequences(seqs):
+    """Concatenated residues + offsets from a list of byte strings / str / uint8 arrays."""
+    parts = []
+    for s in seqs:
+        if isinstance(s, str):
+            s = s.encode()
+        parts.append(np.frombuffer(bytes(s), dtype=np.uint8) if not isinstance(s, np.ndarray) else s.astype(np.uint8))
+    lens = np.array([len(p) for p in parts], dtype=np.int64)
+    off = np.zeros(len(parts) + 1, dtype=np.int64)
+    np.cumsum(lens, out=off[1:])
+    concat = np.concatenate(parts) if parts else np.zeros(0, dtype=np.uint8)
+    return np.ascontiguousarray(concat, dtype=np.uint8), off
+
+
+class Engine:
+    """One device context: configuration, resident sequences, block handler and job driver."""
+
+    def __init__(self, matrix: ScoringMatrix, gap_open=14, gap_extension=4, mode=SWG_MPI,
+                 alignment_type=NUCLEIC, distance_fn=PERCENT_IDENTITY, device=0, lanes=0):
+        cfg = L.sw_config()
+        cfg.mode, cfg.alignment_type, cfg.distance_fn = mode, alignment_type, distance_fn
+        cfg.gap_open, cfg.gap_extension = float(gap_open), float(gap_extension)
+        C.memmove(cfg.scores, matrix.Scores.ctypes.data, 128 * 128 * 2)
+        cfg.device, cfg.lanes = device, lanes
+        h = C.c_void_p()
+        L.check(L.load().sw_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.mode = mode
+        self.nseq = 0
+        self.lengths = np.zeros(0, dtype=np.int64)
+
+    def close(self):
+        if self._h:
+            L.load().sw_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, status):
+        L.check(status, self._h)
+
+    def upload(self, seqs=None, concat=None, offsets=None):
+        if seqs is not None:
+            concat, offsets = pack_sequences(seqs)
+        concat = np.ascontiguousarray(concat, dtype=np.uint8)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        self._ck(L.load().sw_upload_sequences(self._h, L.ptr(concat), L.ptr(offsets), len(offsets) - 1))
+        self.nseq = len(offsets) - 1
+        self.lengths = np.diff(offsets)
+        return self
+
+    def set_option(self, key, value):
+        self._ck(L.load().sw_set_option(self._h, key.encode(), int(value)))
+
+    def query(self, key):
+        v = C.c_int64()
+        self._ck(L.load().sw_query(self._h, key.encode(), C.byref(v)))
+        return v.value
+
+    def use_stream(self, stream_handle):
+        """Order later calls on a caller's CUDA stream (an integer cudaStream_t, 0 = own)."""
+        self.set_option("stream", int(stream_handle))
+
+    def compute_block(self, row_start, row_end, col_start, col_end, is_diagonal, out=None):
+        """The block handler: returns (Int16 block array, pairs computed)."""
+        R, Cc = row_end - row_start + 1, col_end - col_start + 1
+        if out is None:
+            out = np.zeros((R, Cc), dtype=np.int16)
+        n = C.c_int64()
+        self._ck(L.load().sw_compute_block(self._h, row_start, row_end, col_start, col_end,
+                                           int(is_diagonal), L.ptr(out), out.strides[0] // 2, C.byref(n)))
+        return out, n.value
+
+    def compute_block_device(self, row_start, row_end, col_start, col_end, is_diagonal, d_out_ptr, ld):
+        n = C.c_int64()
+        self._ck(L.load().sw_compute_block_device(self._h, row_start, row_end, col_start, col_end,
+                                                  int(is_diagonal), C.c_void_p(d_out_ptr), ld, C.byref(n)))
+        return n.value
+
+    def align(self, s1, s2) -> PairwiseAlignment:
+        a = np.frombuffer(s1.encode() if isinstance(s1, str) else bytes(s1), dtype=np.uint8)
+        b = np.frombuffer(s2.encode() if isinstance(s2, str) else bytes(s2), dtype=np.uint8)
+        a = np.ascontiguousarray(a)
+        b = np.ascontiguousarray(b)
+        r = L.sw_pair_result()
+        self._ck(L.load().sw_align_pair(self._h, L.ptr(a), len(a), L.ptr(b), len(b), C.byref(r)))
+        return PairwiseAlignment(r.score, r.start1, r.start2, r.end1, r.end2, r.identity, r.similarity,
+                                 r.gaps, r.length, r.distance)
+
+    def all_pairs(self, ranks=1):
+        """Whole job to a host N x N Int16 matrix; returns (matrix, pairs, cells)."""
+        out = np.zeros((self.nseq, self.nseq), dtype=np.int16)
+        p, c = C.c_int64(), C.c_int64()
+        self._ck(L.load().sw_all_pairs(self._h, ranks, L.ptr(out), self.nseq, C.byref(p), C.byref(c)))
+        return out, p.value, c.value
+
+    def all_pairs_device(self, d_out_ptr, ld, ranks=1):
+        p, c = C.c_int64(), C.c_int64()
+        self._ck(L.load().sw_all_pairs_device(self._h, ranks, C.c_void_p(d_out_ptr), ld, C.byref(p), C.byref(c)))
+        return p.value, c.value
+
+    def rank_blocks_device(self, rank, world, d_out_ptr, ld):
+        p = C.c_int64()
+        self._ck(L.load().sw_compute_rank_blocks(self._h, rank, world, C.c_void_p(d_out_ptr), ld, C.byref(p)))
+        return p.value
+
+    def rerun_count(self):
+        n = C.c_int64()
+        self._ck(L.load().sw_last_rerun_count(self._h, C.byref(n)))
+        return n.value
+
+    def synchronize(self):
+        self._ck(L.load().sw_synchronize(self._h))
+
+
+class SmithWatermanGotoh:
+    """The reference's aligner object: ``Align(s1, s2, matrix, o, e)`` on the device."""
+
+    def __init__(self, alignment_type=NUCLEIC):
+        self._type = alignment_type
+        self._engines = {}
+
+    def Align(self, s1, s2, matrix: ScoringMatrix, gap_open_penalty, gap_extension_penalty):
+        if s1 is None:
+            raise ValueError("S1 is null")
+        if s2 is None:
+            raise ValueError("S2 is null")
+        key = (matrix.Name, id(matrix), float(gap_open_penalty), float(gap_extension_penalty))
+        eng = self._engines.get(key)
+        if eng is None:
+            eng = Engine(matrix, gap_open_penalty, gap_extension_penalty, alignment_type=self._type)
+            self._engines[key] = eng
+        return eng.align(s1, s2)
+
+
+def measure_int_peak(device=0):
+    """Integer-pipe peak of this device: (max lane-ops/s, add lane-ops/s)."""
+    a, b = C.c_double(), C.c_double()
+    L.check(L.load().sw_measure_int_peak(device, C.byref(a), C.byref(b)))
+    return a.value, b.value

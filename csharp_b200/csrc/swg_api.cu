@@ -1,0 +1,477 @@
+// C-ABI implementation: context lifetime, validation, device residency and dispatch.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/swgb200.h"
+#include "swg_device.cuh"
+#include "swg_engine.h"
+#include "swg_internal.h"
+
+struct sw_ctx {
+  sw_config cfg;
+  int o = 0, e = 0;
+  cudaStream_t stream = nullptr;
+  int sms = 0;
+  std::string err;
+  // sequences
+  uint8_t* d_seq = nullptr;
+  int64_t* d_off = nullptr;
+  std::vector<int64_t> h_off;
+  std::vector<uint8_t> h_seq;
+  int32_t nseq = 0;
+  int maxlen = 0;
+  // tables
+  int16_t* d_scores = nullptr;
+  uint8_t* d_flags = nullptr;
+  int16_t h_scores[128][128];
+  uint8_t h_flags[128][128];
+  int max_abs_score = 0, max_score = 0;
+  // scratch
+  void* d_carry = nullptr;
+  size_t carry_bytes = 0;
+  int16_t* d_stage = nullptr;
+  size_t stage_bytes = 0;
+  swg::Engine* engine = nullptr;
+  int64_t last_reruns = 0;
+  cudaStream_t own_stream = nullptr;  // the context's stream while a caller's stream is in use
+  int64_t last_pairs = 0, last_cells = 0;
+};
+
+namespace {
+
+int fail(sw_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int cuda_fail(sw_ctx* c, cudaError_t e, const char* what) {
+  return fail(c, SW_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call, what)                              \
+  do {                                              \
+    cudaError_t _e = (call);                        \
+    if (_e != cudaSuccess) return cuda_fail(ctx, _e, what); \
+  } while (0)
+
+int ensure(sw_ctx* ctx, void** p, size_t* have, size_t need, const char* what) {
+  if (*have >= need && *p) return SW_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *have = 0;
+  cudaError_t e = cudaMalloc(p, need);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return fail(ctx, SW_E_OOM, std::string("cudaMalloc failed for ") + what);
+  }
+  *have = need;
+  return SW_OK;
+}
+
+// Column flags: which (c1, c2) pairs count toward the distance's numerator.
+void build_flags(sw_ctx* c) {
+  const int mode = c->cfg.mode;
+  const bool protein = c->cfg.alignment_type == SW_PROTEIN;
+  for (int a = 0; a < 128; a++)
+    for (int b = 0; b < 128; b++) {
+      const int s = c->h_scores[a][b];
+      uint32_t f = 0;
+      if (a == b) f |= swg::kFlagIdent;
+      if (a == b || s > 0) f |= swg::kFlagSimNA;
+      bool count;
+      if (!protein) count = (a == b);                 // identity (all three apps)
+      else if (mode == SW_MODE_SWG_MPI) count = (a == b || s > 0);  // NAligner similarity
+      else count = (s > 0);                           // MBF: non-gap pairs with positive score
+      if (count) f |= swg::kFlagCount;
+      if (a == swg::kPadCode || b == swg::kPadCode) f = 0;
+      c->h_flags[a][b] = (uint8_t)f;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* sw_version(void) { return "swgb200 1.0 (sm_100a)"; }
+
+const char* sw_last_error(const sw_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int sw_create(const sw_config* cfg, sw_ctx** out) {
+  if (!cfg || !out) return SW_E_ARG;
+  *out = nullptr;
+  if (cfg->mode < 0 || cfg->mode > 2) return SW_E_ARG;
+  if (cfg->alignment_type != SW_PROTEIN && cfg->alignment_type != SW_NUCLEIC) return SW_E_ARG;
+  if (cfg->distance_fn < 0 || cfg->distance_fn > 2) return SW_E_ARG;
+  if (cfg->lanes != SW_LANES_AUTO && cfg->lanes != SW_LANES_16 && cfg->lanes != SW_LANES_32) return SW_E_ARG;
+  // Kimura2 / JukesCantor need the aligned strings' transition counts: not in this engine.
+  if (cfg->distance_fn != SW_DIST_PERCENT_IDENTITY && cfg->alignment_type == SW_NUCLEIC) return SW_E_UNSUPPORTED;
+  const float o = cfg->gap_open, e = cfg->gap_extension;
+  if (!(std::isfinite(o) && std::isfinite(e))) return SW_E_ARG;
+  if (o != std::floor(o) || e != std::floor(e)) return SW_E_UNSUPPORTED;
+  if (o < 1 || e < 0 || o > 10000 || e > 10000) return SW_E_UNSUPPORTED;
+  if (cfg->mode == SW_MODE_NW && !(o > e)) return SW_E_UNSUPPORTED;
+  sw_ctx* ctx = new (std::nothrow) sw_ctx();
+  if (!ctx) return SW_E_OOM;
+  ctx->cfg = *cfg;
+  ctx->o = (int)o;
+  ctx->e = (int)e;
+  std::memcpy(ctx->h_scores, cfg->scores, sizeof(ctx->h_scores));
+  for (int a = 0; a < 128; a++)
+    for (int b = 0; b < 128; b++) {
+      int s = ctx->h_scores[a][b];
+      if (s < -16383 || s > 16383) { delete ctx; return SW_E_UNSUPPORTED; }
+      if (a == swg::kPadCode || b == swg::kPadCode) ctx->h_scores[a][b] = (int16_t)swg::kPadScore;
+      else {
+        ctx->max_abs_score = std::max(ctx->max_abs_score, std::abs(s));
+        ctx->max_score = std::max(ctx->max_score, s);
+      }
+    }
+  build_flags(ctx);
+  cudaError_t err = cudaSetDevice(cfg->device);
+  if (err != cudaSuccess) { int r = cuda_fail(ctx, err, "cudaSetDevice"); delete ctx; return r; }
+  cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, cfg->device);
+  if ((err = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (err = cudaMalloc(&ctx->d_scores, sizeof(ctx->h_scores))) != cudaSuccess ||
+      (err = cudaMalloc(&ctx->d_flags, sizeof(ctx->h_flags))) != cudaSuccess ||
+      (err = cudaMemcpy(ctx->d_scores, ctx->h_scores, sizeof(ctx->h_scores), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (err = cudaMemcpy(ctx->d_flags, ctx->h_flags, sizeof(ctx->h_flags), cudaMemcpyHostToDevice)) != cudaSuccess) {
+    cudaGetLastError();
+    sw_destroy(ctx);
+    return SW_E_CUDA;
+  }
+  *out = ctx;
+  return SW_OK;
+}
+
+int sw_destroy(sw_ctx* ctx) {
+  if (!ctx) return SW_E_ARG;
+  cudaSetDevice(ctx->cfg.device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->own_stream) ctx->stream = ctx->own_stream;
+  delete ctx->engine;
+  cudaFree(ctx->d_seq);
+  cudaFree(ctx->d_off);
+  cudaFree(ctx->d_scores);
+  cudaFree(ctx->d_flags);
+  cudaFree(ctx->d_carry);
+  cudaFree(ctx->d_stage);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return SW_OK;
+}
+
+int sw_upload_sequences(sw_ctx* ctx, const uint8_t* concat, const int64_t* offsets, int32_t count) {
+  if (!ctx) return SW_E_ARG;
+  if (count < 0 || !offsets || (count > 0 && !concat && offsets[count] > 0))
+    return fail(ctx, SW_E_ARG, "bad sequence arrays");
+  if (offsets[0] != 0) return fail(ctx, SW_E_ARG, "offsets[0] must be 0");
+  int maxlen = 0;
+  for (int32_t k = 0; k < count; k++) {
+    const int64_t len = offsets[k + 1] - offsets[k];
+    if (len < 0) return fail(ctx, SW_E_ARG, "offsets must be non-decreasing");
+    if (len > 32767) return fail(ctx, SW_E_UNSUPPORTED, "sequence longer than 32767 residues");
+    maxlen = std::max(maxlen, (int)len);
+  }
+  const int64_t total = offsets[count];
+  for (int64_t k = 0; k < total; k++)
+    if (concat[k] >= 127)  // ScoringMatrix.Scores is [127,127]: the reference throws
+      return fail(ctx, SW_E_ARG, "residue byte outside the 127-entry scoring table");
+  // The reference's float DP is exact while every value stays below 2^24.
+  const double bound = (double)(ctx->max_abs_score + ctx->e) * 2.0 * maxlen + ctx->o;
+  if (bound >= 16777216.0) return fail(ctx, SW_E_UNSUPPORTED, "scores could exceed float's exact range");
+  cudaSetDevice(ctx->cfg.device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(ctx->d_seq);
+  cudaFree(ctx->d_off);
+  ctx->d_seq = nullptr;
+  ctx->d_off = nullptr;
+  ctx->nseq = 0;
+  // one padding byte block at the end so vector loads past a sequence stay in bounds
+  const size_t seq_bytes = (size_t)total + 64;
+  CK(cudaMalloc(&ctx->d_seq, seq_bytes), "cudaMalloc(sequences)");
+  CK(cudaMalloc(&ctx->d_off, sizeof(int64_t) * (size_t)(count + 1)), "cudaMalloc(offsets)");
+  CK(cudaMemsetAsync(ctx->d_seq, swg::kPadCode, seq_bytes, ctx->stream), "cudaMemset");
+  if (total) CK(cudaMemcpyAsync(ctx->d_seq, concat, (size_t)total, cudaMemcpyHostToDevice, ctx->stream), "upload sequences");
+  CK(cudaMemcpyAsync(ctx->d_off, offsets, sizeof(int64_t) * (size_t)(count + 1), cudaMemcpyHostToDevice, ctx->stream), "upload offsets");
+  CK(cudaStreamSynchronize(ctx->stream), "upload");
+  ctx->h_off.assign(offsets, offsets + count + 1);
+  ctx->h_seq.assign(concat, concat + total);
+  ctx->nseq = count;
+  ctx->maxlen = maxlen;
+  if (ctx->engine) ctx->engine->invalidate();
+  return SW_OK;
+}
+
+static int block_job(sw_ctx* ctx, int32_t rs, int32_t re, int32_t cs, int32_t ce, int32_t diag,
+                     swg::PlainJob* J) {
+  if (!ctx->d_seq) return fail(ctx, SW_E_STATE, "no sequences uploaded");
+  if (rs < 0 || cs < 0 || re >= ctx->nseq || ce >= ctx->nseq || rs > re || cs > ce)
+    return fail(ctx, SW_E_ARG, "block outside the uploaded sequences");
+  const bool tri = diag && ctx->cfg.mode != SW_MODE_SWG_MS;
+  if (tri && (rs != cs || re != ce)) return fail(ctx, SW_E_ARG, "a diagonal block must be square");
+  const long long R = re - rs + 1, Cc = ce - cs + 1;
+  std::memset(J, 0, sizeof(*J));
+  J->seq = ctx->d_seq;
+  J->off = ctx->d_off;
+  J->rs = rs; J->re = re; J->cs = cs; J->ce = ce;
+  J->tri = tri ? 1 : 0;
+  J->npairs = tri ? R * (R - 1) / 2 : R * Cc;
+  J->mirror = tri ? 1 : 0;
+  J->scores = ctx->d_scores;
+  J->flags = ctx->d_flags;
+  J->o = ctx->o;
+  J->e = ctx->e;
+  J->mode = ctx->cfg.mode;
+  J->protein = ctx->cfg.alignment_type == SW_PROTEIN;
+  return SW_OK;
+}
+
+static int run_plain(sw_ctx* ctx, swg::PlainJob& J) {
+  const int block = 128;
+  long threads = (long)ctx->sms * 8 * block;
+  if (J.npairs < threads) threads = ((J.npairs + block - 1) / block) * block;
+  if (threads < block) threads = block;
+  const int grid = (int)(threads / block);
+  int rc = ensure(ctx, &ctx->d_carry, &ctx->carry_bytes,
+                  swg::plain_carry_bytes(J.mode, threads, ctx->maxlen), "carry scratch");
+  if (rc) return rc;
+  J.carry = ctx->d_carry;
+  CK(swg::launch_plain_block(J, grid, block, ctx->stream), "plain block kernel launch");
+  return SW_OK;
+}
+
+int sw_compute_block_device(sw_ctx* ctx, int32_t rs, int32_t re, int32_t cs, int32_t ce,
+                            int32_t diag, int16_t* d_out, int64_t ld, int64_t* pairs) {
+  if (!ctx) return SW_E_ARG;
+  if (!d_out || ld < (int64_t)(ce - cs + 1)) return fail(ctx, SW_E_ARG, "bad output buffer");
+  cudaSetDevice(ctx->cfg.device);
+  swg::PlainJob J;
+  int rc = block_job(ctx, rs, re, cs, ce, diag, &J);
+  if (rc) return rc;
+  J.out = d_out;
+  J.ld = ld;
+  J.out_r0 = rs;
+  J.out_c0 = cs;
+  if ((rc = run_plain(ctx, J))) return rc;
+  if (pairs) *pairs = J.npairs;
+  return SW_OK;
+}
+
+int sw_compute_block(sw_ctx* ctx, int32_t rs, int32_t re, int32_t cs, int32_t ce, int32_t diag,
+                     int16_t* out, int64_t ld, int64_t* pairs) {
+  if (!ctx) return SW_E_ARG;
+  if (!out || ld < (int64_t)(ce - cs + 1)) return fail(ctx, SW_E_ARG, "bad output buffer");
+  cudaSetDevice(ctx->cfg.device);
+  swg::PlainJob J;
+  int rc = block_job(ctx, rs, re, cs, ce, diag, &J);
+  if (rc) return rc;
+  const size_t R = (size_t)(re - rs + 1), Cc = (size_t)(ce - cs + 1);
+  void* stage = ctx->d_stage;
+  if ((rc = ensure(ctx, &stage, &ctx->stage_bytes, R * Cc * sizeof(int16_t), "block staging"))) {
+    ctx->d_stage = nullptr;
+    return rc;
+  }
+  ctx->d_stage = static_cast<int16_t*>(stage);
+  // Start from the caller's values: the handler only writes the pairs it aligns.
+  CK(cudaMemcpy2DAsync(ctx->d_stage, Cc * 2, out, (size_t)ld * 2, Cc * 2, R, cudaMemcpyHostToDevice, ctx->stream), "stage block in");
+  J.out = ctx->d_stage;
+  J.ld = (long long)Cc;
+  J.out_r0 = rs;
+  J.out_c0 = cs;
+  if ((rc = run_plain(ctx, J))) return rc;
+  CK(cudaMemcpy2DAsync(out, (size_t)ld * 2, ctx->d_stage, Cc * 2, Cc * 2, R, cudaMemcpyDeviceToHost, ctx->stream), "copy block out");
+  CK(cudaStreamSynchronize(ctx->stream), "compute block");
+  if (pairs) *pairs = J.npairs;
+  return SW_OK;
+}
+
+int sw_align_pair(sw_ctx* ctx, const uint8_t* s1, int32_t m, const uint8_t* s2, int32_t n,
+                  sw_pair_result* out) {
+  if (!ctx) return SW_E_ARG;
+  if (!out || m < 0 || n < 0) return fail(ctx, SW_E_ARG, "bad arguments");
+  if ((!s1 && m > 0) || (!s2 && n > 0)) return fail(ctx, SW_E_ARG, "S1 or S2 is null");
+  if (m > 32767 || n > 32767) return fail(ctx, SW_E_UNSUPPORTED, "sequence longer than 32767 residues");
+  for (int k = 0; k < m; k++) if (s1[k] >= 127) return fail(ctx, SW_E_ARG, "residue byte outside the scoring table");
+  for (int k = 0; k < n; k++) if (s2[k] >= 127) return fail(ctx, SW_E_ARG, "residue byte outside the scoring table");
+  if (ctx->cfg.mode == SW_MODE_NW) return fail(ctx, SW_E_UNSUPPORTED, "sw_align_pair is the local aligner (SmithWatermanGotoh.Align)");
+  cudaSetDevice(ctx->cfg.device);
+  // one scratch block: [result][s1][s2][carry]
+  const size_t res_b = 256, s_b = ((size_t)m + (size_t)n + 2 + 255) / 256 * 256;
+  const size_t need = res_b + s_b + swg::pair_carry_bytes(n);
+  int rc = ensure(ctx, &ctx->d_carry, &ctx->carry_bytes, need, "pair scratch");
+  if (rc) return rc;
+  char* base = static_cast<char*>(ctx->d_carry);
+  swg::sw_pair_result_dev* d_res = reinterpret_cast<swg::sw_pair_result_dev*>(base);
+  uint8_t* d_s1 = reinterpret_cast<uint8_t*>(base + res_b);
+  uint8_t* d_s2 = d_s1 + m + 1;
+  if (m) CK(cudaMemcpyAsync(d_s1, s1, (size_t)m, cudaMemcpyHostToDevice, ctx->stream), "upload s1");
+  if (n) CK(cudaMemcpyAsync(d_s2, s2, (size_t)n, cudaMemcpyHostToDevice, ctx->stream), "upload s2");
+  swg::PairJob J;
+  J.s1 = d_s1; J.s2 = d_s2; J.m = m; J.n = n;
+  J.scores = ctx->d_scores; J.flags = ctx->d_flags;
+  J.o = ctx->o; J.e = ctx->e;
+  J.carry = base + res_b + s_b;
+  J.out = d_res;
+  CK(swg::launch_align_pair(J, ctx->stream), "align pair launch");
+  swg::sw_pair_result_dev r;
+  CK(cudaMemcpyAsync(&r, d_res, sizeof(r), cudaMemcpyDeviceToHost, ctx->stream), "copy result");
+  CK(cudaStreamSynchronize(ctx->stream), "align pair");
+  out->score = r.score_is_neg_inf ? -INFINITY : (float)r.score;
+  out->end1 = r.end1; out->end2 = r.end2;
+  out->start1 = r.start1; out->start2 = r.start2;
+  out->identity = r.identity; out->similarity = r.similarity;
+  out->gaps = r.gaps; out->length = r.length;
+  // ComputeDistance for this pair on the host, in binary32 like the device epilogue.
+  int count;
+  if (ctx->cfg.alignment_type == SW_NUCLEIC) count = r.identity;
+  else count = r.similarity;
+  volatile float p = (float)count / (float)r.length;
+  volatile float d = (1.0f - p) * 32767.0f;
+  const float x = d;
+  out->distance = (x > -2147483648.0f && x < 2147483648.0f) ? (int16_t)(int32_t)x : 0;
+  out->reserved = 0;
+  return SW_OK;
+}
+
+int sw_synchronize(sw_ctx* ctx) {
+  if (!ctx) return SW_E_ARG;
+  cudaSetDevice(ctx->cfg.device);
+  CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+  return SW_OK;
+}
+
+int sw_last_rerun_count(const sw_ctx* ctx_, int64_t* count) {
+  sw_ctx* ctx = const_cast<sw_ctx*>(ctx_);
+  if (!ctx || !count) return SW_E_ARG;
+  *count = 0;
+  if (!ctx->engine) return SW_OK;
+  cudaSetDevice(ctx->cfg.device);
+  std::string msg;
+  int rc = ctx->engine->rerun_count(ctx->stream, count, &msg);
+  return rc ? fail(ctx, rc, msg) : SW_OK;
+}
+
+static int run_engine(sw_ctx* ctx, int32_t ranks, int row_lo, int row_hi, int16_t* d_out,
+                      int64_t ld, int64_t* pairs, int64_t* cells) {
+  if (!ctx->d_seq) return fail(ctx, SW_E_STATE, "no sequences uploaded");
+  if (!d_out || ld < ctx->nseq || ranks < 1) return fail(ctx, SW_E_ARG, "bad arguments");
+  cudaSetDevice(ctx->cfg.device);
+  if (!ctx->engine) {
+    ctx->engine = swg::Engine::create();
+    if (!ctx->engine) return fail(ctx, SW_E_OOM, "engine");
+  }
+  swg::EngineParams P;
+  P.seq = ctx->d_seq; P.off = ctx->d_off;
+  P.h_off = ctx->h_off.data(); P.h_seq = ctx->h_seq.data();
+  P.nseq = ctx->nseq; P.maxlen = ctx->maxlen;
+  P.scores = ctx->d_scores; P.flags = ctx->d_flags;
+  P.h_scores = &ctx->h_scores[0][0]; P.h_flags = &ctx->h_flags[0][0];
+  P.max_score = ctx->max_score; P.max_abs_score = ctx->max_abs_score;
+  P.o = ctx->o; P.e = ctx->e;
+  P.mode = ctx->cfg.mode;
+  P.protein = ctx->cfg.alignment_type == SW_PROTEIN;
+  P.lanes = ctx->cfg.lanes;
+  P.ranks = ranks;
+  P.row_lo = row_lo;
+  P.row_hi = row_hi;
+  P.out = d_out; P.ld = ld;
+  P.sms = ctx->sms;
+  P.stream = ctx->stream;
+  std::string msg;
+  int64_t np = 0, nc = 0;
+  int rc = ctx->engine->run(P, &np, &nc, &ctx->last_reruns, &msg);
+  if (rc) return fail(ctx, rc, msg);
+  ctx->last_pairs = np;
+  ctx->last_cells = nc;
+  if (pairs) *pairs = np;
+  if (cells) *cells = nc;
+  return SW_OK;
+}
+
+int sw_all_pairs_device(sw_ctx* ctx, int32_t ranks, int16_t* d_out, int64_t ld, int64_t* pairs,
+                        int64_t* cells) {
+  if (!ctx) return SW_E_ARG;
+  return run_engine(ctx, ranks, 0, -1, d_out, ld, pairs, cells);
+}
+
+int sw_compute_rank_blocks(sw_ctx* ctx, int32_t rank, int32_t world, int16_t* d_out, int64_t ld,
+                           int64_t* pairs) {
+  if (!ctx) return SW_E_ARG;
+  if (world < 1 || rank < 0 || rank >= world) return fail(ctx, SW_E_ARG, "rank outside the world");
+  std::vector<int32_t> st(world), en(world);
+  sw_partition_ranges(0, ctx->nseq, world, st.data(), en.data());
+  if (st[rank] > en[rank]) {  // an empty row range owns no pairs
+    if (pairs) *pairs = 0;
+    return SW_OK;
+  }
+  int64_t cells = 0;
+  return run_engine(ctx, world, st[rank], en[rank], d_out, ld, pairs, &cells);
+}
+
+int sw_query(sw_ctx* ctx, const char* key, int64_t* value) {
+  if (!ctx || !key || !value) return SW_E_ARG;
+  const std::string k(key);
+  if (k == "pairs" || k == "cells") {
+    *value = (k == "pairs") ? ctx->last_pairs : ctx->last_cells;
+    return SW_OK;
+  }
+  if (k != "launches" && k != "bins" && k != "alphabet") return fail(ctx, SW_E_ARG, "unknown counter " + k);
+  *value = ctx->engine ? ctx->engine->stat(key) : 0;
+  return SW_OK;
+}
+
+int sw_set_option(sw_ctx* ctx, const char* key, int64_t value) {
+  if (!ctx || !key) return SW_E_ARG;
+  if (!ctx->engine) {
+    ctx->engine = swg::Engine::create();
+    if (!ctx->engine) return fail(ctx, SW_E_OOM, "engine");
+  }
+  const std::string k(key);
+  if (k == "stream") {  // a caller-owned cudaStream_t; 0 restores the context's own stream
+    cudaStreamSynchronize(ctx->stream);
+    if (!ctx->own_stream) ctx->own_stream = ctx->stream;
+    ctx->stream = value ? reinterpret_cast<cudaStream_t>(value) : ctx->own_stream;
+    return SW_OK;
+  }
+  swg::EngineOptions& o = ctx->engine->options();
+  if (k == "int16_threshold") o.int16_threshold = value;
+  else if (k == "use_graph") o.use_graph = value ? 1 : 0;
+  else if (k == "chunk") {
+    if (value < 32 || value > 1024) return fail(ctx, SW_E_ARG, "chunk must be in [32, 1024]");
+    o.chunk = (int)value;
+  } else if (k == "rows_per_lane") {
+    if (value != 0 && value != 4 && value != 8 && value != 12 && value != 16) return fail(ctx, SW_E_ARG, "rows_per_lane must be 0, 4, 8, 12 or 16");
+    o.k_override = (int)value;
+  } else return fail(ctx, SW_E_ARG, "unknown option " + k);
+  return SW_OK;
+}
+
+int sw_all_pairs(sw_ctx* ctx, int32_t ranks, int16_t* out, int64_t ld, int64_t* pairs,
+                 int64_t* cells) {
+  if (!ctx) return SW_E_ARG;
+  if (!out || ld < ctx->nseq) return fail(ctx, SW_E_ARG, "bad output buffer");
+  cudaSetDevice(ctx->cfg.device);
+  const size_t N = (size_t)ctx->nseq;
+  void* stage = ctx->d_stage;
+  int rc = ensure(ctx, &stage, &ctx->stage_bytes, std::max<size_t>(N * N * 2, 2), "result staging");
+  if (rc) { ctx->d_stage = nullptr; return rc; }
+  ctx->d_stage = static_cast<int16_t*>(stage);
+  if ((rc = sw_all_pairs_device(ctx, ranks, ctx->d_stage, (int64_t)N, pairs, cells))) return rc;
+  if (N) CK(cudaMemcpy2DAsync(out, (size_t)ld * 2, ctx->d_stage, N * 2, N * 2, N, cudaMemcpyDeviceToHost, ctx->stream), "copy result");
+  CK(cudaStreamSynchronize(ctx->stream), "all pairs");
+  return SW_OK;
+}
+
+int sw_measure_int_peak(int32_t device, double* max_ops, double* add_ops) {
+  if (!max_ops || !add_ops) return SW_E_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return SW_E_CUDA;
+  return swg::measure_int_peak(max_ops, add_ops) == cudaSuccess ? SW_OK : SW_E_CUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,830 @@
+// Whole-job engine: every pair of an all-pairs job, scheduled by persistent kernels.
+//
+// Work decomposition.  A work item is (query q, a chunk of the database ordered by length).
+// The query is the DP's s1 (rows) and every chunk entry d that the job orients as (s1 = q,
+// s2 = d) is aligned against it: SWG-MPI/NW reproduce the block driver's orientation for a
+// given MPI world size (MPIComputeLowerTriangularBlocked.Compute, Salsa.SmithWatermanMPI/
+// Program.cs:618-642: diagonal blocks align (s_i, s_j) for j < i, off-diagonal block (r, c) is
+// aligned by rank r when r > c with r+c even or r < c with r+c odd), SWG-MS aligns every
+// ordered pair (Salsa.SmithWatermanMS/Program.cs:341-375).  Items are binned by the query's
+// rows-per-lane K and sorted longest first; one persistent kernel per bin pops items from a
+// device counter.  The per-bin launches are captured in a CUDA graph and replayed.
+//
+// Kernel.  A CTA stages the query profile in shared memory; each warp aligns the query against
+// two database sequences at once, one per 16-bit half of every score register (lane A = low
+// half, lane B = high half).  Lane t of the warp owns K consecutive query rows; the DP sweeps
+// the database columns as a wavefront, row-block t working on column s - t at step s and
+// receiving the state of the row above it from lane t-1 by shuffle.  Queries longer than 32*K
+// rows take several passes, the last row of a pass reaching the next through per-warp scratch.
+//
+// Score lanes hold value + bias in [0, 32767]: 32-bit integer adds never carry between the
+// halves and the signed 16x2 max instructions see the true order.  A pair is given to these
+// lanes only when max(score) * (min(m, n) + 1) + bias <= 32767 (static guard); a lane whose
+// best score still reaches the trip threshold is rerun with 32-bit lanes.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <map>
+#include <memory>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "../../include/swgb200.h"
+#include "swg_device.cuh"
+#include "swg_engine.h"
+#include "swg_internal.h"
+
+namespace swg {
+
+constexpr int kEngWarps = 8;
+constexpr int kEngThreads = kEngWarps * 32;
+constexpr int kMaxChunk = 1024;
+constexpr int kScrWords = 8;  // words of carried state per column in the pass scratch
+
+struct EngineJob {
+  const uint8_t* code;      // dense residue codes (pad code = A), same offsets as the residues
+  const int64_t* off;
+  const int32_t* sorted;    // sequence indices by length
+  const int4* items;        // (query, chunk begin, chunk end, passes)
+  int nitems;
+  int* counter;             // next item of this launch
+  const int32_t* lettab;    // [(A+1)*(A+1)] S(a, b) + o; pad row/column -bias + o
+  const uint32_t* flagtab;  // [(A+1)*(A+1)] counted-column flags
+  int A, o, e, bias, thresh;
+  int mode, ranks, nseq, rb_a, rb_b;
+  int16_t* out;
+  long long ld;
+  uint32_t* scratch;        // per (CTA, warp) slot: maxcol * kScrWords words
+  int maxcol;               // longest database sequence
+  int2* rerun;              // pairs to redo with 32-bit lanes
+  int* rerun_count;
+  int rerun_cap;
+  int mpad;                 // profile rows staged (passes * 32 * K of the bin)
+};
+
+// Rank owning a global row index under RangePartitioner (Program.cs:791-802).
+__device__ __forceinline__ int block_of(int x, int a, int b) {
+  return x < b * (a + 1) ? x / (a + 1) : b + (x - b * (a + 1)) / a;
+}
+
+__device__ __forceinline__ bool oriented(const EngineJob& J, int q, int d) {
+  if (J.mode == kModeSwgMs) return true;
+  if (q == d) return false;
+  const int bq = block_of(q, J.rb_a, J.rb_b), bd = block_of(d, J.rb_a, J.rb_b);
+  if (bq == bd) return q > d;
+  const bool odd = ((bq + bd) & 1) != 0;
+  return (bq > bd && !odd) || (bq < bd && odd);
+}
+
+__device__ __forceinline__ uint32_t vmax2(uint32_t a, uint32_t b, bool& hi, bool& lo) {
+  return __vibmax_s16x2(a, b, &hi, &lo);
+}
+
+// One warp, query rows in registers, two database sequences (lanes A/B) in lockstep.
+// prof: shared-memory profile planes, plane(c, kind) at ((c*3+kind) * mpad) words, rows stored
+// per pass in lane-interleaved groups of 4 so each lane's 128-bit load hits distinct banks.
+// ca/cb: shared-memory code buffers with 32 pad entries before column 0.
+template <int K>
+__device__ __forceinline__ void align_two(const uint32_t* __restrict__ prof, int mpad, int passes,
+                                          const uint8_t* __restrict__ ca,
+                                          const uint8_t* __restrict__ cb, int ncols,
+                                          const EngineJob& J, uint32_t* __restrict__ scr,
+                                          int lane, int& bestA, int& rowA, uint32_t& cntA,
+                                          int& bestB, int& rowB, uint32_t& cntB) {
+  const uint32_t bias2 = (uint32_t)J.bias * 0x10001u;
+  const uint32_t O2 = (uint32_t)J.o * 0x10001u, E2 = (uint32_t)J.e * 0x10001u;
+  const uint32_t sent2 = (uint32_t)(J.bias - J.o - J.e) * 0x10001u;  // -infinity + bias
+  const uint32_t best0 = (uint32_t)(J.bias - 1) * 0x10001u;          // below any V
+  const uint32_t vo_top = (uint32_t)(J.bias - J.o) * 0x10001u;        // V(0,j) - o + bias
+  const int plane = 3 * mpad;
+  bestA = bestB = -1;
+  rowA = rowB = 0;
+  cntA = cntB = 0u;
+  for (int p = 0; p < passes; p++) {
+    uint32_t VOL[K], H[K], BEST[K], clA[K], clB[K], chA[K], chB[K], bcA[K], bcB[K];
+#pragma unroll
+    for (int r = 0; r < K; r++) {
+      VOL[r] = vo_top; H[r] = sent2; BEST[r] = best0;
+      clA[r] = clB[r] = chA[r] = chB[r] = bcA[r] = bcB[r] = 0u;
+    }
+    // state received from the row block above (lane - 1), and its previous column
+    uint32_t uVO = vo_top, uG = sent2, ucvA = 0, ucvB = 0, ucgA = 0, ucgB = 0;
+    uint32_t dVO = vo_top, dcA = 0, dcB = 0;
+    const int pbase = p * 32 * K;
+    const uint32_t* pl = prof + pbase + lane * 4;
+    const int nsteps = ncols + 31;
+    for (int s = 0; s < nsteps; s++) {
+      // bottom row of this lane after the previous step, sent down one lane
+      const uint32_t bVO = __shfl_up_sync(0xffffffffu, uVO, 1);
+      const uint32_t bG = __shfl_up_sync(0xffffffffu, uG, 1);
+      const uint32_t bcvA = __shfl_up_sync(0xffffffffu, ucvA, 1);
+      const uint32_t bcvB = __shfl_up_sync(0xffffffffu, ucvB, 1);
+      const uint32_t bcgA = __shfl_up_sync(0xffffffffu, ucgA, 1);
+      const uint32_t bcgB = __shfl_up_sync(0xffffffffu, ucgB, 1);
+      uint32_t VOU, GU, cvuA, cvuB, cguA, cguB;
+      if (lane == 0) {
+        if (p == 0 || s >= ncols) {
+          VOU = vo_top; GU = sent2; cvuA = cvuB = cguA = cguB = 0u;
+        } else {
+          const uint4 x = *reinterpret_cast<const uint4*>(scr + (long)s * kScrWords);
+          const uint2 y = *reinterpret_cast<const uint2*>(scr + (long)s * kScrWords + 4);
+          VOU = x.x; GU = x.y; cvuA = x.z; cvuB = x.w; cguA = y.x; cguB = y.y;
+        }
+      } else {
+        VOU = bVO; GU = bG; cvuA = bcvA; cvuB = bcvB; cguA = bcgA; cguB = bcgB;
+      }
+      // diagonal of the first row: the row above at the previous column
+      uint32_t VOD = dVO, cdA = dcA, cdB = dcB;
+      dVO = VOU; dcA = cvuA; dcB = cvuB;
+      const int col = 32 + s - lane;  // index into the code buffers (pad before column 0)
+      const int xa = ca[col], xb = cb[col];
+      const uint32_t* pla = pl + xa * plane;
+      const uint32_t* phb = pl + xb * plane + mpad;
+      const uint32_t* pma = pl + xa * plane + 2 * mpad;
+      const uint32_t* pmb = pl + xb * plane + 2 * mpad;
+#pragma unroll
+      for (int g = 0; g < K / 4; g++) {
+        const uint4 PL = *reinterpret_cast<const uint4*>(pla + g * 128);
+        const uint4 PH = *reinterpret_cast<const uint4*>(phb + g * 128);
+        const uint4 MA = *reinterpret_cast<const uint4*>(pma + g * 128);
+        const uint4 MB = *reinterpret_cast<const uint4*>(pmb + g * 128);
+        const uint32_t pl4[4] = {PL.x, PL.y, PL.z, PL.w};
+        const uint32_t ph4[4] = {PH.x, PH.y, PH.z, PH.w};
+        const uint32_t ma4[4] = {MA.x, MA.y, MA.z, MA.w};
+        const uint32_t mb4[4] = {MB.x, MB.y, MB.z, MB.w};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const int r = g * 4 + k;
+          const uint32_t F = VOD + pl4[k] + ph4[k];
+          const uint32_t cfA = cdA + ma4[k] + 0x10000u;
+          const uint32_t cfB = cdB + mb4[k] + 0x10000u;
+          bool hiB, loA;
+          // vertical gap: reopen from V above unless extending is strictly better
+          const uint32_t G = vmax2(VOU, GU - E2, hiB, loA);
+          const uint32_t cgA = (loA ? cvuA : cguA) + 0x10000u;
+          const uint32_t cgB = (hiB ? cvuB : cguB) + 0x10000u;
+          // horizontal gap
+          H[r] = vmax2(VOL[r], H[r] - E2, hiB, loA);
+          chA[r] = (loA ? clA[r] : chA[r]) + 0x10000u;
+          chB[r] = (hiB ? clB[r] : chB[r]) + 0x10000u;
+          // V = max(F, G, H, 0) with STOP > DIAGONAL > UP > LEFT on ties
+          const uint32_t GHv = vmax2(G, H[r], hiB, loA);
+          const uint32_t cghA = loA ? cgA : chA[r];
+          const uint32_t cghB = hiB ? cgB : chB[r];
+          const uint32_t FGH = vmax2(F, GHv, hiB, loA);
+          const uint32_t cfgA = loA ? cfA : cghA;
+          const uint32_t cfgB = hiB ? cfB : cghB;
+          const uint32_t V = vmax2(bias2, FGH, hiB, loA);
+          const uint32_t cvA = loA ? 0u : cfgA;
+          const uint32_t cvB = hiB ? 0u : cfgB;
+          // first strictly greater V of this row (columns ascend within a lane)
+          BEST[r] = vmax2(BEST[r], V, hiB, loA);
+          bcA[r] = loA ? bcA[r] : cvA;
+          bcB[r] = hiB ? bcB[r] : cvB;
+          const uint32_t VO = V - O2;
+          VOD = VOL[r]; cdA = clA[r]; cdB = clB[r];
+          VOL[r] = VO; clA[r] = cvA; clB[r] = cvB;
+          VOU = VO; GU = G; cvuA = cvA; cvuB = cvB; cguA = cgA; cguB = cgB;
+        }
+      }
+      uVO = VOU; uG = GU; ucvA = cvuA; ucvB = cvuB; ucgA = cguA; ucgB = cguB;
+      if (lane == 31 && p + 1 < passes) {
+        const int j = s - 31;
+        if (j >= 0 && j < ncols) {
+          *reinterpret_cast<uint4*>(scr + (long)j * kScrWords) = make_uint4(uVO, uG, ucvA, ucvB);
+          *reinterpret_cast<uint2*>(scr + (long)j * kScrWords + 4) = make_uint2(ucgA, ucgB);
+        }
+      }
+    }
+    __syncwarp();
+    // rows ascend within a lane and across passes: keep the first strictly greater
+#pragma unroll
+    for (int r = 0; r < K; r++) {
+      const int row = pbase + lane * K + r;
+      const int sA = (int)(int16_t)(BEST[r] & 0xFFFFu) - J.bias;
+      const int sB = (int)(int16_t)(BEST[r] >> 16) - J.bias;
+      if (sA > bestA) { bestA = sA; rowA = row; cntA = bcA[r]; }
+      if (sB > bestB) { bestB = sB; rowB = row; cntB = bcB[r]; }
+    }
+  }
+}
+
+// Lexicographic (max score, min row) over the warp; lane 0 ends with the winner.
+__device__ __forceinline__ void warp_best(int& best, int& row, uint32_t& cnt) {
+#pragma unroll
+  for (int d = 16; d >= 1; d >>= 1) {
+    const int ob = __shfl_down_sync(0xffffffffu, best, d);
+    const int orow = __shfl_down_sync(0xffffffffu, row, d);
+    const uint32_t oc = __shfl_down_sync(0xffffffffu, cnt, d);
+    if (ob > best || (ob == best && orow < row)) { best = ob; row = orow; cnt = oc; }
+  }
+}
+
+__device__ __forceinline__ void emit(const EngineJob& J, int q, int d, int16_t dist) {
+  J.out[(long long)q * J.ld + d] = dist;
+  if (J.mode != kModeSwgMs) J.out[(long long)d * J.ld + q] = dist;
+}
+
+template <int K>
+__global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineJob J) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint32_t* prof = reinterpret_cast<uint32_t*>(smem);
+  const int A1 = J.A + 1;
+  int* list = reinterpret_cast<int*>(smem + (size_t)A1 * 3 * J.mpad * 4);
+  uint8_t* codes = reinterpret_cast<uint8_t*>(list + kMaxChunk);
+  const int cbuf = 64 + ((J.maxcol + 31) / 32) * 32;
+  __shared__ int s_item, s_count, s_next, s_q;
+  __shared__ int s_wc[kEngWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint8_t* ca = codes + (size_t)warp * 2 * cbuf;
+  uint8_t* cb = ca + cbuf;
+  uint32_t* scr = J.scratch + ((long)blockIdx.x * kEngWarps + warp) * (long)J.maxcol * kScrWords;
+  if (threadIdx.x == 0) s_q = -1;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(J.counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= J.nitems) break;
+    const int4 item = J.items[it];
+    const int q = item.x, c0 = item.y, c1 = item.z, passes = item.w;
+    const int m = (int)(J.off[q + 1] - J.off[q]);
+    const int mrows = passes * 32 * K;
+    // query profile (rows beyond m and the pad column score -bias, count nothing)
+    const bool rebuild = (q != s_q);
+    __syncthreads();
+    if (rebuild) {
+      const uint8_t* qc = J.code + J.off[q];
+      for (int idx = threadIdx.x; idx < A1 * mrows; idx += blockDim.x) {
+        const int c = idx / mrows, i = idx - c * mrows;
+        const int pp = i / (32 * K), rem = i - pp * 32 * K, t = rem / K, rr = rem - t * K;
+        const int pos = pp * 32 * K + ((rr >> 2) * 32 + t) * 4 + (rr & 3);
+        const int a = (i < m) ? (int)qc[i] : J.A;
+        const int v = J.lettab[a * A1 + c];
+        uint32_t* pc = prof + (size_t)c * 3 * J.mpad;
+        pc[pos] = (uint32_t)v;
+        pc[J.mpad + pos] = (uint32_t)v << 16;
+        pc[2 * J.mpad + pos] = J.flagtab[a * A1 + c];
+      }
+    }
+    if (threadIdx.x == 0) { s_q = q; s_count = 0; s_next = 0; }
+    __syncthreads();
+    // compact the chunk entries this query aligns, keeping the chunk's ascending-length order
+    for (int base = c0; base < c1; base += blockDim.x) {
+      const int k = base + threadIdx.x;
+      const int d = (k < c1) ? J.sorted[k] : -1;
+      const bool ok = d >= 0 && oriented(J, q, d);
+      const unsigned bal = __ballot_sync(0xffffffffu, ok);
+      if (lane == 0) s_wc[warp] = __popc(bal);
+      __syncthreads();
+      int before = s_count;
+      for (int w = 0; w < warp; w++) before += s_wc[w];
+      if (ok) list[before + __popc(bal & ((1u << lane) - 1u))] = d;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int w = 0; w < kEngWarps; w++) tot += s_wc[w];
+        s_count += tot;
+      }
+      __syncthreads();
+    }
+    const int cnt = s_count;
+    for (;;) {
+      int pi = 0;
+      if (lane == 0) pi = atomicAdd(&s_next, 2);
+      pi = __shfl_sync(0xffffffffu, pi, 0);
+      if (pi >= cnt) break;
+      const int dA = list[pi];
+      const int dB = (pi + 1 < cnt) ? list[pi + 1] : -1;
+      const int nA = (int)(J.off[dA + 1] - J.off[dA]);
+      const int nB = dB >= 0 ? (int)(J.off[dB + 1] - J.off[dB]) : 0;
+      const int ncols = max(nA, nB);
+      const uint8_t* sa = J.code + J.off[dA];
+      const uint8_t* sb = dB >= 0 ? J.code + J.off[dB] : sa;
+      for (int k = lane; k < 32 + ncols; k += 32) {
+        const int j = k - 32;
+        ca[k] = (j >= 0 && j < nA) ? sa[j] : (uint8_t)J.A;
+        cb[k] = (j >= 0 && j < nB) ? sb[j] : (uint8_t)J.A;
+      }
+      for (int k = 32 + ncols + lane; k < 64 + ncols; k += 32) { ca[k] = (uint8_t)J.A; cb[k] = (uint8_t)J.A; }
+      __syncwarp();
+      int bA, rA, bB, rB;
+      uint32_t cA, cB;
+      if (m > 0 && ncols > 0) {
+        align_two<K>(prof, J.mpad, passes, ca, cb, ncols, J, scr, lane, bA, rA, cA, bB, rB, cB);
+      } else {
+        bA = bB = 0; rA = rB = 0; cA = cB = 0u;
+      }
+      warp_best(bA, rA, cA);
+      warp_best(bB, rB, cB);
+      if (lane == 0) {
+        // a lane whose best reached the trip level is redone with 32-bit lanes
+        if (bA > J.thresh && m > 0 && nA > 0) {
+          const int w = atomicAdd(J.rerun_count, 1);
+          if (w < J.rerun_cap) J.rerun[w] = make_int2(q, dA);
+        } else {
+          const uint32_t c = (m > 0 && nA > 0) ? cA : 0u;
+          emit(J, q, dA, fraction_distance((int)(c & 0xFFFFu), (int)(c >> 16)));
+        }
+        if (dB >= 0) {
+          if (bB > J.thresh && m > 0 && nB > 0) {
+            const int w = atomicAdd(J.rerun_count, 1);
+            if (w < J.rerun_cap) J.rerun[w] = make_int2(q, dB);
+          } else {
+            const uint32_t c = (m > 0 && nB > 0) ? cB : 0u;
+            emit(J, q, dB, fraction_distance((int)(c & 0xFFFFu), (int)(c >> 16)));
+          }
+        }
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void zero_diagonal_kernel(int16_t* out, long long ld, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[(long long)i * ld + i] = 0;
+}
+
+// ------------------------------------------------------------------------------------------------
+namespace {
+
+constexpr int kKs[4] = {4, 8, 12, 16};
+
+size_t engine_smem(int A, int mpad, int maxcol) {
+  const int cbuf = 64 + ((maxcol + 31) / 32) * 32;
+  return (size_t)(A + 1) * 3 * mpad * 4 + kMaxChunk * 4 + (size_t)kEngWarps * 2 * cbuf;
+}
+
+template <int K>
+cudaError_t launch_engine(const EngineJob& J, int grid, size_t smem, cudaStream_t st) {
+  engine_kernel<K><<<grid, kEngThreads, smem, st>>>(J);
+  return cudaGetLastError();
+}
+
+template <int K>
+cudaError_t allow_smem(size_t smem) {
+  return cudaFuncSetAttribute(engine_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+cudaError_t allow_smem_k(int K, size_t smem) {
+  switch (K) {
+    case 4: return allow_smem<4>(smem);
+    case 8: return allow_smem<8>(smem);
+    case 12: return allow_smem<12>(smem);
+    default: return allow_smem<16>(smem);
+  }
+}
+
+__global__ void set_int_kernel(int* p, int v) { *p = v; }
+
+cudaError_t launch_engine_k(int K, const EngineJob& J, int grid, size_t smem, cudaStream_t st) {
+  switch (K) {
+    case 4: return launch_engine<4>(J, grid, smem, st);
+    case 8: return launch_engine<8>(J, grid, smem, st);
+    case 12: return launch_engine<12>(J, grid, smem, st);
+    default: return launch_engine<16>(J, grid, smem, st);
+  }
+}
+
+int occupancy_k(int K, size_t smem) {
+  int n = 0;
+  switch (K) {
+    case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel<4>, kEngThreads, smem); break;
+    case 8: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel<8>, kEngThreads, smem); break;
+    case 12: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel<12>, kEngThreads, smem); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel<16>, kEngThreads, smem); break;
+  }
+  return n;
+}
+
+// Rows per lane and passes for a query of m rows: fewest padded rows, then fewest passes.
+void choose_k(int m, int kov, int* K, int* passes) {
+  if (kov) { *K = kov; *passes = std::max(1, (m + 32 * kov - 1) / (32 * kov)); return; }
+  long best = -1;
+  for (int k : kKs) {
+    const int p = std::max(1, (m + 32 * k - 1) / (32 * k));
+    // padded rows first (the wavefront fill is proportional to them too), then fewer passes
+    const long cost = (long)p * 32 * k * 1000 + p;
+    if (best < 0 || cost < best) { best = cost; *K = k; *passes = p; }
+  }
+}
+
+struct Bin {
+  int K;
+  int mpad;
+  std::vector<int4> items;
+  std::vector<double> cost;
+  int item_offset = 0;
+  size_t smem = 0;
+  int grid = 0;
+};
+
+template <class T>
+int upload_vec(T** dst, const std::vector<T>& v, std::string* msg, const char* what) {
+  cudaFree(*dst);
+  *dst = nullptr;
+  if (cudaMalloc(dst, std::max<size_t>(v.size(), 1) * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    *msg = std::string("cudaMalloc ") + what;
+    return SW_E_OOM;
+  }
+  if (!v.empty() && cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) {
+    *msg = std::string("upload ") + what;
+    return SW_E_CUDA;
+  }
+  return SW_OK;
+}
+
+// State of one sequence set shared by every plan: residue codes, length order, tables.
+struct Base {
+  int alpha = 0, bias = 1, max_s = 0, maxcol = 1;
+  std::vector<int> len, sorted_h;
+  uint8_t* d_code = nullptr;
+  int32_t* d_sorted = nullptr;
+  int32_t* d_lettab = nullptr;
+  uint32_t* d_flagtab = nullptr;
+  uint32_t* d_scratch = nullptr;
+  size_t scratch_bytes = 0;
+  void* d_carry = nullptr;
+  long carry_threads = 0;
+  ~Base() {
+    cudaFree(d_code); cudaFree(d_sorted); cudaFree(d_lettab); cudaFree(d_flagtab);
+    cudaFree(d_scratch); cudaFree(d_carry);
+  }
+};
+
+// One job (mode, world size, query range): its work items, 32-bit pair list and CUDA graph.
+struct Plan {
+  bool plain_only = false;
+  bool zeroes_diagonal = false;
+  int thresh = 0;
+  std::vector<Bin> bins;
+  int big_count = 0, rerun_cap = 0;
+  int64_t npairs = 0, ncells = 0;
+  int4* d_items = nullptr;
+  int* d_counters = nullptr;
+  int2* d_rerun = nullptr;
+  int* d_rerun_count = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int16_t* graph_out = nullptr;
+  long long graph_ld = 0;
+  cudaStream_t graph_stream = nullptr;
+  ~Plan() {
+    if (graph) cudaGraphExecDestroy(graph);
+    cudaFree(d_items); cudaFree(d_counters); cudaFree(d_rerun); cudaFree(d_rerun_count);
+  }
+};
+
+struct PlanKey {
+  int mode, ranks, row_lo, row_hi;
+  bool operator<(const PlanKey& o) const {
+    if (mode != o.mode) return mode < o.mode;
+    if (ranks != o.ranks) return ranks < o.ranks;
+    if (row_lo != o.row_lo) return row_lo < o.row_lo;
+    return row_hi < o.row_hi;
+  }
+};
+
+bool oriented_host(int mode, const std::vector<int>& blk, int q, int d) {
+  if (mode == kModeSwgMs) return true;
+  if (q == d) return false;
+  if (blk[q] == blk[d]) return q > d;
+  const bool odd = ((blk[q] + blk[d]) & 1) != 0;
+  return (blk[q] > blk[d] && !odd) || (blk[q] < blk[d] && odd);
+}
+
+class EngineImpl : public Engine {
+ public:
+  ~EngineImpl() override { invalidate(); }
+  void invalidate() override {
+    plans_.clear();
+    base_.reset();
+    last_ = nullptr;
+  }
+  EngineOptions& options() override {
+    plans_.clear();  // options shape the plans; sequence state stays
+    last_ = nullptr;
+    return opt_;
+  }
+
+  int64_t stat(const char* key) const override {
+    const std::string k(key);
+    if (!last_) return 0;
+    if (k == "launches") {
+      int64_t n = 2;  // the 32-bit lane kernel and the rerun-count reset
+      for (auto& bn : last_->bins) n += bn.items.empty() ? 0 : 1;
+      return n + (last_->zeroes_diagonal ? 1 : 0);
+    }
+    if (k == "bins") {
+      int64_t n = 0;
+      for (auto& bn : last_->bins) n += bn.items.empty() ? 0 : 1;
+      return n;
+    }
+    if (k == "alphabet") return base_ ? base_->alpha : 0;
+    return -1;
+  }
+
+  int rerun_count(cudaStream_t st, int64_t* count, std::string* msg) override {
+    *count = 0;
+    if (!last_ || last_->plain_only || !last_->d_rerun_count) return SW_OK;
+    int hc = 0;
+    cudaError_t e = cudaMemcpyAsync(&hc, last_->d_rerun_count, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { *msg = std::string("rerun count: ") + cudaGetErrorString(e); return SW_E_CUDA; }
+    if (hc > last_->rerun_cap) { *msg = "rerun list overflow"; return SW_E_OOM; }
+    *count = hc;
+    return SW_OK;
+  }
+
+  int run(const EngineParams& P, int64_t* pairs, int64_t* cells, int64_t* reruns,
+          std::string* msg) override {
+    int rc;
+    if (!base_) {
+      base_.reset(new Base());
+      if ((rc = build_base(P, msg))) { base_.reset(); return rc; }
+    }
+    const int N = P.nseq;
+    PlanKey key{P.mode, P.ranks, std::max(0, P.row_lo), P.row_hi < 0 ? N - 1 : std::min(N - 1, P.row_hi)};
+    auto it = plans_.find(key);
+    if (it == plans_.end()) {
+      std::unique_ptr<Plan> pl(new Plan());
+      if ((rc = build_plan(P, key, *pl, msg))) return rc;
+      it = plans_.emplace(key, std::move(pl)).first;
+    }
+    Plan& pl = *it->second;
+    last_ = &pl;
+    cudaError_t e;
+    if (opt_.use_graph) {
+      if (!pl.graph || P.out != pl.graph_out || P.ld != pl.graph_ld || P.stream != pl.graph_stream) {
+        if (pl.graph) cudaGraphExecDestroy(pl.graph);
+        pl.graph = nullptr;
+        cudaStreamBeginCapture(P.stream, cudaStreamCaptureModeThreadLocal);
+        e = enqueue(P, key, pl);
+        cudaGraph_t g = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(P.stream, &g);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+          if (g) cudaGraphDestroy(g);
+          cudaGetLastError();
+          *msg = std::string("graph capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2);
+          return SW_E_CUDA;
+        }
+        e = cudaGraphInstantiate(&pl.graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { pl.graph = nullptr; *msg = "graph instantiate"; return SW_E_CUDA; }
+        pl.graph_out = P.out; pl.graph_ld = P.ld; pl.graph_stream = P.stream;
+      }
+      e = cudaGraphLaunch(pl.graph, P.stream);
+    } else {
+      e = enqueue(P, key, pl);
+    }
+    if (e != cudaSuccess) { *msg = std::string("engine launch: ") + cudaGetErrorString(e); return SW_E_CUDA; }
+    *reruns = -1;  // known once the stream is done (rerun_count)
+    *pairs = pl.npairs;
+    *cells = pl.ncells;
+    return SW_OK;
+  }
+
+ private:
+  int build_base(const EngineParams& P, std::string* msg) {
+    Base& B = *base_;
+    const int N = P.nseq;
+    const int64_t total = P.h_off[N];
+    int code_of[128];
+    std::fill(code_of, code_of + 128, -1);
+    std::vector<int> letters;
+    for (int64_t k = 0; k < total; k++) {
+      const int b = P.h_seq[k];
+      if (code_of[b] < 0) { code_of[b] = (int)letters.size(); letters.push_back(b); }
+    }
+    B.alpha = (int)letters.size();
+    B.len.resize(N);
+    for (int i = 0; i < N; i++) B.len[i] = (int)(P.h_off[i + 1] - P.h_off[i]);
+    B.maxcol = std::max(P.maxlen, 1);
+    int rc;
+    // the 32-bit lanes (reruns, NW, large alphabets) need the plain kernel's scratch
+    B.carry_threads = (long)P.sms * 8 * 128;
+    if (cudaMalloc(&B.d_carry, plain_carry_bytes(P.mode == kModeNw ? kModeNw : kModeSwgMpi, B.carry_threads, B.maxcol)) != cudaSuccess) {
+      cudaGetLastError(); B.d_carry = nullptr; *msg = "cudaMalloc 32-bit lane scratch"; return SW_E_OOM;
+    }
+    if (B.alpha > 8 || P.mode == kModeNw || P.lanes == SW_LANES_32) return SW_OK;
+    const int A = B.alpha, A1 = A + 1;
+    int maxS = 0, minS = 0;
+    for (int a : letters)
+      for (int b : letters) {
+        const int s = P.h_scores[a * 128 + b];
+        maxS = std::max(maxS, s);
+        minS = std::min(minS, s);
+      }
+    B.bias = std::max(std::max(P.o + 2 * P.e, -minS), 1);
+    B.max_s = maxS;
+    std::vector<int32_t> lettab((size_t)A1 * A1);
+    std::vector<uint32_t> flagtab((size_t)A1 * A1, 0u);
+    for (int a = 0; a < A1; a++)
+      for (int c = 0; c < A1; c++) {
+        int s;
+        uint32_t f = 0;
+        if (a == A || c == A) s = -B.bias;
+        else {
+          s = P.h_scores[letters[a] * 128 + letters[c]];
+          f = P.h_flags[letters[a] * 128 + letters[c]] & kFlagCount;
+        }
+        lettab[(size_t)a * A1 + c] = s + P.o;
+        flagtab[(size_t)a * A1 + c] = f;
+      }
+    std::vector<uint8_t> code((size_t)total + 64, (uint8_t)A);
+    for (int64_t k = 0; k < total; k++) code[(size_t)k] = (uint8_t)code_of[P.h_seq[k]];
+    B.sorted_h.resize(N);
+    std::iota(B.sorted_h.begin(), B.sorted_h.end(), 0);
+    std::stable_sort(B.sorted_h.begin(), B.sorted_h.end(), [&](int a, int b) { return B.len[a] < B.len[b]; });
+    if ((rc = upload_vec(&B.d_code, code, msg, "codes"))) return rc;
+    if ((rc = upload_vec(&B.d_sorted, B.sorted_h, msg, "order"))) return rc;
+    if ((rc = upload_vec(&B.d_lettab, lettab, msg, "score table"))) return rc;
+    if ((rc = upload_vec(&B.d_flagtab, flagtab, msg, "flag table"))) return rc;
+    return SW_OK;
+  }
+
+  int build_plan(const EngineParams& P, const PlanKey& key, Plan& pl, std::string* msg) {
+    Base& B = *base_;
+    const int N = P.nseq;
+    std::vector<int> starts(P.ranks), ends(P.ranks), blk(N);
+    sw_partition_ranges(0, N, P.ranks, starts.data(), ends.data());
+    for (int r = 0; r < P.ranks; r++)
+      for (int x = starts[r]; x <= ends[r]; x++) blk[x] = r;
+    int rc;
+    pl.plain_only = B.alpha > 8 || P.mode == kModeNw || P.lanes == SW_LANES_32;
+    std::vector<int2> big;
+    if (pl.plain_only) {
+      for (int q = key.row_lo; q <= key.row_hi; q++)
+        for (int d = 0; d < N; d++) {
+          if (!oriented_host(P.mode, blk, q, d)) continue;
+          big.push_back(make_int2(q, d));
+          pl.ncells += (int64_t)B.len[q] * B.len[d];
+        }
+      pl.npairs = (int64_t)big.size();
+      pl.big_count = (int)big.size();
+      pl.rerun_cap = std::max(pl.big_count, 1);
+      if ((rc = upload_vec(&pl.d_rerun, big, msg, "pair list"))) return rc;
+      std::vector<int> cnt(1, pl.big_count);
+      return upload_vec(&pl.d_rerun_count, cnt, msg, "pair count");
+    }
+    const int A = B.alpha;
+    pl.thresh = (opt_.int16_threshold >= 0) ? (int)opt_.int16_threshold : 32767 - B.bias - B.max_s;
+    const int chunk = std::min(std::max(opt_.chunk, 32), kMaxChunk);
+    const int nchunks = (N + chunk - 1) / chunk;
+    std::vector<std::vector<int>> cidx(nchunks);
+    std::vector<std::vector<double>> csum(nchunks);
+    std::vector<int> cmaxlen(nchunks, 0);
+    for (int c = 0; c < nchunks; c++) {
+      for (int k = c * chunk; k < std::min(N, (c + 1) * chunk); k++) {
+        cidx[c].push_back(B.sorted_h[k]);
+        cmaxlen[c] = std::max(cmaxlen[c], B.len[B.sorted_h[k]]);
+      }
+      std::sort(cidx[c].begin(), cidx[c].end());
+      csum[c].assign(cidx[c].size() + 1, 0.0);
+      for (size_t k = 0; k < cidx[c].size(); k++) csum[c][k + 1] = csum[c][k] + B.len[cidx[c][k]];
+    }
+    pl.bins.clear();
+    for (int k : kKs) { Bin b; b.K = k; b.mpad = 0; pl.bins.push_back(b); }
+    for (int q = key.row_lo; q <= key.row_hi; q++) {
+      const int m = B.len[q];
+      int K, passes;
+      choose_k(m, opt_.k_override, &K, &passes);
+      const int bi = (K == 4) ? 0 : (K == 8) ? 1 : (K == 12) ? 2 : 3;
+      const int bq = blk[q];
+      for (int c = 0; c < nchunks; c++) {
+        const auto& ix = cidx[c];
+        long cnt = 0;
+        double lsum = 0;
+        auto range_count = [&](int lo, int hi) {  // entries with lo <= index < hi
+          const auto a = std::lower_bound(ix.begin(), ix.end(), lo) - ix.begin();
+          const auto b = std::lower_bound(ix.begin(), ix.end(), hi) - ix.begin();
+          cnt += (long)(b - a);
+          lsum += csum[c][b] - csum[c][a];
+        };
+        if (P.mode == kModeSwgMs) {
+          range_count(0, N);
+        } else {
+          for (int r = 0; r < P.ranks; r++) {
+            if (starts[r] > ends[r]) continue;
+            if (r == bq) range_count(starts[r], q);
+            else {
+              const bool odd = ((bq + r) & 1) != 0;
+              if ((bq > r && !odd) || (bq < r && odd)) range_count(starts[r], ends[r] + 1);
+            }
+          }
+        }
+        if (cnt == 0) continue;
+        pl.npairs += cnt;
+        pl.ncells += (int64_t)((double)m * lsum);
+        const int mn = std::min(m, cmaxlen[c]);
+        if ((long)B.max_s * (mn + 1) + B.bias > 32767) {
+          // 16-bit lanes cannot hold this item's scores: its pairs go to 32-bit lanes
+          for (int k = c * chunk; k < std::min(N, (c + 1) * chunk); k++) {
+            const int d = B.sorted_h[k];
+            if (oriented_host(P.mode, blk, q, d)) big.push_back(make_int2(q, d));
+          }
+          continue;
+        }
+        Bin& bn = pl.bins[bi];
+        bn.mpad = std::max(bn.mpad, passes * 32 * K);
+        bn.items.push_back(make_int4(q, c * chunk, std::min(N, (c + 1) * chunk), passes));
+        bn.cost.push_back((double)passes * 32 * K * (lsum + 31.0 * cnt));
+      }
+    }
+    std::vector<int4> all;
+    for (auto& bn : pl.bins) {
+      std::vector<size_t> ord(bn.items.size());
+      std::iota(ord.begin(), ord.end(), 0);
+      std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return bn.cost[a] > bn.cost[b]; });
+      bn.item_offset = (int)all.size();
+      for (size_t k : ord) all.push_back(bn.items[k]);
+    }
+    if ((rc = upload_vec(&pl.d_items, all, msg, "items"))) return rc;
+    std::vector<int> zeros(pl.bins.size() + 1, 0);
+    if ((rc = upload_vec(&pl.d_counters, zeros, msg, "counters"))) return rc;
+    int max_slots = 0;
+    for (auto& bn : pl.bins) {
+      if (bn.items.empty()) continue;
+      bn.smem = engine_smem(A, bn.mpad, B.maxcol);
+      if (bn.smem > 227 * 1024) { *msg = "query profile exceeds shared memory"; return SW_E_UNSUPPORTED; }
+      if (allow_smem_k(bn.K, bn.smem) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
+      const int occ = std::max(1, occupancy_k(bn.K, bn.smem));
+      bn.grid = (int)std::min<long>((long)P.sms * occ, (long)bn.items.size());
+      max_slots = std::max(max_slots, bn.grid);
+    }
+    const size_t scr = std::max<size_t>((size_t)max_slots * kEngWarps * B.maxcol * kScrWords * 4, 16);
+    if (scr > B.scratch_bytes) {
+      cudaFree(B.d_scratch);
+      B.d_scratch = nullptr;
+      B.scratch_bytes = 0;
+      // every plan's graph holds the scratch pointer: growing it retires them
+      for (auto& kv : plans_) if (kv.second->graph) { cudaGraphExecDestroy(kv.second->graph); kv.second->graph = nullptr; }
+      if (cudaMalloc(&B.d_scratch, scr) != cudaSuccess) { cudaGetLastError(); *msg = "cudaMalloc pass scratch"; return SW_E_OOM; }
+      B.scratch_bytes = scr;
+    }
+    pl.big_count = (int)big.size();
+    pl.rerun_cap = (int)std::min<int64_t>(pl.npairs + 1, (int64_t)big.size() + std::max<int64_t>(1 << 16, pl.npairs / 16));
+    std::vector<int2> rl(big);
+    rl.resize((size_t)pl.rerun_cap);
+    if ((rc = upload_vec(&pl.d_rerun, rl, msg, "rerun list"))) return rc;
+    std::vector<int> cnt(1, 0);
+    return upload_vec(&pl.d_rerun_count, cnt, msg, "rerun count");
+  }
+
+  cudaError_t enqueue(const EngineParams& P, const PlanKey& key, Plan& pl) {
+    Base& B = *base_;
+    cudaError_t e;
+    pl.zeroes_diagonal = P.mode != kModeSwgMs && P.nseq > 0 && key.row_lo == 0 && key.row_hi == P.nseq - 1;
+    if (pl.zeroes_diagonal)
+      zero_diagonal_kernel<<<(P.nseq + 255) / 256, 256, 0, P.stream>>>(P.out, P.ld, P.nseq);
+    set_int_kernel<<<1, 1, 0, P.stream>>>(pl.d_rerun_count, pl.big_count);
+    if (!pl.plain_only) {
+      if ((e = cudaMemsetAsync(pl.d_counters, 0, sizeof(int) * (pl.bins.size() + 1), P.stream)) != cudaSuccess) return e;
+      EngineJob J;
+      std::memset(&J, 0, sizeof(J));
+      J.code = B.d_code; J.off = P.off; J.sorted = B.d_sorted;
+      J.lettab = B.d_lettab; J.flagtab = B.d_flagtab;
+      J.A = B.alpha; J.o = P.o; J.e = P.e; J.bias = B.bias; J.thresh = pl.thresh;
+      J.mode = P.mode; J.ranks = P.ranks; J.nseq = P.nseq;
+      J.rb_a = P.nseq / P.ranks; J.rb_b = P.nseq % P.ranks;
+      J.out = P.out; J.ld = P.ld;
+      J.scratch = B.d_scratch; J.maxcol = B.maxcol;
+      J.rerun = pl.d_rerun; J.rerun_count = pl.d_rerun_count; J.rerun_cap = pl.rerun_cap;
+      for (size_t b = 0; b < pl.bins.size(); b++) {
+        const Bin& bn = pl.bins[b];
+        if (bn.items.empty()) continue;
+        J.items = pl.d_items + bn.item_offset;
+        J.nitems = (int)bn.items.size();
+        J.counter = pl.d_counters + b;
+        J.mpad = bn.mpad;
+        if ((e = launch_engine_k(bn.K, J, bn.grid, bn.smem, P.stream)) != cudaSuccess) return e;
+      }
+    }
+    // 32-bit lanes: pairs the static guard routed here, those whose 16-bit lanes tripped, or all
+    PlainJob R;
+    std::memset(&R, 0, sizeof(R));
+    R.seq = P.seq; R.off = P.off;
+    R.list = pl.d_rerun; R.list_count = pl.d_rerun_count;
+    R.npairs = pl.rerun_cap;
+    R.out = P.out; R.ld = P.ld; R.out_r0 = 0; R.out_c0 = 0;
+    R.mirror = P.mode != kModeSwgMs;
+    R.scores = P.scores; R.flags = P.flags;
+    R.o = P.o; R.e = P.e; R.mode = P.mode; R.protein = P.protein;
+    R.carry = B.d_carry;
+    const int grid = pl.big_count > 0 ? (int)(B.carry_threads / 128) : P.sms;
+    return launch_plain_block(R, grid, 128, P.stream);
+  }
+
+  EngineOptions opt_;
+  std::unique_ptr<Base> base_;
+  std::map<PlanKey, std::unique_ptr<Plan>> plans_;
+  Plan* last_ = nullptr;
+};
+
+}  // namespace
+
+Engine* Engine::create() { return new (std::nothrow) EngineImpl(); }
+
+}  // namespace swg

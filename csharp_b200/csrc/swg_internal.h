@@ -1,0 +1,54 @@
+// Internal interfaces between the C-ABI layer (swg_api.cu) and the kernel files.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+
+namespace swg {
+
+enum { kModeSwgMpi = 0, kModeSwgMs = 1, kModeNw = 2 };
+
+// One plain-kernel launch: the pairs of one block.
+struct PlainJob {
+  const uint8_t* seq;      // device: concatenated residues
+  const int64_t* off;      // device: offsets, count + 1 entries
+  int rs, re, cs, ce;      // block (inclusive global indices)
+  int tri;                 // 1: pairs (i, j) with cs <= j < i (diagonal SWG-MPI/NW block)
+  long long npairs;
+  int16_t* out;            // device output
+  long long ld;
+  int out_r0, out_c0;      // global index of out's element (0, 0)
+  int mirror;              // also write (j, i)
+  const int16_t* scores;   // device [128*128]
+  const uint8_t* flags;    // device [128*128]
+  int o, e;
+  int mode;
+  int protein;
+  void* carry;             // device scratch, plain_carry_bytes(mode, threads, maxlen)
+  const int2* list;        // optional explicit pairs (s1 index, s2 index); replaces the block
+  const int* list_count;   // device count of list entries (at most npairs are read)
+};
+
+struct sw_pair_result_dev {
+  int score, score_is_neg_inf;
+  int end1, end2, start1, start2, identity, similarity, gaps, length;
+};
+
+struct PairJob {
+  const uint8_t* s1;
+  const uint8_t* s2;
+  int m, n;
+  const int16_t* scores;
+  const uint8_t* flags;
+  int o, e;
+  void* carry;  // pair_carry_bytes(n)
+  sw_pair_result_dev* out;
+};
+
+size_t plain_carry_bytes(int mode, long threads, int maxlen);
+cudaError_t launch_plain_block(const PlainJob& J, int grid, int block, cudaStream_t st);
+size_t pair_carry_bytes(int n);
+cudaError_t launch_align_pair(const PairJob& J, cudaStream_t st);
+cudaError_t measure_int_peak(double* max_ops, double* add_ops);
+
+}  // namespace swg

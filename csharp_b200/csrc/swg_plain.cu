@@ -1,0 +1,317 @@
+// Plain block kernel: the drop-in replacement of one ComputeBlock call
+// (SalsaTPL/Salsa.SmithWatermanMPI/Program.cs:203-257, Salsa.SmithWatermanMS/Program.cs:341-375,
+// Salsa.NeedlemanWunschTPL/Program.cs:206-267).  One launch per block, one thread per pair,
+// int32 score lanes.  A thread walks its pair in strips of K rows held in registers; the row
+// below each strip (V, G and their counters per column) is carried to the next strip through a
+// per-thread slice of global scratch, interleaved across threads so a warp's accesses coalesce.
+// Substitution scores and column flags are staged in shared memory.
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "swg_device.cuh"
+#include "swg_internal.h"
+
+namespace swg {
+
+template <class CP>
+struct Carry {
+  int v, g;
+  typename CP::T cv, cg;
+};
+
+template <class CP>
+struct DpResult {
+  int best;  // SW: traceback start score; NW: V(m,n)
+  int bi, bj;
+  typename CP::T c;
+};
+
+// The DP of one pair.  s1 rows (1..m), s2 columns (1..n), both non-empty.
+template <bool LOCAL, class CP, int K, bool TRACK_POS>
+__device__ __forceinline__ DpResult<CP> dp_pair(const uint8_t* __restrict__ s1, int m,
+                                                const uint8_t* __restrict__ s2, int n,
+                                                const int16_t* sc, const uint8_t* fl, int o, int e,
+                                                Carry<CP>* carry, long stride) {
+  typedef typename CP::T T;
+  DpResult<CP> res;
+  res.best = kNegInf;
+  res.bi = res.bj = 0;
+  res.c = CP::origin();
+  for (int s0 = 0; s0 < m; s0 += K) {
+    int c1[K], vl[K], h[K], bv[K], bj[K];
+    T cl[K], ch[K], bc[K];
+#pragma unroll
+    for (int r = 0; r < K; r++) {
+      const int i = s0 + r + 1;
+      c1[r] = (i <= m) ? (int)s1[i - 1] * kTable : kPadCode * kTable;
+      vl[r] = LOCAL ? 0 : (-o - (i - 1) * e);
+      cl[r] = LOCAL ? CP::stop(i, 0) : CP::col0(i);
+      h[r] = kNegInf;
+      ch[r] = CP::origin();
+      bv[r] = kNegInf;
+      bc[r] = CP::origin();
+      bj[r] = 0;
+    }
+    int vdiag = (LOCAL || s0 == 0) ? 0 : (-o - (s0 - 1) * e);
+    T cdiag = LOCAL ? CP::stop(s0, 0) : (s0 == 0 ? CP::origin() : CP::col0(s0));
+    for (int j = 1; j <= n; j++) {
+      const int c2 = s2[j - 1];
+      int vu, gu;
+      T cvu, cgu;
+      if (s0 == 0) {
+        vu = LOCAL ? 0 : (-o - (j - 1) * e);
+        gu = kNegInf;
+        cvu = LOCAL ? CP::stop(0, j) : CP::row0(j);
+        cgu = cvu;
+      } else {
+        const Carry<CP> cr = carry[(long)j * stride];
+        vu = cr.v; gu = cr.g; cvu = cr.cv; cgu = cr.cg;
+      }
+      int vd = vdiag;
+      T cd = cdiag;
+      vdiag = vu;
+      cdiag = cvu;
+#pragma unroll
+      for (int r = 0; r < K; r++) {
+        const int s = sc[c1[r] + c2];
+        const uint32_t f = fl[c1[r] + c2];
+        int v, g;
+        T cv, cg;
+        gotoh_cell<LOCAL, CP>(s, f, vd, cd, vu, gu, cvu, cgu, vl[r], cl[r], h[r], ch[r], o, e,
+                              s0 + r + 1, j, v, g, cv, cg);
+        vd = vl[r];
+        cd = cl[r];
+        vl[r] = v;
+        cl[r] = cv;
+        vu = v; gu = g; cvu = cv; cgu = cg;
+        if (LOCAL && v > bv[r]) {
+          bv[r] = v;
+          bc[r] = cv;
+          if (TRACK_POS) bj[r] = j;
+        }
+      }
+      if (s0 + K < m) {
+        Carry<CP> cw;
+        cw.v = vu; cw.g = gu; cw.cv = cvu; cw.cg = cgu;
+        carry[(long)j * stride] = cw;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < K; r++) {
+      const int i = s0 + r + 1;
+      if (LOCAL) {
+        if (i <= m && bv[r] > res.best) {
+          res.best = bv[r];
+          res.c = bc[r];
+          res.bi = i;
+          res.bj = bj[r];
+        }
+      } else if (i == m) {
+        res.best = vl[r];
+        res.c = cl[r];
+        res.bi = m;
+        res.bj = n;
+      }
+    }
+  }
+  return res;
+}
+
+// ---- pair enumeration of a block -----------------------------------------------------------
+// tri: rows rs..re, columns cs..i-1 (diagonal blocks of SWG-MPI/NW, cs == rs); else the full
+// rectangle.
+__device__ __forceinline__ void pair_of(long long p, const PlainJob& J, int& i, int& j) {
+  if (J.tri) {
+    // p = a(a-1)/2 + b with a = i - rs >= 1, 0 <= b < a
+    long long a = (long long)((1.0 + sqrt(1.0 + 8.0 * (double)p)) * 0.5);
+    while (a * (a - 1) / 2 > p) a--;
+    while ((a + 1) * a / 2 <= p) a++;
+    i = J.rs + (int)a;
+    j = J.cs + (int)(p - a * (a - 1) / 2);
+  } else {
+    const int cols = J.ce - J.cs + 1;
+    i = J.rs + (int)(p / cols);
+    j = J.cs + (int)(p % cols);
+  }
+}
+
+__device__ __forceinline__ void load_tables(const PlainJob& J, int16_t* sc, uint8_t* fl) {
+  for (int k = threadIdx.x; k < kTable * kTable; k += blockDim.x) {
+    sc[k] = J.scores[k];
+    fl[k] = J.flags[k];
+  }
+  __syncthreads();
+}
+
+// NW distance (Salsa.NeedlemanWunschTPL/Program.cs:547-571): identity over the aligned region
+// with the leading and trailing same-type gap runs removed; protein: similarity over the full
+// aligned length (:583-604).
+__device__ __forceinline__ int16_t nw_distance(const NwCnt::T& c, int m, int n, int protein) {
+  const int count = (int)(c.w0 & 0xFFFFu), len = (int)(c.w0 >> 16);
+  if (protein) return fraction_distance(count, len);
+  const int lead = (int)(c.w1 >> 16);
+  const int run = (int)(int16_t)(c.w1 & 0xFFFFu);
+  int trimmed = len - lead - (run < 0 ? -run : run);
+  if (m == 0 || n == 0) trimmed = 0;  // a single gap run: first non-gap index > last
+  return fraction_distance(count, trimmed);
+}
+
+template <bool LOCAL, class CP, int K>
+__global__ void __launch_bounds__(128) plain_block_kernel(PlainJob J) {
+  __shared__ int16_t sc[kTable * kTable];
+  __shared__ uint8_t fl[kTable * kTable];
+  load_tables(J, sc, fl);
+  const long stride = (long)gridDim.x * blockDim.x;
+  const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  Carry<CP>* carry = reinterpret_cast<Carry<CP>*>(J.carry) + tid;
+  long long np = J.npairs;
+  if (J.list) np = min(np, (long long)*J.list_count);
+  for (long long p = tid; p < np; p += stride) {
+    int i, j;
+    if (J.list) {
+      const int2 pr = J.list[p];
+      i = pr.x;
+      j = pr.y;
+    } else {
+      pair_of(p, J, i, j);
+    }
+    const uint8_t* s1 = J.seq + J.off[i];
+    const uint8_t* s2 = J.seq + J.off[j];
+    const int m = (int)(J.off[i + 1] - J.off[i]), n = (int)(J.off[j + 1] - J.off[j]);
+    int16_t d;
+    if (LOCAL) {
+      if (m == 0 || n == 0) {
+        d = fraction_distance(0, 0);
+      } else {
+        DpResult<CP> r = dp_pair<LOCAL, CP, K, false>(s1, m, s2, n, sc, fl, J.o, J.e, carry, stride);
+        const uint32_t w = *reinterpret_cast<const uint32_t*>(&r.c);
+        d = fraction_distance((int)(w & 0xFFFFu), (int)(w >> 16));
+      }
+    } else {
+      NwCnt::T c;
+      if (m == 0 && n == 0) c = NwCnt::origin();
+      else if (m == 0) c = NwCnt::row0(n);
+      else if (n == 0) c = NwCnt::col0(m);
+      else {
+        DpResult<CP> r = dp_pair<LOCAL, CP, K, false>(s1, m, s2, n, sc, fl, J.o, J.e, carry, stride);
+        c = *reinterpret_cast<const NwCnt::T*>(&r.c);
+      }
+      d = nw_distance(c, m, n, J.protein);
+    }
+    J.out[(long long)(i - J.out_r0) * J.ld + (j - J.out_c0)] = d;
+    if (J.mirror) J.out[(long long)(j - J.out_r0) * J.ld + (i - J.out_c0)] = d;
+  }
+}
+
+// Single pair with every PairwiseAlignment field (SmithWatermanGotoh.Align).
+__global__ void __launch_bounds__(32) align_pair_kernel(PairJob J) {
+  __shared__ int16_t sc[kTable * kTable];
+  __shared__ uint8_t fl[kTable * kTable];
+  for (int k = threadIdx.x; k < kTable * kTable; k += blockDim.x) {
+    sc[k] = J.scores[k];
+    fl[k] = J.flags[k];
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  sw_pair_result_dev out;
+  if (J.m == 0 || J.n == 0) {
+    out.score_is_neg_inf = 1;
+    out.score = 0;
+    out.end1 = out.end2 = out.start1 = out.start2 = 0;
+    out.identity = out.similarity = out.gaps = out.length = 0;
+  } else {
+    DpResult<FullCnt> r = dp_pair<true, FullCnt, 4, true>(J.s1, J.m, J.s2, J.n, sc, fl, J.o, J.e,
+                                                          reinterpret_cast<Carry<FullCnt>*>(J.carry), 1);
+    out.score_is_neg_inf = 0;
+    out.score = r.best;
+    out.end1 = r.bi;
+    out.end2 = r.bj;
+    out.start1 = r.c.si;
+    out.start2 = r.c.sj;
+    out.identity = r.c.id;
+    out.similarity = r.c.sim;
+    out.length = r.c.len;
+    out.gaps = r.c.len - ((r.bi - r.c.si) + (r.bj - r.c.sj) - r.c.len);
+  }
+  *J.out = out;
+}
+
+// ---- launchers -----------------------------------------------------------------------------
+size_t plain_carry_bytes(int mode, long threads, int maxlen) {
+  const size_t per = (mode == kModeNw) ? sizeof(Carry<NwCnt>) : sizeof(Carry<SwCnt>);
+  return per * (size_t)threads * (size_t)(maxlen + 1);
+}
+
+cudaError_t launch_plain_block(const PlainJob& J, int grid, int block, cudaStream_t st) {
+  if (J.npairs == 0) return cudaSuccess;
+  if (J.mode == kModeNw) plain_block_kernel<false, NwCnt, 8><<<grid, block, 0, st>>>(J);
+  else plain_block_kernel<true, SwCnt, 8><<<grid, block, 0, st>>>(J);
+  return cudaGetLastError();
+}
+
+size_t pair_carry_bytes(int n) { return sizeof(Carry<FullCnt>) * (size_t)(n + 1); }
+
+cudaError_t launch_align_pair(const PairJob& J, cudaStream_t st) {
+  align_pair_kernel<<<1, 32, 0, st>>>(J);
+  return cudaGetLastError();
+}
+
+// ---- integer-pipe calibration --------------------------------------------------------------
+// Eight ring-coupled chains of a 2-input op per thread (no chain folds because each op reads a
+// different neighbour).  Used as the roofline denominator of the cell-update kernels.
+template <int OP>
+__global__ void int_peak_kernel(int* out, int seed, int iters) {
+  int x[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) x[k] = seed * (k + 1) + (int)threadIdx.x * 7 + k;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      int r;
+      if (OP == 0) asm volatile("max.s32 %0, %1, %2;" : "=r"(r) : "r"(x[k]), "r"(x[(k + 1) & 7]));
+      else asm volatile("add.s32 %0, %1, %2;" : "=r"(r) : "r"(x[k]), "r"(x[(k + 1) & 7]));
+      x[k] = r;
+    }
+  }
+  int s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) s ^= x[k];
+  out[(long)blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+cudaError_t measure_int_peak(double* max_ops, double* add_ops) {
+  int dev;
+  cudaGetDevice(&dev);
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int blocks = sms * 8, threads = 256, iters = 4096;
+  int* d = nullptr;
+  cudaError_t err = cudaMalloc(&d, sizeof(int) * (size_t)blocks * threads);
+  if (err != cudaSuccess) return err;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  double res[2];
+  for (int op = 0; op < 2; op++) {
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; rep++) {
+      cudaEventRecord(e0);
+      if (op == 0) int_peak_kernel<0><<<blocks, threads>>>(d, rep + 1, iters);
+      else int_peak_kernel<1><<<blocks, threads>>>(d, rep + 1, iters);
+      cudaEventRecord(e1);
+      cudaEventSynchronize(e1);
+      float ms;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep > 0 && ms < best) best = ms;
+    }
+    res[op] = (double)blocks * threads * iters * 8.0 / (best * 1e-3);
+  }
+  err = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d);
+  *max_ops = res[0];
+  *add_ops = res[1];
+  return err;
+}
+
+}  // namespace swg

@@ -1,0 +1,82 @@
+"""File formats around the distance path, through the C ABI's host library.
+
+* FASTA input            Salsa.CoreTPL/Bio/IO/Parser.cs:123-180 (residues trimmed, upper-cased)
+* full Int16 matrix      Salsa.SmithWatermanMPI/Program.cs:786-888 (raw little-endian, no header)
+* SWG-MS block files     Salsa.SmithWatermanMS/Program.cs:1081-1160 ({rank}-{cb}.bin)
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import lib as L
+
+
+def parse_fasta(text):
+    """Returns (labels, concatenated residues uint8, offsets int64)."""
+    if isinstance(text, str):
+        text = text.encode()
+    cnt, res = C.c_int32(), C.c_int64()
+    L.check(L.load().sw_parse_fasta(text, len(text), None, None, C.byref(cnt), C.byref(res)))
+    concat = np.zeros(max(res.value, 1), dtype=np.uint8)
+    off = np.zeros(cnt.value + 1, dtype=np.int64)
+    L.check(L.load().sw_parse_fasta(text, len(text), L.ptr(concat), L.ptr(off), C.byref(cnt), C.byref(res)))
+    labels = [ln[1:].strip() for ln in text.decode(errors="replace").splitlines() if ln.strip().startswith(">")]
+    return labels, concat[: res.value], off
+
+
+def read_fasta(path):
+    with open(path, "rb") as f:
+        return parse_fasta(f.read())
+
+
+def write_fasta(path, labels, seqs):
+    with open(path, "w") as f:
+        for lab, s in zip(labels, seqs):
+            f.write(f">{lab}\n")
+            s = s.decode() if isinstance(s, (bytes, bytearray)) else (s.tobytes().decode() if isinstance(s, np.ndarray) else s)
+            for k in range(0, len(s), 80):
+                f.write(s[k:k + 80] + "\n")
+
+
+def write_full_matrix(path, m: np.ndarray):
+    m = np.ascontiguousarray(m, dtype=np.int16)
+    L.check(L.load().sw_write_full_matrix(os.fsencode(path), L.ptr(m), m.shape[0], m.shape[1], m.shape[1]))
+
+
+def read_full_matrix(path, n):
+    return np.fromfile(path, dtype="<i2").reshape(n, n)
+
+
+def write_ms_block(path, values: np.ndarray, rank, row_block, col_block, row_range, col_range,
+                   ids, project="swg", system="b200", fasta="input.fasta"):
+    """One SWG-MS block file; ids[k] is the label of sequence k (Range.StartSeqName etc.)."""
+    v = np.ascontiguousarray(values, dtype=np.int16)
+    h = L.sw_ms_block_header(project.encode(), system.encode(), fasta.encode(), rank, row_block,
+                             col_block, row_range[0], row_range[1], col_range[0], col_range[1],
+                             ids[row_range[0]].encode(), ids[row_range[1]].encode(),
+                             ids[col_range[0]].encode(), ids[col_range[1]].encode())
+    L.check(L.load().sw_write_ms_block(os.fsencode(path), C.byref(h), L.ptr(v), v.shape[1]))
+
+
+def read_ms_block(path):
+    """Returns (dict of header numbers, values)."""
+    vals = [C.c_int32() for _ in range(7)]
+    L.check(L.load().sw_read_ms_block_dims(os.fsencode(path), *[C.byref(x) for x in vals]))
+    rank, rb, cb, rs, re, cs, ce = (x.value for x in vals)
+    out = np.zeros((re - rs + 1, ce - cs + 1), dtype=np.int16)
+    L.check(L.load().sw_read_ms_block_values(os.fsencode(path), L.ptr(out), out.shape[1]))
+    return dict(rank=rank, row_block=rb, col_block=cb, row_start=rs, row_end=re, col_start=cs, col_end=ce), out
+
+
+def read_restart_file(path):
+    """SWG-MS restart file (Program.cs:245-262): world size, then 'rank lastSavedBlock' lines."""
+    with open(path) as f:
+        world = int(f.readline().strip())
+        entries = []
+        for ln in f:
+            ln = ln.strip()
+            if ln:
+                a, b = ln.replace("\t", " ").split()[:2]
+                entries.append((int(a), int(b)))
+    return world, entries

@@ -1,0 +1,233 @@
+/*
+ * swgb200.h - C ABI of the B200 all-pairs alignment -> distance engine.
+ *
+ * The engine replaces the per-pair aligner calls inside the reference's block handlers
+ * (DSC-SPIDAL/csharp, SalsaTPL/) with CUDA kernels for sm_100a.  Every entry point takes plain
+ * pointers and sizes, returns an int status (SW_OK = 0) and never throws; sw_last_error() gives
+ * the text of the last failure on a context.  A context is bound to one CUDA device and one
+ * stream, is not re-entrant, and distinct contexts may be used from distinct threads.
+ *
+ * Sequences are byte strings (the upper-cased residue characters, as the reference's FASTA
+ * parser produces them: Salsa.CoreTPL/Bio/IO/Parser.cs:140-144).  Scores index the 128 x 128
+ * substitution table by those bytes, as ScoringMatrix.Scores[char, char] does
+ * (Salsa.CoreTPL/Bio/Algorithms/ScoringMatrix.cs:34, :130-143).
+ */
+#ifndef SWGB200_H
+#define SWGB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference raises exceptions; none cross this boundary) ------------- */
+#define SW_OK 0
+#define SW_E_ARG 1          /* bad argument (null pointer, range outside the uploaded set, ...) */
+#define SW_E_OOM 2          /* device or host allocation failed */
+#define SW_E_CUDA 3         /* a CUDA runtime call failed */
+#define SW_E_TIMEOUT 4      /* a bounded device-side wait ran out */
+#define SW_E_UNSUPPORTED 5  /* configuration the exact integer kernels cannot reproduce */
+#define SW_E_STATE 6        /* call order (e.g. compute before sequences were uploaded) */
+#define SW_E_IO 7           /* file could not be read or written */
+#define SW_E_THROWS 8       /* the reference would throw for this input (JukesCantor log(0)) */
+
+/* AlignmentType (Salsa.CoreTPL/Bio/Algorithms/AlignmentType.cs:3-7) */
+#define SW_PROTEIN 0
+#define SW_NUCLEIC 1
+
+/* DistanceFunctionType (AlignmentType.cs:9-15) */
+#define SW_DIST_PERCENT_IDENTITY 0
+#define SW_DIST_KIMURA2 1
+#define SW_DIST_JUKES_CANTOR 2
+
+/* Which reference application's semantics a context reproduces. */
+#define SW_MODE_SWG_MPI 0 /* Salsa.SmithWatermanMPI: NAligner SW-Gotoh, diagonal blocks j < i */
+#define SW_MODE_SWG_MS 1  /* Salsa.SmithWatermanMS: SW-Gotoh, full blocks, MBF distance rules */
+#define SW_MODE_NW 2      /* Salsa.NeedlemanWunschTPL: global affine alignment, trimmed identity */
+
+/* Score lane width policy. */
+#define SW_LANES_AUTO 0   /* 16-bit packed lanes where a pair provably fits, else 32-bit */
+#define SW_LANES_32 32    /* 32-bit lanes only */
+#define SW_LANES_16 16    /* 16-bit packed lanes; a pair whose scores could leave int16 reruns in 32-bit */
+
+typedef struct sw_ctx sw_ctx;
+
+typedef struct {
+  int32_t mode;           /* SW_MODE_* */
+  int32_t alignment_type; /* SW_NUCLEIC or SW_PROTEIN (selects identity vs similarity) */
+  int32_t distance_fn;    /* SW_DIST_* */
+  float gap_open;         /* positive cost of a gap's first column (GapOpenPenalty) */
+  float gap_extension;    /* positive cost of each further column (GapExtensionPenalty) */
+  int16_t scores[128][128]; /* substitution table indexed by residue bytes */
+  int32_t device;         /* CUDA device ordinal */
+  int32_t lanes;          /* SW_LANES_* */
+} sw_config;
+
+/* One pair's alignment summary: the PairwiseAlignment fields the reference's distance
+ * functions read (Salsa.CoreTPL/Bio/Algorithms/Alignment.cs:124-195). */
+typedef struct {
+  float score;        /* PairwiseAlignment.Score; -inf for an empty input (Cell.cs:43) */
+  int32_t end1, end2; /* traceback start cell (Cell.Row, Cell.Column); SW only */
+  int32_t start1, start2; /* PairwiseAlignment.Start1/Start2 */
+  int32_t identity;   /* identical columns */
+  int32_t similarity; /* identical or positive-score columns (NAligner rule) */
+  int32_t gaps;       /* gap columns */
+  int32_t length;     /* aligned columns (Sequence1.Length) */
+  int16_t distance;   /* the context's Int16 distance for this pair */
+  int16_t reserved;
+} sw_pair_result;
+
+/* ---- context ---------------------------------------------------------------------------- */
+/* Replaces the handler's ambient configuration: the static fields _gapOpen, _gapExtension,
+ * _scoringMatrixName, _alignmentType and _distanceFunction that ComputeBlock reads
+ * (Salsa.SmithWatermanMPI/Program.cs:58-62, :206-207; Salsa.SmithWatermanMS/Program.cs:275-276;
+ * Salsa.NeedlemanWunschTPL/Program.cs:210-213).  Non-integer penalties are SW_E_UNSUPPORTED:
+ * the reference's float DP is exact only on integers, which the integer kernels reproduce. */
+int sw_create(const sw_config* cfg, sw_ctx** out);
+int sw_destroy(sw_ctx* ctx);
+const char* sw_last_error(const sw_ctx* ctx);
+const char* sw_version(void);
+
+/* Replaces the parsed FASTA list _sequences (Salsa.SmithWatermanMPI/Program.cs:94-95): the
+ * sequences stay resident on the device for every later call.  concat holds all residues,
+ * sequence k is concat[offsets[k] .. offsets[k+1]).  Lengths up to 32767. */
+int sw_upload_sequences(sw_ctx* ctx, const uint8_t* concat, const int64_t* offsets, int32_t count);
+
+/* ---- the block handler (drop-in) ---------------------------------------------------------- */
+/* Replaces ComputeBlockHandler / ComputeBlock:
+ *   Salsa.SmithWatermanMPI/Program.cs:203-257 (delegate :561),
+ *   Salsa.SmithWatermanMS/Program.cs:265-387  (delegate :1018),
+ *   Salsa.NeedlemanWunschTPL/Program.cs:206-267 (delegate :977).
+ * Rows row_start..row_end and columns col_start..col_end are inclusive global sequence indices
+ * (Block.RowRange / Block.ColumnRange).  out is the caller's row-major Int16 buffer over the
+ * block, element (i, j) at out[(i - row_start) * ld_out + (j - col_start)].  For a diagonal
+ * block in SWG-MPI and NW mode only j < i is aligned (s1 = sequence i) and each distance is
+ * also written at the mirrored (j, i) position, as `matrix[i, j] = matrix[j, i]` does; SWG-MS
+ * mode aligns every (i, j) of the block.  *pairs_computed receives the handler's return value.
+ * sw_compute_block copies to host memory and returns when done; sw_compute_block_device writes
+ * device memory, is ordered on the context's stream and does not wait. */
+int sw_compute_block(sw_ctx* ctx, int32_t row_start, int32_t row_end, int32_t col_start,
+                     int32_t col_end, int32_t is_diagonal, int16_t* out, int64_t ld_out,
+                     int64_t* pairs_computed);
+int sw_compute_block_device(sw_ctx* ctx, int32_t row_start, int32_t row_end, int32_t col_start,
+                            int32_t col_end, int32_t is_diagonal, int16_t* d_out, int64_t ld_out,
+                            int64_t* pairs_computed);
+
+/* ---- the per-pair aligner ----------------------------------------------------------------- */
+/* Replaces SmithWatermanGotoh.Align (Salsa.CoreTPL/Bio/Algorithms/SmithWaterman/
+ * SmithWatermanGotoh.cs:52-110) plus the handler's ComputeDistance for that pair
+ * (Salsa.SmithWatermanMPI/Program.cs:259-285).  A null sequence pointer with a non-zero length
+ * is SW_E_ARG, as Align throws SmithWatermanGotohException for a null sequence (:55-65). */
+int sw_align_pair(sw_ctx* ctx, const uint8_t* s1, int32_t m, const uint8_t* s2, int32_t n,
+                  sw_pair_result* out);
+
+/* ---- whole-job engine ---------------------------------------------------------------------- */
+/* All blocks of one job in one call: the block driver MPIComputeLowerTriangularBlocked.Compute
+ * (Salsa.SmithWatermanMPI/Program.cs:618-642) followed by its Scatter (:645-677), which fills
+ * the mirrored half, for `ranks` = the MPI world size whose pair orientation is reproduced
+ * (checkerboard rule :628-639; ranks = 1 aligns (s_i, s_j) for every i > j).  SWG-MS mode
+ * fills every (i, j).  Work is length-binned and scheduled by a persistent kernel from a device
+ * work queue; the launch sequence is captured in a CUDA graph and replayed on later calls.
+ * d_out is a device N x N row-major Int16 matrix (leading dimension ld_out); the call is
+ * ordered on the context's stream and does not wait.  *pairs receives the number of aligned
+ * pairs and *cells the DP cells (sum of m*n). */
+int sw_all_pairs_device(sw_ctx* ctx, int32_t ranks, int16_t* d_out, int64_t ld_out,
+                        int64_t* pairs, int64_t* cells);
+/* Host-memory variant: uploads nothing new, copies the N x N result to out and waits. */
+int sw_all_pairs(sw_ctx* ctx, int32_t ranks, int16_t* out, int64_t ld_out, int64_t* pairs,
+                 int64_t* cells);
+/* Pairs whose 16-bit lanes tripped the saturation check and were rerun in 32-bit lanes by the
+ * last engine call (diagnostic). */
+int sw_last_rerun_count(const sw_ctx* ctx, int64_t* count);
+/* Waits for all work on the context's stream. */
+int sw_synchronize(sw_ctx* ctx);
+
+/* One rank's share of the job, for one process per GPU: the pairs that rank `rank` of a
+ * `world_size`-rank job aligns in MPIComputeLowerTriangularBlocked.Compute (its row block r,
+ * diagonal block lower triangle and the checkerboard half of the off-diagonal blocks,
+ * Salsa.SmithWatermanMPI/Program.cs:618-642), through the same engine as sw_all_pairs_device.
+ * Distances land at (i, j) and, for the symmetric modes, at the mirrored (j, i), so the
+ * entries of all ranks are disjoint and sum to the full matrix (the exchange Scatter and
+ * WriteFullMatrixOnRank0 do, :645-677 and :786-888).  d_out is a device N x N matrix whose
+ * entries this rank does not own are left unchanged; the call is ordered on the context's
+ * stream and does not wait. */
+int sw_compute_rank_blocks(sw_ctx* ctx, int32_t rank, int32_t world_size, int16_t* d_out,
+                           int64_t ld_out, int64_t* pairs);
+
+/* Engine knobs: "stream" (a caller's cudaStream_t as an integer, 0 = the context's own; later
+ * calls are ordered on it), "int16_threshold" (best score above which a 16-bit lane is redone in 32-bit
+ * lanes; -1 restores the value derived from the lane range), "use_graph" (0/1), "chunk"
+ * (database entries per work item), "rows_per_lane" (0 = chosen per query, else 4/8/12/16).
+ * Unknown keys are SW_E_ARG. */
+int sw_set_option(sw_ctx* ctx, const char* key, int64_t value);
+
+/* Counters of the last engine call: "launches" (kernels it enqueued), "pairs", "cells",
+ * "bins" (rows-per-lane classes used), "alphabet" (distinct residue bytes).  Unknown keys are
+ * SW_E_ARG. */
+int sw_query(sw_ctx* ctx, const char* key, int64_t* value);
+
+/* ---- host-side library (formats the reference reads and writes) --------------------------- */
+/* ScoringMatrix.Load (Salsa.CoreTPL/Bio/Algorithms/ScoringMatrix.cs:145-196) over the matrix
+ * text (header of column letters, then one "<letter> <scores...>" line per row; '#' comment
+ * lines first).  Letters absent from the header score 0.  Non-integer entries are
+ * SW_E_UNSUPPORTED. */
+int sw_parse_scoring_matrix(const char* text, int64_t text_len, int16_t out[128][128]);
+/* The matrices the reference embeds that the engine ships built in: "EDNAFULL", "BLOSUM62",
+ * "IDENTITY" and "MATCH" (the reference's Matrices/ resources of those names). */
+int sw_builtin_scoring_matrix(const char* name, int16_t out[128][128]);
+
+/* FastaSequenceParser (Salsa.CoreTPL/Bio/IO/FastaRecord.cs:112-118, Parser.cs:123-180):
+ * records start at '>', the label is the trimmed rest of that line, residue lines are trimmed,
+ * upper-cased and concatenated.  Two-phase: call with concat/offsets NULL to get the sizes. */
+int sw_parse_fasta(const char* text, int64_t text_len, uint8_t* concat, int64_t* offsets,
+                   int32_t* count, int64_t* residues);
+
+/* RangePartitioner.Partition (Salsa.CoreTPL/RangePartitioner.cs:17-55): starts/ends receive
+ * the inclusive ranges; the first length % parts ranges get one extra element. */
+int sw_partition_ranges(int32_t start, int32_t length, int32_t parts, int32_t* starts,
+                        int32_t* ends);
+
+/* The computing rank of block (r, c) under the SWG-MPI checkerboard (Program.cs:628-639):
+ * returns 1 if rank r computes it, else 0. */
+int sw_block_is_computed(int32_t r, int32_t c);
+
+/* Full matrix writer: raw row-major little-endian Int16, no header, as WriteFullMatrixOnRank0
+ * (Salsa.SmithWatermanMPI/Program.cs:786-888) and MatrixBinaryWriter.Write(Matrix<short>)
+ * (Salsa.CoreTPL/Blas/MatrixBinaryWriter.cs:73-92) produce. */
+int sw_write_full_matrix(const char* path, const int16_t* m, int64_t rows, int64_t cols,
+                         int64_t ld);
+
+/* SWG-MS block file {BlockDir}/{rank}-{cb}.bin (Salsa.SmithWatermanMS/Program.cs:1081-1160):
+ * header (u16-length-prefixed ASCII project, u16 rank, system, fasta names, u16 row/col block
+ * numbers, u32 row/col range bounds, four length-prefixed sequence IDs) then the block's Int16
+ * values row-major. */
+typedef struct {
+  const char* project;
+  const char* system;
+  const char* fasta;
+  int32_t rank;
+  int32_t row_block, col_block;
+  int32_t row_start, row_end, col_start, col_end;
+  const char* row_start_id;
+  const char* row_end_id;
+  const char* col_start_id;
+  const char* col_end_id;
+} sw_ms_block_header;
+int sw_write_ms_block(const char* path, const sw_ms_block_header* h, const int16_t* values,
+                      int64_t ld);
+/* Reads one block file back (two-phase like sw_parse_fasta for the values). */
+int sw_read_ms_block_dims(const char* path, int32_t* rank, int32_t* row_block, int32_t* col_block,
+                          int32_t* row_start, int32_t* row_end, int32_t* col_start,
+                          int32_t* col_end);
+int sw_read_ms_block_values(const char* path, int16_t* values, int64_t ld);
+
+/* ---- measurement ----------------------------------------------------------------------------- */
+/* Integer-pipe peak on this device: lane-ops per second of a 2-input integer max (the op the
+ * cell update is made of), measured by a calibration kernel.  Denominator of the roofline. */
+int sw_measure_int_peak(int32_t device, double* max_ops_per_s, double* add_ops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SWGB200_H */

@@ -88,6 +88,8 @@ def ref():
         L.ref_compute_block.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_float, C.c_float, P, P,
                                         C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P]
         L.ref_compute_block.restype = C.c_long
+        L.ref_distances.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_float, C.c_float, P, P, P, P, C.c_long, P]
+        L.ref_distances.restype = C.c_long
         L.ref_set_matrix_dir(str(HERE / "_ref" / "Matrices").encode())
         _ref = L
     return _ref
@@ -241,3 +243,20 @@ def ref_compute_block(matrix_name, alignment_type, dist_fn, o, e, seqs, offsets,
     if n < 0:
         raise RuntimeError("reference ComputeBlock raised")
     return out, n
+
+
+def ref_distances(matrix_name, alignment_type, dist_fn, o, e, seqs, offsets, rows, cols):
+    """The reference's aligner + ComputeDistance over explicit pairs (one matrix load)."""
+    L = ref()
+    if L is None:
+        raise FileNotFoundError("oracle/_ref not built")
+    sq = np.ascontiguousarray(seqs, dtype=np.uint8)
+    of = np.ascontiguousarray(offsets, dtype=np.int64)
+    r = np.ascontiguousarray(rows, dtype=np.int32)
+    c = np.ascontiguousarray(cols, dtype=np.int32)
+    out = np.zeros(len(r), dtype=np.int16)
+    n = L.ref_distances(matrix_name.encode(), alignment_type, dist_fn, o, e, sq.ctypes.data, of.ctypes.data,
+                        r.ctypes.data, c.ctypes.data, len(r), out.ctypes.data)
+    if n < 0:
+        raise RuntimeError("reference aligner raised")
+    return out

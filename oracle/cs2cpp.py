@@ -245,6 +245,27 @@ int ref_align(const char* matrix, const uint8_t* s1, int m, const uint8_t* s2, i
   } catch (...) { return -1; }
 }
 
+// The body of ComputeBlock's loop (Align, then ComputeDistance) over an explicit pair list with
+// one ScoringMatrix.Load, as one ComputeBlock call does: the timed CPU reference.
+long ref_distances(const char* matrix, int alignment_type, int dist_fn, float o, float e,
+                   const uint8_t* seqs, const int64_t* offsets, const int32_t* rows,
+                   const int32_t* cols, long npairs, int16_t* out) {
+  try {
+    _alignmentType = alignment_type ? AlignmentType::Nucleic : AlignmentType::Protein;
+    _distanceFunction = (DistanceFunctionType)dist_fn;
+    ScoringMatrix scoringMatrix = ScoringMatrix::Load(CsString(matrix));
+    SmithWatermanGotoh aligner(_alignmentType);
+    for (long k = 0; k < npairs; k++) {
+      const int i = rows[k], j = cols[k];
+      Sequence si = make_seq(seqs + offsets[i], (int)(offsets[i + 1] - offsets[i]));
+      Sequence sj = make_seq(seqs + offsets[j], (int)(offsets[j + 1] - offsets[j]));
+      PairwiseAlignment alignment = aligner.Align(si, sj, scoringMatrix, o, e);
+      out[k] = ComputeDistance(alignment);
+    }
+    return npairs;
+  } catch (...) { return -1; }
+}
+
 // Program.ComputeBlock (SWG-MPI) over one block; out is an N x N row-major Int16 matrix that
 // receives matrix[i,j] (and matrix[j,i] for diagonal blocks) at global indices.
 long ref_compute_block(const char* matrix, int alignment_type, int dist_fn, float o, float e,

@@ -1,0 +1,217 @@
+"""GPU parity through the C ABI: every distance bit-exact against the reference.
+
+Golden vectors come from the reference's own aligner and block driver (tests/golden); larger
+inputs are checked against the oracle (the CPU restatement, itself pinned to those vectors).
+Tolerance: exact Int16 equality everywhere.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_npz, unpack
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def cs():
+    from csharp_b200 import build
+    build.build()
+    import csharp_b200
+    return csharp_b200
+
+
+_engines = {}
+
+
+def engine(cs, matrix, o, e, atype=1, mode=0, lanes=0):
+    key = (matrix, o, e, atype, mode, lanes)
+    if key not in _engines:
+        _engines[key] = cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=mode, alignment_type=atype, lanes=lanes)
+    return _engines[key]
+
+
+def test_align_pair_matches_reference_kats(cs, kats):
+    for k in kats:
+        eng = engine(cs, k["matrix"], k["o"], k["e"], k["alignment_type"])
+        r = eng.align(k["s1"], k["s2"])
+        got = dict(identity=r.Identity, similarity=r.Similarity, length=r.Length, start1=r.Start1,
+                   start2=r.Start2, gaps=r.Gaps, distance=r.Distance)
+        want = {f: k[f] for f in got}
+        assert got == want, k
+        if k["score"] is None:
+            assert np.isinf(r.Score) and r.Score < 0
+        else:
+            assert r.Score == k["score"]
+
+
+def _golden_engine(cs, z, mode=0, lanes=0):
+    eng = cs.Engine(cs.ScoringMatrix.Load(z["matrix"].tobytes().decode()), float(z["o"]), float(z["e"]),
+                    mode=mode, alignment_type=int(z["alignment_type"]), lanes=lanes)
+    eng.upload(concat=z["concat"], offsets=z["offsets"])
+    return eng
+
+
+@pytest.mark.parametrize("name", ["mpi_p1.npz", "mpi_p3.npz", "mpi_p4.npz", "protein_mpi.npz", "identity_mpi.npz"])
+def test_plain_block_kernel_matches_reference_block_driver(cs, name):
+    """One drop-in call per block of the reference's driver, mirrored like Scatter."""
+    z = load_npz(name)
+    eng = _golden_engine(cs, z)
+    N, P = len(z["offsets"]) - 1, int(z["ranks"])
+    rr = cs.range_partition(N, P)
+    full = np.zeros((N, N), dtype=np.int16)
+    pairs = 0
+    for r in range(P):
+        for c in range(P):
+            if not (r == c or cs.block_is_computed(r, c)):
+                continue
+            a, b = rr[r], rr[c]
+            blk, n = eng.compute_block(a.StartIndex, a.EndIndex, b.StartIndex, b.EndIndex, r == c)
+            pairs += n
+            full[a.StartIndex:a.EndIndex + 1, b.StartIndex:b.EndIndex + 1] = blk
+            if r != c:
+                full[b.StartIndex:b.EndIndex + 1, a.StartIndex:a.EndIndex + 1] = blk.T
+    assert pairs == int(z["pairs"])
+    np.testing.assert_array_equal(full, z["distances"])
+
+
+@pytest.mark.parametrize("name", ["mpi_p1.npz", "mpi_p3.npz", "mpi_p4.npz", "protein_mpi.npz", "identity_mpi.npz"])
+@pytest.mark.parametrize("lanes", [0, 32])
+def test_engine_matches_reference_driver(cs, name, lanes):
+    z = load_npz(name)
+    eng = _golden_engine(cs, z, lanes=lanes)
+    full, pairs, cells = eng.all_pairs(int(z["ranks"]))
+    assert pairs == int(z["pairs"])
+    np.testing.assert_array_equal(full, z["distances"])
+
+
+def test_block_handler_leaves_unaligned_entries_alone(cs):
+    z = load_npz("mpi_p1.npz")
+    eng = _golden_engine(cs, z)
+    out = np.full((10, 10), 1234, dtype=np.int16)
+    eng.compute_block(3, 12, 3, 12, True, out=out)
+    assert (np.diag(out) == 1234).all()
+    np.testing.assert_array_equal(out[~np.eye(10, dtype=bool)], z["distances"][3:13, 3:13][~np.eye(10, dtype=bool)])
+
+
+@pytest.mark.parametrize("name,mode", [("nw_restated.npz", 2), ("ms_restated.npz", 1),
+                                       ("ms_protein_restated.npz", 1), ("nw_protein_restated.npz", 2)])
+def test_nw_and_ms_modes_match_restatement(cs, name, mode):
+    z = load_npz(name)
+    eng = _golden_engine(cs, z, mode=mode)
+    full, _, _ = eng.all_pairs(1)
+    want = z["distances"].copy()
+    if mode == 2:
+        np.fill_diagonal(want, 0)
+    np.testing.assert_array_equal(full, want)
+    N = len(z["offsets"]) - 1
+    blk, n = eng.compute_block(0, N - 1, 0, N - 1, True)
+    if mode == 1:
+        np.testing.assert_array_equal(blk, z["distances"])
+    else:
+        off = ~np.eye(N, dtype=bool)
+        np.testing.assert_array_equal(blk[off], want[off])
+
+
+def _oracle_distances(oracle, seqs, pairs, matrix, o, e, atype=1):
+    from csharp_b200 import ScoringMatrix, pack_sequences
+    sc = ScoringMatrix.Load(matrix).Scores[:127, :127].astype(np.float32)
+    concat, off = pack_sequences(seqs)
+    return oracle.pairs(concat, off, pairs[:, 0], pairs[:, 1], sc, o, e, atype)
+
+
+def test_engine_long_and_uneven_sequences_against_oracle(cs, oracle_mod):
+    """Multi-pass queries (up to 2600 rows), empty and 1-residue sequences, every K bin."""
+    from csharp_b200 import synth
+    rng = np.random.default_rng(123)
+    lens = np.concatenate([rng.integers(1, 120, 40), rng.integers(400, 700, 20), rng.integers(1400, 2600, 8), [1, 2, 3]])
+    seqs = [s.tobytes() for s in synth.dna_family(len(lens), 5, lens, seed=77)] + [b"", b"G"]
+    eng = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4).upload(seqs)
+    full, pairs, _ = eng.all_pairs(1)
+    N = len(seqs)
+    ii, jj = np.tril_indices(N, -1)
+    sel = rng.choice(len(ii), min(len(ii), 2500), replace=False)
+    pr = np.stack([ii[sel], jj[sel]], 1)
+    want = _oracle_distances(oracle_mod, seqs, pr, "EDNAFULL", 16, 4)
+    np.testing.assert_array_equal(full[pr[:, 0], pr[:, 1]], want)
+    np.testing.assert_array_equal(full[pr[:, 1], pr[:, 0]], want)
+    assert pairs == N * (N - 1) // 2
+    # the drop-in block kernel agrees on the same pairs
+    blk, _ = eng.compute_block(0, N - 1, 0, N - 1, True)
+    off = ~np.eye(N, dtype=bool)
+    np.testing.assert_array_equal(blk[off], full[off])
+
+
+@pytest.mark.parametrize("opt", [("rows_per_lane", 4), ("rows_per_lane", 8), ("rows_per_lane", 12),
+                                 ("rows_per_lane", 16), ("chunk", 32), ("chunk", 1024), ("use_graph", 0)])
+def test_engine_options_do_not_change_results(cs, opt):
+    from csharp_b200 import synth
+    rng = np.random.default_rng(5)
+    lens = np.concatenate([rng.integers(20, 700, 120), [0, 1, 1500]])
+    seqs = [s.tobytes() for s in synth.dna_family(len(lens), 6, lens, seed=9)]
+    base = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4).upload(seqs)
+    want, _, _ = base.all_pairs(1)
+    eng = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4).upload(seqs)
+    eng.set_option(*opt)
+    got, _, _ = eng.all_pairs(1)
+    np.testing.assert_array_equal(got, want)
+    got2, _, _ = eng.all_pairs(1)  # replay
+    np.testing.assert_array_equal(got2, want)
+
+
+def test_tripped_16bit_lanes_rerun_in_32bit(cs):
+    """Force the trip level below the scores reached: every tripped pair is redone with 32-bit
+    lanes and the matrix is unchanged."""
+    z = load_npz("mpi_p1.npz")
+    eng = _golden_engine(cs, z)
+    eng.set_option("int16_threshold", 40)
+    full, _, _ = eng.all_pairs(1)
+    assert eng.rerun_count() > 0
+    np.testing.assert_array_equal(full, z["distances"])
+
+
+def test_int16_static_guard_routes_high_scoring_pairs(cs, oracle_mod):
+    """A matrix whose scores cannot stay in 16-bit lanes for long pairs goes to 32-bit lanes."""
+    txt = "   A C G T\nA 300 -100 -100 -100\nC -100 300 -100 -100\nG -100 -100 300 -100\nT -100 -100 -100 300\n"
+    m = cs.ScoringMatrix.Parse(txt, "HIGH")
+    from csharp_b200 import synth
+    lens = np.array([150, 160, 170, 40, 50, 300])
+    seqs = [s.tobytes() for s in synth.dna_family(6, 1, lens, seed=3, sub_range=(0.01, 0.02), indel_range=(0.0, 0.01))]
+    eng = cs.Engine(m, 16, 4).upload(seqs)
+    full, _, _ = eng.all_pairs(1)
+    assert eng.rerun_count() > 0
+    sc = m.Scores[:127, :127].astype(np.float32)
+    for i in range(6):
+        for j in range(i):
+            a = oracle_mod.align(seqs[i], seqs[j], sc, 16, 4)
+            assert full[i, j] == oracle_mod.distance_i16(a), (i, j)
+
+
+def test_rank_blocks_partition_the_job(cs):
+    import torch
+    z = load_npz("mpi_p4.npz")
+    eng = _golden_engine(cs, z)
+    N = len(z["offsets"]) - 1
+    total = torch.zeros((N, N), dtype=torch.int16, device="cuda")
+    npairs = 0
+    for r in range(4):
+        part = torch.zeros((N, N), dtype=torch.int16, device="cuda")
+        npairs += eng.rank_blocks_device(r, 4, part.data_ptr(), N)
+        eng.synchronize()
+        assert not ((total != 0) & (part != 0)).any()
+        total += part
+    assert npairs == int(z["pairs"])
+    np.testing.assert_array_equal(total.cpu().numpy(), z["distances"])
+
+
+def test_sequence_validation(cs):
+    from csharp_b200.lib import SwError
+    eng = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4)
+    with pytest.raises(SwError):
+        eng.upload([b"ACGT", bytes([200, 65])])  # byte outside the 127-entry table
+    with pytest.raises(SwError):
+        eng.compute_block(0, 1, 0, 1, True)  # nothing uploaded
+    eng.upload([b"ACGT", b"ACG"])
+    with pytest.raises(SwError):
+        eng.compute_block(0, 5, 0, 1, False)  # block outside the set
+    with pytest.raises(SwError):
+        eng.compute_block(0, 1, 1, 1, True)  # diagonal block must be square
