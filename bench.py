@@ -196,7 +196,8 @@ def main():
     N = a.n
     eng = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4, device=local)
     eng.upload(concat=concat, offsets=off)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # a real stream handle (the legacy default stream's is 0)
+    torch.cuda.set_stream(stream)
     eng.use_stream(stream.cuda_stream)
     out = torch.zeros((N, N), dtype=torch.int16, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2

@@ -421,7 +421,9 @@ int sw_query(sw_ctx* ctx, const char* key, int64_t* value) {
     *value = (k == "pairs") ? ctx->last_pairs : ctx->last_cells;
     return SW_OK;
   }
-  if (k != "launches" && k != "bins" && k != "alphabet") return fail(ctx, SW_E_ARG, "unknown counter " + k);
+  if (k != "launches" && k != "bins" && k != "alphabet" && k != "items" && k != "lane16_pairs" &&
+      k != "tripped" && k != "planned_items")
+    return fail(ctx, SW_E_ARG, "unknown counter " + k);
   *value = ctx->engine ? ctx->engine->stat(key) : 0;
   return SW_OK;
 }

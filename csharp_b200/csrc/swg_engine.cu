@@ -61,6 +61,7 @@ struct EngineJob {
   int* rerun_count;
   int rerun_cap;
   int mpad;                 // profile rows staged (passes * 32 * K of the bin)
+  unsigned long long* stats; // [0] items taken, [1] pairs finished in 16-bit lanes, [2] tripped
 };
 
 // Rank owning a global row index under RangePartitioner (Program.cs:791-802).
@@ -77,8 +78,29 @@ __device__ __forceinline__ bool oriented(const EngineJob& J, int q, int d) {
   return (bq > bd && !odd) || (bq < bd && odd);
 }
 
+// Per-halfword signed max of a and b, with hi/lo = (a >= b) for the high/low halves.  The halves
+// of a and b are compared directly (not the max against a), and the result register is
+// early-clobbered, so the predicates stay right when the result overwrites an operand
+// (BEST = max(BEST, V)): a formulation that compares the max against a register that may share
+// storage with it reports "a won" for every lane in that case.
 __device__ __forceinline__ uint32_t vmax2(uint32_t a, uint32_t b, bool& hi, bool& lo) {
-  return __vibmax_s16x2(a, b, &hi, &lo);
+  uint32_t r, ph, pl;
+  asm("{\n\t"
+      ".reg .pred pa, pb;\n\t"
+      ".reg .s16 a0, a1, b0, b1;\n\t"
+      "mov.b32 {a0, a1}, %3;\n\t"
+      "mov.b32 {b0, b1}, %4;\n\t"
+      "setp.ge.s16 pa, a0, b0;\n\t"
+      "setp.ge.s16 pb, a1, b1;\n\t"
+      "max.s16x2 %0, %3, %4;\n\t"
+      "selp.u32 %2, 1, 0, pa;\n\t"
+      "selp.u32 %1, 1, 0, pb;\n\t"
+      "}"
+      : "=&r"(r), "=&r"(ph), "=&r"(pl)
+      : "r"(a), "r"(b));
+  hi = ph != 0u;
+  lo = pl != 0u;
+  return r;
 }
 
 // One warp, query rows in registers, two database sequences (lanes A/B) in lockstep.
@@ -248,6 +270,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineJob J) {
     if (it >= J.nitems) break;
     const int4 item = J.items[it];
     const int q = item.x, c0 = item.y, c1 = item.z, passes = item.w;
+    if (threadIdx.x == 0) atomicAdd(J.stats, 1ull);
     const int m = (int)(J.off[q + 1] - J.off[q]);
     const int mrows = passes * 32 * K;
     // query profile (rows beyond m and the pad column score -bias, count nothing)
@@ -318,6 +341,9 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineJob J) {
       warp_best(bA, rA, cA);
       warp_best(bB, rB, cB);
       if (lane == 0) {
+        const unsigned long long tripped = (bA > J.thresh && m > 0 && nA > 0) + (dB >= 0 && bB > J.thresh && m > 0 && nB > 0);
+        atomicAdd(J.stats + 1, (unsigned long long)(1 + (dB >= 0)) - tripped);
+        if (tripped) atomicAdd(J.stats + 2, tripped);
         // a lane whose best reached the trip level is redone with 32-bit lanes
         if (bA > J.thresh && m > 0 && nA > 0) {
           const int w = atomicAdd(J.rerun_count, 1);
@@ -467,13 +493,14 @@ struct Plan {
   int* d_counters = nullptr;
   int2* d_rerun = nullptr;
   int* d_rerun_count = nullptr;
+  unsigned long long* d_stats = nullptr;
   cudaGraphExec_t graph = nullptr;
   int16_t* graph_out = nullptr;
   long long graph_ld = 0;
   cudaStream_t graph_stream = nullptr;
   ~Plan() {
     if (graph) cudaGraphExecDestroy(graph);
-    cudaFree(d_items); cudaFree(d_counters); cudaFree(d_rerun); cudaFree(d_rerun_count);
+    cudaFree(d_items); cudaFree(d_counters); cudaFree(d_rerun); cudaFree(d_rerun_count); cudaFree(d_stats);
   }
 };
 
@@ -523,6 +550,18 @@ class EngineImpl : public Engine {
       return n;
     }
     if (k == "alphabet") return base_ ? base_->alpha : 0;
+    if (k == "items" || k == "lane16_pairs" || k == "tripped") {
+      if (!last_->d_stats) return 0;
+      unsigned long long h[4] = {0, 0, 0, 0};
+      cudaDeviceSynchronize();
+      cudaMemcpy(h, last_->d_stats, sizeof(h), cudaMemcpyDeviceToHost);
+      return (int64_t)(k == "items" ? h[0] : (k == "lane16_pairs" ? h[1] : h[2]));
+    }
+    if (k == "planned_items") {
+      int64_t n = 0;
+      for (auto& bn : last_->bins) n += (int64_t)bn.items.size();
+      return n;
+    }
     return -1;
   }
 
@@ -742,6 +781,8 @@ class EngineImpl : public Engine {
       for (size_t k : ord) all.push_back(bn.items[k]);
     }
     if ((rc = upload_vec(&pl.d_items, all, msg, "items"))) return rc;
+    std::vector<unsigned long long> st0(4, 0ull);
+    if ((rc = upload_vec(&pl.d_stats, st0, msg, "stats"))) return rc;
     std::vector<int> zeros(pl.bins.size() + 1, 0);
     if ((rc = upload_vec(&pl.d_counters, zeros, msg, "counters"))) return rc;
     int max_slots = 0;
@@ -782,6 +823,7 @@ class EngineImpl : public Engine {
     set_int_kernel<<<1, 1, 0, P.stream>>>(pl.d_rerun_count, pl.big_count);
     if (!pl.plain_only) {
       if ((e = cudaMemsetAsync(pl.d_counters, 0, sizeof(int) * (pl.bins.size() + 1), P.stream)) != cudaSuccess) return e;
+      if ((e = cudaMemsetAsync(pl.d_stats, 0, sizeof(unsigned long long) * 4, P.stream)) != cudaSuccess) return e;
       EngineJob J;
       std::memset(&J, 0, sizeof(J));
       J.code = B.d_code; J.off = P.off; J.sorted = B.d_sorted;
@@ -792,6 +834,7 @@ class EngineImpl : public Engine {
       J.out = P.out; J.ld = P.ld;
       J.scratch = B.d_scratch; J.maxcol = B.maxcol;
       J.rerun = pl.d_rerun; J.rerun_count = pl.d_rerun_count; J.rerun_cap = pl.rerun_cap;
+      J.stats = pl.d_stats;
       for (size_t b = 0; b < pl.bins.size(); b++) {
         const Bin& bn = pl.bins[b];
         if (bn.items.empty()) continue;

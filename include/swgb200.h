@@ -163,7 +163,9 @@ int sw_compute_rank_blocks(sw_ctx* ctx, int32_t rank, int32_t world_size, int16_
 int sw_set_option(sw_ctx* ctx, const char* key, int64_t value);
 
 /* Counters of the last engine call: "launches" (kernels it enqueued), "pairs", "cells",
- * "bins" (rows-per-lane classes used), "alphabet" (distinct residue bytes).  Unknown keys are
+ * "bins" (rows-per-lane classes used), "alphabet" (distinct residue bytes), "planned_items",
+ * and, after waiting for the device, "items" (work items taken), "lane16_pairs" (pairs finished
+ * in 16-bit lanes) and "tripped" (16-bit lanes handed to 32-bit lanes).  Unknown keys are
  * SW_E_ARG. */
 int sw_query(sw_ctx* ctx, const char* key, int64_t* value);
 

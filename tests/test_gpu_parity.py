@@ -215,3 +215,27 @@ def test_sequence_validation(cs):
         eng.compute_block(0, 5, 0, 1, False)  # block outside the set
     with pytest.raises(SwError):
         eng.compute_block(0, 1, 1, 1, True)  # diagonal block must be square
+
+
+def test_running_best_keeps_the_first_maximum_cell(cs):
+    """The running best overwrites its own operand (BEST = max(BEST, V)); its 'keep' decision
+    must still see the old value, or every pair reports the counters of the wrong cell."""
+    eng = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4)
+    # pairs whose best local alignment is long and partial: distance well inside (0, 32767)
+    seqs = [b"ACGTACGTTTGCAACGTAGGCTA" * 3, b"TTACGTACGTTTGCAACGAAGGCTATT" * 2, b"GGGGACGTACGATTGCAACG"]
+    eng.upload(seqs)
+    full, _, _ = eng.all_pairs(1)
+    for i in range(3):
+        for j in range(i):
+            r = eng.align(seqs[i], seqs[j])
+            assert full[i, j] == r.Distance and 0 < r.Distance < 32767, (i, j, full[i, j], r)
+
+
+def test_engine_accounts_for_every_pair(cs):
+    from csharp_b200 import synth
+    rng = np.random.default_rng(8)
+    seqs = [s.tobytes() for s in synth.dna_family(90, 4, rng.integers(30, 900, 90), seed=21)]
+    eng = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4).upload(seqs)
+    _, pairs, _ = eng.all_pairs(1)
+    assert eng.query("items") == eng.query("planned_items") > 0
+    assert eng.query("lane16_pairs") + eng.rerun_count() == pairs
