@@ -206,10 +206,11 @@ def main():
         return (step * world + rank) % SHARES
 
     share_cells = {}
-    for s in range(SHARES):  # plan every share once (host) before timing
+    eng.set_option("plan_only", 1)  # plan and capture every share before timing; launch nothing
+    for s in range(SHARES):
         eng.rank_blocks_device(s, SHARES, out.data_ptr(), N)
         share_cells[s] = eng.query("cells")
-    launches_per_step = eng.query("launches")
+    eng.set_option("plan_only", 0)
     torch.cuda.synchronize()
 
     for w in range(a.warmup):

@@ -441,6 +441,10 @@ int sw_set_option(sw_ctx* ctx, const char* key, int64_t value) {
     ctx->stream = value ? reinterpret_cast<cudaStream_t>(value) : ctx->own_stream;
     return SW_OK;
   }
+  if (k == "plan_only") {
+    ctx->engine->set_plan_only(value ? 1 : 0);
+    return SW_OK;
+  }
   swg::EngineOptions& o = ctx->engine->options();
   if (k == "int16_threshold") o.int16_threshold = value;
   else if (k == "use_graph") o.use_graph = value ? 1 : 0;

@@ -535,6 +535,7 @@ class EngineImpl : public Engine {
     last_ = nullptr;
     return opt_;
   }
+  void set_plan_only(int v) override { opt_.plan_only = v; }
 
   int64_t stat(const char* key) const override {
     const std::string k(key);
@@ -614,9 +615,9 @@ class EngineImpl : public Engine {
         if (e != cudaSuccess) { pl.graph = nullptr; *msg = "graph instantiate"; return SW_E_CUDA; }
         pl.graph_out = P.out; pl.graph_ld = P.ld; pl.graph_stream = P.stream;
       }
-      e = cudaGraphLaunch(pl.graph, P.stream);
+      e = opt_.plan_only ? cudaSuccess : cudaGraphLaunch(pl.graph, P.stream);
     } else {
-      e = enqueue(P, key, pl);
+      e = opt_.plan_only ? cudaSuccess : enqueue(P, key, pl);
     }
     if (e != cudaSuccess) { *msg = std::string("engine launch: ") + cudaGetErrorString(e); return SW_E_CUDA; }
     *reruns = -1;  // known once the stream is done (rerun_count)

@@ -32,6 +32,7 @@ struct EngineOptions {
   int use_graph = 1;
   int chunk = 512;                 // database entries per work item
   int k_override = 0;              // 0: per-query choice; else rows per lane
+  int plan_only = 0;               // build plans and graphs, launch nothing
 };
 
 class Engine {
@@ -40,6 +41,7 @@ class Engine {
   virtual ~Engine() {}
   virtual void invalidate() = 0;
   virtual EngineOptions& options() = 0;
+  virtual void set_plan_only(int v) = 0;  // keeps the plans (options() drops them)
   // Returns an SW_* status.
   virtual int run(const EngineParams& p, int64_t* pairs, int64_t* cells, int64_t* reruns,
                   std::string* msg) = 0;
