@@ -170,6 +170,26 @@ int sw_set_option(sw_ctx* ctx, const char* key, int64_t value);
  * SW_E_ARG. */
 int sw_query(sw_ctx* ctx, const char* key, int64_t* value);
 
+/* ---- block handler without device allocation ------------------------------------------------ */
+/* No counterpart in the reference: this entry point serves callers that cannot allocate device
+ * memory (a host that gives all GPU memory to its own pool allocator, code running while a CUDA
+ * graph is captured, a plug-in with a fixed memory budget).  It aligns the pairs of one block like
+ * sw_compute_block_device, with the same ranges, modes, orientation and mirror rule, but needs
+ * no context: the configuration comes in cfg, the residues and offsets (sw_upload_sequences'
+ * layout) and the output are the caller's device buffers, and the work is ordered on `stream`
+ * (a cudaStream_t, NULL = the legacy default stream).  It calls no cudaMalloc or cudaFree: the
+ * kernel's scratch is a 64 MiB array in the library's device image, present on every GPU that
+ * loads the library until the process exits.  Sequences up to 16,383 residues.  The first call
+ * on a device looks up that array's address with the device current; make that first call before
+ * any stream capture.  Calls share the array: calls whose kernels overlap on the GPU race and
+ * must be ordered by the caller.  The call waits for its input checks (small copies of the
+ * block's offsets and residues) and does not wait for the kernel. */
+int sw_compute_block_static(const sw_config* cfg, const uint8_t* d_residues,
+                            const int64_t* d_offsets, int32_t count, int32_t row_start,
+                            int32_t row_end, int32_t col_start, int32_t col_end,
+                            int32_t is_diagonal, int16_t* d_out, int64_t ld_out,
+                            int64_t* pairs_computed, void* stream);
+
 /* ---- host-side library (formats the reference reads and writes) --------------------------- */
 /* ScoringMatrix.Load (Salsa.CoreTPL/Bio/Algorithms/ScoringMatrix.cs:145-196) over the matrix
  * text (header of column letters, then one "<letter> <scores...>" line per row; '#' comment
