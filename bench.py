@@ -177,6 +177,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-step-seconds", type=float, default=6.0)
     ap.add_argument("--skip-extras", action="store_true", help="headline only (profiling runs)")
+    ap.add_argument("--rows-per-lane", type=int, default=0, help="engine rows per lane (0 = per query)")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference_arm(a)
@@ -196,6 +197,8 @@ def main():
     N = a.n
     eng = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4, device=local)
     eng.upload(concat=concat, offsets=off)
+    if a.rows_per_lane:
+        eng.set_option("rows_per_lane", a.rows_per_lane)
     stream = torch.cuda.Stream()  # a real stream handle (the legacy default stream's is 0)
     torch.cuda.set_stream(stream)
     eng.use_stream(stream.cuda_stream)

@@ -78,25 +78,24 @@ __device__ __forceinline__ bool oriented(const EngineJob& J, int q, int d) {
   return (bq > bd && !odd) || (bq < bd && odd);
 }
 
-// Per-halfword signed max of a and b, with hi/lo = (a >= b) for the high/low halves.  The halves
-// of a and b are compared directly (not the max against a), and the result register is
-// early-clobbered, so the predicates stay right when the result overwrites an operand
-// (BEST = max(BEST, V)): a formulation that compares the max against a register that may share
-// storage with it reports "a won" for every lane in that case.
+// Per-halfword signed max of a and b, with hi/lo = (a >= b) for the high/low halves, i.e. "the
+// max of that half is a's".  The result register is early-clobbered: it must never share a
+// register with a, or the comparison below would see the max in place of a and report "a won"
+// for every half -- which happens exactly when the result overwrites a (BEST = max(BEST, V)).
 __device__ __forceinline__ uint32_t vmax2(uint32_t a, uint32_t b, bool& hi, bool& lo) {
   uint32_t r, ph, pl;
   asm("{\n\t"
-      ".reg .pred pa, pb;\n\t"
-      ".reg .s16 a0, a1, b0, b1;\n\t"
-      "mov.b32 {a0, a1}, %3;\n\t"
-      "mov.b32 {b0, b1}, %4;\n\t"
-      "setp.ge.s16 pa, a0, b0;\n\t"
-      "setp.ge.s16 pb, a1, b1;\n\t"
+      ".reg .pred p0, p1;\n\t"
+      ".reg .s16 m0, m1, a0, a1;\n\t"
       "max.s16x2 %0, %3, %4;\n\t"
-      "selp.u32 %2, 1, 0, pa;\n\t"
-      "selp.u32 %1, 1, 0, pb;\n\t"
+      "mov.b32 {m0, m1}, %0;\n\t"
+      "mov.b32 {a0, a1}, %3;\n\t"
+      "setp.eq.s16 p0, m0, a0;\n\t"
+      "setp.eq.s16 p1, m1, a1;\n\t"
+      "selp.u32 %2, 1, 0, p0;\n\t"
+      "selp.u32 %1, 1, 0, p1;\n\t"
       "}"
-      : "=&r"(r), "=&r"(ph), "=&r"(pl)
+      : "=&r"(r), "=r"(ph), "=r"(pl)
       : "r"(a), "r"(b));
   hi = ph != 0u;
   lo = pl != 0u;
