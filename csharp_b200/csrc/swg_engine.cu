@@ -248,7 +248,7 @@ __device__ __forceinline__ void emit(const EngineJob& J, int q, int d, int16_t d
 }
 
 template <int K>
-__global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineJob J) {
+__global__ void __launch_bounds__(kEngThreads, (K <= 8) ? 2 : 1) engine_kernel(EngineJob J) {
   extern __shared__ __align__(16) uint8_t smem[];
   uint32_t* prof = reinterpret_cast<uint32_t*>(smem);
   const int A1 = J.A + 1;
@@ -430,8 +430,12 @@ void choose_k(int m, int kov, int* K, int* passes) {
   long best = -1;
   for (int k : kKs) {
     const int p = std::max(1, (m + 32 * k - 1) / (32 * k));
-    // padded rows first (the wavefront fill is proportional to them too), then fewer passes
-    const long cost = (long)p * 32 * k * 1000 + p;
+    // rows computed (padding included) times the per-row cost of that K, measured on B200 for
+    // the uneven 3,000-sequence job with K forced: 4 rows per lane cost 1.55x a row at 8-16
+    // (too few rows to amortise the per-step shuffles, loads and column bookkeeping); ties go to
+    // fewer passes (each pass adds a wavefront fill and a scratch round trip)
+    const long weight = (k == 4) ? 155 : 100;
+    const long cost = (long)p * 32 * k * weight * 16 + p;
     if (best < 0 || cost < best) { best = cost; *K = k; *passes = p; }
   }
 }
