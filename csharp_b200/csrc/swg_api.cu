@@ -452,7 +452,7 @@ int sw_set_option(sw_ctx* ctx, const char* key, int64_t value) {
     if (value < 32 || value > 1024) return fail(ctx, SW_E_ARG, "chunk must be in [32, 1024]");
     o.chunk = (int)value;
   } else if (k == "rows_per_lane") {
-    if (value != 0 && value != 4 && value != 8 && value != 12 && value != 16) return fail(ctx, SW_E_ARG, "rows_per_lane must be 0, 4, 8, 12 or 16");
+    if (value != 0 && (value < 4 || value > 16 || (value & 1))) return fail(ctx, SW_E_ARG, "rows_per_lane must be 0 or an even number from 4 to 16");
     o.k_override = (int)value;
   } else return fail(ctx, SW_E_ARG, "unknown option " + k);
   return SW_OK;

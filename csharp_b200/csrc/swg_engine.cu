@@ -28,6 +28,7 @@
 #include <cstdio>
 #include <cstring>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/swgb200.h"
@@ -37,8 +38,13 @@
 
 namespace swg {
 
-constexpr int kEngWarps = 8;
-constexpr int kEngThreads = kEngWarps * 32;
+// Warps per CTA and CTAs per SM for K rows per lane, from the registers a lane needs (65,536 per
+// SM): up to 8 rows fit 128 registers (2 CTAs of 8 warps), 10-12 rows fit 168 (1 CTA of 12
+// warps), 14-16 rows need up to 255 (1 CTA of 8 warps).  Measured on B200, 12 warps run the
+// 10- and 12-row kernels 16% faster than 8.
+constexpr int kMaxWarps = 12;
+__host__ __device__ constexpr int warps_of(int K) { return K <= 8 ? 8 : K <= 12 ? 12 : 8; }
+__host__ __device__ constexpr int ctas_of(int K) { return K <= 8 ? 2 : 1; }
 constexpr int kMaxChunk = 1024;
 constexpr int kScrWords = 8;  // words of carried state per column in the pass scratch
 
@@ -135,6 +141,10 @@ __device__ __forceinline__ void align_two(const uint32_t* __restrict__ prof, int
     const int pbase = p * 32 * K;
     const uint32_t* pl = prof + pbase + lane * 4;
     const int nsteps = ncols + 31;
+    // 14-16 rows per lane: the next column's residue codes are loaded one step ahead (the
+    // 168-register kernels at 10-12 rows lose more to the extra registers than they gain)
+    constexpr bool kPrefetch = K >= 14;
+    int nxa = kPrefetch ? ca[32 - lane] : 0, nxb = kPrefetch ? cb[32 - lane] : 0;
     for (int s = 0; s < nsteps; s++) {
       // bottom row of this lane after the previous step, sent down one lane
       const uint32_t bVO = __shfl_up_sync(0xffffffffu, uVO, 1);
@@ -159,55 +169,71 @@ __device__ __forceinline__ void align_two(const uint32_t* __restrict__ prof, int
       uint32_t VOD = dVO, cdA = dcA, cdB = dcB;
       dVO = VOU; dcA = cvuA; dcB = cvuB;
       const int col = 32 + s - lane;  // index into the code buffers (pad before column 0)
-      const int xa = ca[col], xb = cb[col];
+      int xa, xb;
+      if (kPrefetch) {
+        xa = nxa; xb = nxb;
+        nxa = ca[col + 1]; nxb = cb[col + 1];  // col + 1 <= ncols + 63: inside the pad
+      } else {
+        xa = ca[col]; xb = cb[col];
+      }
       const uint32_t* pla = pl + xa * plane;
       const uint32_t* phb = pl + xb * plane + mpad;
       const uint32_t* pma = pl + xa * plane + 2 * mpad;
       const uint32_t* pmb = pl + xb * plane + 2 * mpad;
+      // one row of the lane's block: the cell (row r, column col) of both pairs
+      auto cell = [&](const int r, const uint32_t pl_r, const uint32_t ph_r, const uint32_t ma_r,
+                      const uint32_t mb_r) {
+        const uint32_t F = VOD + pl_r + ph_r;
+        const uint32_t cfA = cdA + ma_r + 0x10000u;
+        const uint32_t cfB = cdB + mb_r + 0x10000u;
+        bool hiB, loA;
+        // vertical gap: reopen from V above unless extending is strictly better
+        const uint32_t G = vmax2(VOU, GU - E2, hiB, loA);
+        const uint32_t cgA = (loA ? cvuA : cguA) + 0x10000u;
+        const uint32_t cgB = (hiB ? cvuB : cguB) + 0x10000u;
+        // horizontal gap
+        H[r] = vmax2(VOL[r], H[r] - E2, hiB, loA);
+        chA[r] = (loA ? clA[r] : chA[r]) + 0x10000u;
+        chB[r] = (hiB ? clB[r] : chB[r]) + 0x10000u;
+        // V = max(F, G, H, 0) with STOP > DIAGONAL > UP > LEFT on ties
+        const uint32_t GHv = vmax2(G, H[r], hiB, loA);
+        const uint32_t cghA = loA ? cgA : chA[r];
+        const uint32_t cghB = hiB ? cgB : chB[r];
+        const uint32_t FGH = vmax2(F, GHv, hiB, loA);
+        const uint32_t cfgA = loA ? cfA : cghA;
+        const uint32_t cfgB = hiB ? cfB : cghB;
+        const uint32_t V = vmax2(bias2, FGH, hiB, loA);
+        const uint32_t cvA = loA ? 0u : cfgA;
+        const uint32_t cvB = hiB ? 0u : cfgB;
+        // first strictly greater V of this row (columns ascend within a lane)
+        BEST[r] = vmax2(BEST[r], V, hiB, loA);
+        bcA[r] = loA ? bcA[r] : cvA;
+        bcB[r] = hiB ? bcB[r] : cvB;
+        const uint32_t VO = V - O2;
+        VOD = VOL[r]; cdA = clA[r]; cdB = clB[r];
+        VOL[r] = VO; clA[r] = cvA; clB[r] = cvB;
+        VOU = VO; GU = G; cvuA = cvA; cvuB = cvB; cguA = cgA; cguB = cgB;
+      };
 #pragma unroll
       for (int g = 0; g < K / 4; g++) {
         const uint4 PL = *reinterpret_cast<const uint4*>(pla + g * 128);
         const uint4 PH = *reinterpret_cast<const uint4*>(phb + g * 128);
         const uint4 MA = *reinterpret_cast<const uint4*>(pma + g * 128);
         const uint4 MB = *reinterpret_cast<const uint4*>(pmb + g * 128);
-        const uint32_t pl4[4] = {PL.x, PL.y, PL.z, PL.w};
-        const uint32_t ph4[4] = {PH.x, PH.y, PH.z, PH.w};
-        const uint32_t ma4[4] = {MA.x, MA.y, MA.z, MA.w};
-        const uint32_t mb4[4] = {MB.x, MB.y, MB.z, MB.w};
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          const int r = g * 4 + k;
-          const uint32_t F = VOD + pl4[k] + ph4[k];
-          const uint32_t cfA = cdA + ma4[k] + 0x10000u;
-          const uint32_t cfB = cdB + mb4[k] + 0x10000u;
-          bool hiB, loA;
-          // vertical gap: reopen from V above unless extending is strictly better
-          const uint32_t G = vmax2(VOU, GU - E2, hiB, loA);
-          const uint32_t cgA = (loA ? cvuA : cguA) + 0x10000u;
-          const uint32_t cgB = (hiB ? cvuB : cguB) + 0x10000u;
-          // horizontal gap
-          H[r] = vmax2(VOL[r], H[r] - E2, hiB, loA);
-          chA[r] = (loA ? clA[r] : chA[r]) + 0x10000u;
-          chB[r] = (hiB ? clB[r] : chB[r]) + 0x10000u;
-          // V = max(F, G, H, 0) with STOP > DIAGONAL > UP > LEFT on ties
-          const uint32_t GHv = vmax2(G, H[r], hiB, loA);
-          const uint32_t cghA = loA ? cgA : chA[r];
-          const uint32_t cghB = hiB ? cgB : chB[r];
-          const uint32_t FGH = vmax2(F, GHv, hiB, loA);
-          const uint32_t cfgA = loA ? cfA : cghA;
-          const uint32_t cfgB = hiB ? cfB : cghB;
-          const uint32_t V = vmax2(bias2, FGH, hiB, loA);
-          const uint32_t cvA = loA ? 0u : cfgA;
-          const uint32_t cvB = hiB ? 0u : cfgB;
-          // first strictly greater V of this row (columns ascend within a lane)
-          BEST[r] = vmax2(BEST[r], V, hiB, loA);
-          bcA[r] = loA ? bcA[r] : cvA;
-          bcB[r] = hiB ? bcB[r] : cvB;
-          const uint32_t VO = V - O2;
-          VOD = VOL[r]; cdA = clA[r]; cdB = clB[r];
-          VOL[r] = VO; clA[r] = cvA; clB[r] = cvB;
-          VOU = VO; GU = G; cvuA = cvA; cvuB = cvB; cguA = cgA; cguB = cgB;
-        }
+        cell(g * 4 + 0, PL.x, PH.x, MA.x, MB.x);
+        cell(g * 4 + 1, PL.y, PH.y, MA.y, MB.y);
+        cell(g * 4 + 2, PL.z, PH.z, MA.z, MB.z);
+        cell(g * 4 + 3, PL.w, PH.w, MA.w, MB.w);
+      }
+      if (K % 4 == 2) {
+        // the last two rows of each lane sit after the groups of four, two words per lane
+        const int t2 = (K / 4) * 128 - lane * 2;
+        const uint2 PL = *reinterpret_cast<const uint2*>(pla + t2);
+        const uint2 PH = *reinterpret_cast<const uint2*>(phb + t2);
+        const uint2 MA = *reinterpret_cast<const uint2*>(pma + t2);
+        const uint2 MB = *reinterpret_cast<const uint2*>(pmb + t2);
+        cell(K - 2, PL.x, PH.x, MA.x, MB.x);
+        cell(K - 1, PL.y, PH.y, MA.y, MB.y);
       }
       uVO = VOU; uG = GU; ucvA = cvuA; ucvB = cvuB; ucgA = cguA; ucgB = cguB;
       if (lane == 31 && p + 1 < passes) {
@@ -248,7 +274,8 @@ __device__ __forceinline__ void emit(const EngineJob& J, int q, int d, int16_t d
 }
 
 template <int K>
-__global__ void __launch_bounds__(kEngThreads, (K <= 8) ? 2 : 1) engine_kernel(EngineJob J) {
+__global__ void __launch_bounds__(warps_of(K) * 32, ctas_of(K)) engine_kernel(EngineJob J) {
+  constexpr int kEngWarps = warps_of(K);
   extern __shared__ __align__(16) uint8_t smem[];
   uint32_t* prof = reinterpret_cast<uint32_t*>(smem);
   const int A1 = J.A + 1;
@@ -256,7 +283,7 @@ __global__ void __launch_bounds__(kEngThreads, (K <= 8) ? 2 : 1) engine_kernel(E
   uint8_t* codes = reinterpret_cast<uint8_t*>(list + kMaxChunk);
   const int cbuf = 64 + ((J.maxcol + 31) / 32) * 32;
   __shared__ int s_item, s_count, s_next, s_q;
-  __shared__ int s_wc[kEngWarps];
+  __shared__ int s_wc[kMaxWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint8_t* ca = codes + (size_t)warp * 2 * cbuf;
   uint8_t* cb = ca + cbuf;
@@ -280,7 +307,9 @@ __global__ void __launch_bounds__(kEngThreads, (K <= 8) ? 2 : 1) engine_kernel(E
       for (int idx = threadIdx.x; idx < A1 * mrows; idx += blockDim.x) {
         const int c = idx / mrows, i = idx - c * mrows;
         const int pp = i / (32 * K), rem = i - pp * 32 * K, t = rem / K, rr = rem - t * K;
-        const int pos = pp * 32 * K + ((rr >> 2) * 32 + t) * 4 + (rr & 3);
+        // rows in groups of four per lane (lane-interleaved), then a group of two when K % 4 == 2
+        const int pos = pp * 32 * K + (rr < (K & ~3) ? ((rr >> 2) * 32 + t) * 4 + (rr & 3)
+                                                     : (K & ~3) * 32 + t * 2 + (rr & 1));
         const int a = (i < m) ? (int)qc[i] : J.A;
         const int v = J.lettab[a * A1 + c];
         uint32_t* pc = prof + (size_t)c * 3 * J.mpad;
@@ -375,53 +404,65 @@ __global__ void zero_diagonal_kernel(int16_t* out, long long ld, int n) {
 // ------------------------------------------------------------------------------------------------
 namespace {
 
-constexpr int kKs[4] = {4, 8, 12, 16};
+constexpr int kNumK = 7;
+constexpr int kKs[kNumK] = {4, 6, 8, 10, 12, 14, 16};
 
-size_t engine_smem(int A, int mpad, int maxcol) {
+size_t engine_smem(int A, int mpad, int maxcol, int K) {
   const int cbuf = 64 + ((maxcol + 31) / 32) * 32;
-  return (size_t)(A + 1) * 3 * mpad * 4 + kMaxChunk * 4 + (size_t)kEngWarps * 2 * cbuf;
-}
-
-template <int K>
-cudaError_t launch_engine(const EngineJob& J, int grid, size_t smem, cudaStream_t st) {
-  engine_kernel<K><<<grid, kEngThreads, smem, st>>>(J);
-  return cudaGetLastError();
-}
-
-template <int K>
-cudaError_t allow_smem(size_t smem) {
-  return cudaFuncSetAttribute(engine_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-}
-
-cudaError_t allow_smem_k(int K, size_t smem) {
-  switch (K) {
-    case 4: return allow_smem<4>(smem);
-    case 8: return allow_smem<8>(smem);
-    case 12: return allow_smem<12>(smem);
-    default: return allow_smem<16>(smem);
-  }
+  return (size_t)(A + 1) * 3 * mpad * 4 + kMaxChunk * 4 + (size_t)warps_of(K) * 2 * cbuf;
 }
 
 __global__ void set_int_kernel(int* p, int v) { *p = v; }
 
-cudaError_t launch_engine_k(int K, const EngineJob& J, int grid, size_t smem, cudaStream_t st) {
+// Calls fn(std::integral_constant<int, K>) for the engine instantiation of K rows per lane.
+template <class Fn>
+auto with_k(int K, Fn fn) {
   switch (K) {
-    case 4: return launch_engine<4>(J, grid, smem, st);
-    case 8: return launch_engine<8>(J, grid, smem, st);
-    case 12: return launch_engine<12>(J, grid, smem, st);
-    default: return launch_engine<16>(J, grid, smem, st);
+    case 4: return fn(std::integral_constant<int, 4>());
+    case 6: return fn(std::integral_constant<int, 6>());
+    case 8: return fn(std::integral_constant<int, 8>());
+    case 10: return fn(std::integral_constant<int, 10>());
+    case 12: return fn(std::integral_constant<int, 12>());
+    case 14: return fn(std::integral_constant<int, 14>());
+    default: return fn(std::integral_constant<int, 16>());
   }
 }
 
+cudaError_t allow_smem_k(int K, size_t smem) {
+  return with_k(K, [&](auto k) {
+    return cudaFuncSetAttribute(engine_kernel<decltype(k)::value>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  });
+}
+
+cudaError_t launch_engine_k(int K, const EngineJob& J, int grid, size_t smem, cudaStream_t st) {
+  return with_k(K, [&](auto k) {
+    engine_kernel<decltype(k)::value><<<grid, warps_of(decltype(k)::value) * 32, smem, st>>>(J);
+    return cudaGetLastError();
+  });
+}
+
 int occupancy_k(int K, size_t smem) {
-  int n = 0;
-  switch (K) {
-    case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel<4>, kEngThreads, smem); break;
-    case 8: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel<8>, kEngThreads, smem); break;
-    case 12: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel<12>, kEngThreads, smem); break;
-    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel<16>, kEngThreads, smem); break;
+  return with_k(K, [&](auto k) {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel<decltype(k)::value>,
+                                                  warps_of(decltype(k)::value) * 32, smem);
+    return n;
+  });
+}
+
+// Relative cost of one computed row at K rows per lane (100 = 16 rows): B200 row-padded cell
+// rates of the uneven 3,000-sequence DNA job with K forced for every query.
+long k_weight(int k) {
+  switch (k) {
+    case 4: return 188;
+    case 6: return 157;
+    case 8: return 132;
+    case 10: return 106;
+    case 12: return 101;
+    case 14: return 111;
+    default: return 100;
   }
-  return n;
 }
 
 // Rows per lane and passes for a query of m rows: fewest padded rows, then fewest passes.
@@ -434,7 +475,7 @@ void choose_k(int m, int kov, int* K, int* passes) {
     // the uneven 3,000-sequence job with K forced: 4 rows per lane cost 1.55x a row at 8-16
     // (too few rows to amortise the per-step shuffles, loads and column bookkeeping); ties go to
     // fewer passes (each pass adds a wavefront fill and a scratch round trip)
-    const long weight = (k == 4) ? 155 : 100;
+    const long weight = k_weight(k);
     const long cost = (long)p * 32 * k * weight * 16 + p;
     if (best < 0 || cost < best) { best = cost; *K = k; *passes = p; }
   }
@@ -443,11 +484,14 @@ void choose_k(int m, int kov, int* K, int* passes) {
 struct Bin {
   int K;
   int mpad;
+  int max_passes = 0;
   std::vector<int4> items;
   std::vector<double> cost;
+  double total_cost = 0;
   int item_offset = 0;
   size_t smem = 0;
   int grid = 0;
+  size_t scratch_off = 0;  // words into the pass scratch (bins run concurrently)
 };
 
 template <class T>
@@ -490,6 +534,7 @@ struct Plan {
   bool zeroes_diagonal = false;
   int thresh = 0;
   std::vector<Bin> bins;
+  std::vector<int> order;  // non-empty bins in launch order
   int big_count = 0, rerun_cap = 0;
   int64_t npairs = 0, ncells = 0;
   int4* d_items = nullptr;
@@ -527,7 +572,7 @@ bool oriented_host(int mode, const std::vector<int>& blk, int q, int d) {
 
 class EngineImpl : public Engine {
  public:
-  ~EngineImpl() override { invalidate(); }
+  ~EngineImpl() override { invalidate(); release_streams(); }
   void invalidate() override {
     plans_.clear();
     base_.reset();
@@ -598,6 +643,7 @@ class EngineImpl : public Engine {
     }
     Plan& pl = *it->second;
     last_ = &pl;
+    if ((rc = ensure_streams(msg))) return rc;
     cudaError_t e;
     if (opt_.use_graph) {
       if (!pl.graph || P.out != pl.graph_out || P.ld != pl.graph_ld || P.stream != pl.graph_stream) {
@@ -734,7 +780,7 @@ class EngineImpl : public Engine {
       const int m = B.len[q];
       int K, passes;
       choose_k(m, opt_.k_override, &K, &passes);
-      const int bi = (K == 4) ? 0 : (K == 8) ? 1 : (K == 12) ? 2 : 3;
+      const int bi = (int)(std::find(std::begin(kKs), std::end(kKs), K) - std::begin(kKs));
       const int bq = blk[q];
       for (int c = 0; c < nchunks; c++) {
         const auto& ix = cidx[c];
@@ -772,8 +818,10 @@ class EngineImpl : public Engine {
         }
         Bin& bn = pl.bins[bi];
         bn.mpad = std::max(bn.mpad, passes * 32 * K);
+        bn.max_passes = std::max(bn.max_passes, passes);
         bn.items.push_back(make_int4(q, c * chunk, std::min(N, (c + 1) * chunk), passes));
-        bn.cost.push_back((double)passes * 32 * K * (lsum + 31.0 * cnt));
+        bn.cost.push_back((double)passes * 32 * K * (lsum + 31.0 * cnt) * k_weight(K));
+        bn.total_cost += bn.cost.back();
       }
     }
     std::vector<int4> all;
@@ -789,17 +837,25 @@ class EngineImpl : public Engine {
     if ((rc = upload_vec(&pl.d_stats, st0, msg, "stats"))) return rc;
     std::vector<int> zeros(pl.bins.size() + 1, 0);
     if ((rc = upload_vec(&pl.d_counters, zeros, msg, "counters"))) return rc;
-    int max_slots = 0;
+    // the bins run concurrently: each multi-pass bin gets its own scratch slots
+    size_t scr_words = 0;
     for (auto& bn : pl.bins) {
       if (bn.items.empty()) continue;
-      bn.smem = engine_smem(A, bn.mpad, B.maxcol);
+      bn.smem = engine_smem(A, bn.mpad, B.maxcol, bn.K);
       if (bn.smem > 227 * 1024) { *msg = "query profile exceeds shared memory"; return SW_E_UNSUPPORTED; }
       if (allow_smem_k(bn.K, bn.smem) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
       const int occ = std::max(1, occupancy_k(bn.K, bn.smem));
       bn.grid = (int)std::min<long>((long)P.sms * occ, (long)bn.items.size());
-      max_slots = std::max(max_slots, bn.grid);
+      bn.scratch_off = scr_words;
+      if (bn.max_passes > 1) scr_words += (size_t)bn.grid * warps_of(bn.K) * B.maxcol * kScrWords;
     }
-    const size_t scr = std::max<size_t>((size_t)max_slots * kEngWarps * B.maxcol * kScrWords * 4, 16);
+    pl.order.clear();
+    for (size_t b = 0; b < pl.bins.size(); b++)
+      if (!pl.bins[b].items.empty()) pl.order.push_back((int)b);
+    // most work first: its CTAs take the SMs, the lighter bins fill in as its queue drains
+    std::stable_sort(pl.order.begin(), pl.order.end(),
+                     [&](int a, int b) { return pl.bins[a].total_cost > pl.bins[b].total_cost; });
+    const size_t scr = std::max<size_t>(scr_words * 4, 16);
     if (scr > B.scratch_bytes) {
       cudaFree(B.d_scratch);
       B.d_scratch = nullptr;
@@ -839,14 +895,24 @@ class EngineImpl : public Engine {
       J.scratch = B.d_scratch; J.maxcol = B.maxcol;
       J.rerun = pl.d_rerun; J.rerun_count = pl.d_rerun_count; J.rerun_cap = pl.rerun_cap;
       J.stats = pl.d_stats;
-      for (size_t b = 0; b < pl.bins.size(); b++) {
+      // fork: each bin on its own stream, all after the resets above; join before the rerun
+      const bool fork = pl.order.size() > 1;
+      if (fork && (e = cudaEventRecord(fork_, P.stream)) != cudaSuccess) return e;
+      for (size_t x = 0; x < pl.order.size(); x++) {
+        const int b = pl.order[x];
         const Bin& bn = pl.bins[b];
-        if (bn.items.empty()) continue;
+        cudaStream_t st = fork ? side_[x] : P.stream;
+        if (fork && (e = cudaStreamWaitEvent(st, fork_, 0)) != cudaSuccess) return e;
         J.items = pl.d_items + bn.item_offset;
         J.nitems = (int)bn.items.size();
         J.counter = pl.d_counters + b;
         J.mpad = bn.mpad;
-        if ((e = launch_engine_k(bn.K, J, bn.grid, bn.smem, P.stream)) != cudaSuccess) return e;
+        J.scratch = B.d_scratch + bn.scratch_off;
+        if ((e = launch_engine_k(bn.K, J, bn.grid, bn.smem, st)) != cudaSuccess) return e;
+        if (fork) {
+          if ((e = cudaEventRecord(join_[x], st)) != cudaSuccess) return e;
+          if ((e = cudaStreamWaitEvent(P.stream, join_[x], 0)) != cudaSuccess) return e;
+        }
       }
     }
     // 32-bit lanes: pairs the static guard routed here, those whose 16-bit lanes tripped, or all
@@ -864,7 +930,32 @@ class EngineImpl : public Engine {
     return launch_plain_block(R, grid, 128, P.stream);
   }
 
+  // Streams and events of the bins' fork/join, made once on the engine's device.
+  int ensure_streams(std::string* msg) {
+    if (streams_ok_) return SW_OK;
+    if (cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError(); *msg = "event create"; return SW_E_CUDA;
+    }
+    for (int x = 0; x < kNumK; x++)
+      if (cudaStreamCreateWithFlags(&side_[x], cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&join_[x], cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError(); *msg = "stream create"; return SW_E_CUDA;
+      }
+    streams_ok_ = true;
+    return SW_OK;
+  }
+  void release_streams() {
+    if (!streams_ok_) return;
+    cudaEventDestroy(fork_);
+    for (int x = 0; x < kNumK; x++) { cudaStreamDestroy(side_[x]); cudaEventDestroy(join_[x]); }
+    streams_ok_ = false;
+  }
+
   EngineOptions opt_;
+  bool streams_ok_ = false;
+  cudaEvent_t fork_ = nullptr;
+  cudaStream_t side_[kNumK] = {};
+  cudaEvent_t join_[kNumK] = {};
   std::unique_ptr<Base> base_;
   std::map<PlanKey, std::unique_ptr<Plan>> plans_;
   Plan* last_ = nullptr;

@@ -158,7 +158,7 @@ int sw_compute_rank_blocks(sw_ctx* ctx, int32_t rank, int32_t world_size, int16_
 /* Engine knobs: "stream" (a caller's cudaStream_t as an integer, 0 = the context's own; later
  * calls are ordered on it), "int16_threshold" (best score above which a 16-bit lane is redone in 32-bit
  * lanes; -1 restores the value derived from the lane range), "use_graph" (0/1), "chunk"
- * (database entries per work item), "rows_per_lane" (0 = chosen per query, else 4/8/12/16),
+ * (database entries per work item), "rows_per_lane" (0 = chosen per query, else an even number 4..16),
  * "plan_only" (1: engine calls build their work plans and graphs but launch nothing; 0: run).
  * Unknown keys are SW_E_ARG. */
 int sw_set_option(sw_ctx* ctx, const char* key, int64_t value);

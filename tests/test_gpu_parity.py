@@ -141,8 +141,8 @@ def test_engine_long_and_uneven_sequences_against_oracle(cs, oracle_mod):
     np.testing.assert_array_equal(blk[off], full[off])
 
 
-@pytest.mark.parametrize("opt", [("rows_per_lane", 4), ("rows_per_lane", 8), ("rows_per_lane", 12),
-                                 ("rows_per_lane", 16), ("chunk", 32), ("chunk", 1024), ("use_graph", 0)])
+@pytest.mark.parametrize("opt", [("rows_per_lane", k) for k in (4, 6, 8, 10, 12, 14, 16)] +
+                                [("chunk", 32), ("chunk", 1024), ("use_graph", 0)])
 def test_engine_options_do_not_change_results(cs, opt):
     from csharp_b200 import synth
     rng = np.random.default_rng(5)
