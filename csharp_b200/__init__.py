@@ -10,8 +10,9 @@ from .core import (Block, Engine, NUCLEIC, NW, PROTEIN, PairwiseAlignment, Range
                    SmithWatermanGotoh, SWG_MPI, SWG_MS, block_is_computed, block_partition,
                    measure_int_peak, pack_sequences, range_partition)
 from .core import JUKES_CANTOR, KIMURA2, PERCENT_IDENTITY
+from .lib import SwError
 
 __all__ = ["Block", "Engine", "NUCLEIC", "NW", "PROTEIN", "PairwiseAlignment", "Range",
            "ScoringMatrix", "SmithWatermanGotoh", "SWG_MPI", "SWG_MS", "block_is_computed",
            "block_partition", "measure_int_peak", "pack_sequences", "range_partition",
-           "PERCENT_IDENTITY", "KIMURA2", "JUKES_CANTOR"]
+           "PERCENT_IDENTITY", "KIMURA2", "JUKES_CANTOR", "SwError"]

@@ -245,6 +245,51 @@ class Engine:
     def synchronize(self):
         self._ck(L.load().sw_synchronize(self._h))
 
+    # ---- serving: query batches against the uploaded sequences (the database) --------------
+    def submit(self, queries, out=None):
+        """Queues a batch of queries (byte strings) against the database; returns a ticket.
+        The result (len(queries) x database Int16, query i = s1 of row i) is ``job_result``."""
+        concat, off = pack_sequences(queries)
+        nq = len(off) - 1
+        if out is None:
+            out = np.empty((nq, self.nseq), dtype=np.int16)
+        t = C.c_int64()
+        self._ck(L.load().sw_submit_job(self._h, L.ptr(concat), L.ptr(off), nq, L.ptr(out),
+                                        out.strides[0] // 2, C.byref(t)))
+        if not hasattr(self, "_jobs"):
+            self._jobs = {}
+        self._jobs[t.value] = out  # the library writes into it until the job is done
+        return t.value
+
+    def poll(self, ticket, timeout_ms=0):
+        """None while the job runs; else a dict of its sw_job_info with the result under "out"."""
+        done, info = C.c_int32(), L.sw_job_info()
+        self._ck(L.load().sw_poll(self._h, ticket, int(timeout_ms), C.byref(done), C.byref(info)))
+        if not done.value:
+            return None
+        r = {f: getattr(info, f) for f, _ in L.sw_job_info._fields_ if f != "reserved"}
+        r["out"] = self._jobs.pop(ticket)
+        return r
+
+    def wait(self, ticket, timeout_s=600.0):
+        """Polls until the job is done (raises TimeoutError after timeout_s)."""
+        import time
+        t_end = time.monotonic() + timeout_s
+        while True:
+            r = self.poll(ticket, 200)
+            if r is not None:
+                return r
+            if time.monotonic() > t_end:
+                raise TimeoutError(f"job {ticket} not done after {timeout_s} s")
+
+    def serve_stats(self):
+        s = L.sw_serve_counters()
+        self._ck(L.load().sw_serve_stats(self._h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in L.sw_serve_counters._fields_ if f != "reserved"}
+
+    def serve_drain(self):
+        self._ck(L.load().sw_serve_drain(self._h))
+
 
 class SmithWatermanGotoh:
     """The reference's aligner object: ``Align(s1, s2, matrix, o, e)`` on the device."""

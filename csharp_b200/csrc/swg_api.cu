@@ -10,6 +10,7 @@
 #include "../../include/swgb200.h"
 #include "swg_device.cuh"
 #include "swg_engine.h"
+#include "swg_serve.h"
 #include "swg_internal.h"
 
 struct sw_ctx {
@@ -40,6 +41,9 @@ struct sw_ctx {
   int64_t last_reruns = 0;
   cudaStream_t own_stream = nullptr;  // the context's stream while a caller's stream is in use
   int64_t last_pairs = 0, last_cells = 0;
+  // serving (query batches against the uploaded sequences)
+  swg::Server* server = nullptr;
+  swg::ServeOptions serve_opt;
 };
 
 namespace {
@@ -154,6 +158,7 @@ int sw_destroy(sw_ctx* ctx) {
   cudaSetDevice(ctx->cfg.device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->own_stream) ctx->stream = ctx->own_stream;
+  delete ctx->server;
   delete ctx->engine;
   cudaFree(ctx->d_seq);
   cudaFree(ctx->d_off);
@@ -186,6 +191,8 @@ int sw_upload_sequences(sw_ctx* ctx, const uint8_t* concat, const int64_t* offse
   const double bound = (double)(ctx->max_abs_score + ctx->e) * 2.0 * maxlen + ctx->o;
   if (bound >= 16777216.0) return fail(ctx, SW_E_UNSUPPORTED, "scores could exceed float's exact range");
   cudaSetDevice(ctx->cfg.device);
+  delete ctx->server;  // the database changes: jobs still running end with SW_E_STATE
+  ctx->server = nullptr;
   cudaStreamSynchronize(ctx->stream);
   cudaFree(ctx->d_seq);
   cudaFree(ctx->d_off);
@@ -445,6 +452,17 @@ int sw_set_option(sw_ctx* ctx, const char* key, int64_t value) {
     ctx->engine->set_plan_only(value ? 1 : 0);
     return SW_OK;
   }
+  if (k.compare(0, 6, "serve_") == 0) {
+    if (ctx->server) return fail(ctx, SW_E_STATE, "serving options are read when the first job is submitted");
+    if (value < 0) return fail(ctx, SW_E_ARG, "serving options are non-negative");
+    swg::ServeOptions& so = ctx->serve_opt;
+    if (k == "serve_memory_mb") so.memory_bytes = (size_t)value << 20;
+    else if (k == "serve_arena_mb") so.arena_bytes = std::max<size_t>(1, (size_t)value) << 20;
+    else if (k == "serve_slots") so.slots = (int)std::max<int64_t>(1, std::min<int64_t>(value, 1 << 20));
+    else if (k == "serve_wave_us") so.wave_seconds = std::max<int64_t>(100, value) * 1e-6;
+    else return fail(ctx, SW_E_ARG, "unknown option " + k);
+    return SW_OK;
+  }
   swg::EngineOptions& o = ctx->engine->options();
   if (k == "int16_threshold") o.int16_threshold = value;
   else if (k == "use_graph") o.use_graph = value ? 1 : 0;
@@ -471,6 +489,82 @@ int sw_all_pairs(sw_ctx* ctx, int32_t ranks, int16_t* out, int64_t ld, int64_t* 
   if ((rc = sw_all_pairs_device(ctx, ranks, ctx->d_stage, (int64_t)N, pairs, cells))) return rc;
   if (N) CK(cudaMemcpy2DAsync(out, (size_t)ld * 2, ctx->d_stage, N * 2, N * 2, N, cudaMemcpyDeviceToHost, ctx->stream), "copy result");
   CK(cudaStreamSynchronize(ctx->stream), "all pairs");
+  return SW_OK;
+}
+
+static swg::EngineParams db_params(sw_ctx* ctx) {
+  swg::EngineParams P;
+  P.seq = ctx->d_seq; P.off = ctx->d_off;
+  P.h_off = ctx->h_off.data(); P.h_seq = ctx->h_seq.data();
+  P.nseq = ctx->nseq; P.maxlen = ctx->maxlen;
+  P.scores = ctx->d_scores; P.flags = ctx->d_flags;
+  P.h_scores = &ctx->h_scores[0][0]; P.h_flags = &ctx->h_flags[0][0];
+  P.max_score = ctx->max_score; P.max_abs_score = ctx->max_abs_score;
+  P.o = ctx->o; P.e = ctx->e;
+  P.mode = ctx->cfg.mode;
+  P.protein = ctx->cfg.alignment_type == SW_PROTEIN;
+  P.lanes = ctx->cfg.lanes;
+  P.ranks = 1;
+  P.out = nullptr; P.ld = 0;
+  P.sms = ctx->sms;
+  P.stream = ctx->stream;
+  return P;
+}
+
+int sw_submit_job(sw_ctx* ctx, const uint8_t* q_concat, const int64_t* q_offsets, int32_t nq,
+                  int16_t* out, int64_t ld_out, int64_t* ticket) {
+  if (!ctx) return SW_E_ARG;
+  if (!ctx->d_seq) return fail(ctx, SW_E_STATE, "no database uploaded");
+  if (nq < 1 || !q_offsets || !out || !ticket || ld_out < ctx->nseq) return fail(ctx, SW_E_ARG, "bad arguments");
+  if (q_offsets[0] != 0) return fail(ctx, SW_E_ARG, "offsets[0] must be 0");
+  if (!q_concat && q_offsets[nq] > 0) return fail(ctx, SW_E_ARG, "bad query arrays");
+  int maxlen = ctx->maxlen;
+  for (int32_t k = 0; k < nq; k++) {
+    const int64_t len = q_offsets[k + 1] - q_offsets[k];
+    if (len < 0) return fail(ctx, SW_E_ARG, "offsets must be non-decreasing");
+    if (len > 32767) return fail(ctx, SW_E_UNSUPPORTED, "query longer than 32767 residues");
+    maxlen = std::max(maxlen, (int)len);
+  }
+  for (int64_t k = 0; k < q_offsets[nq]; k++)
+    if (q_concat[k] >= 127) return fail(ctx, SW_E_ARG, "residue byte outside the 127-entry scoring table");
+  const double bound = (double)(ctx->max_abs_score + ctx->e) * 2.0 * maxlen + ctx->o;
+  if (bound >= 16777216.0) return fail(ctx, SW_E_UNSUPPORTED, "scores could exceed float's exact range");
+  cudaSetDevice(ctx->cfg.device);
+  std::string msg;
+  if (!ctx->server) {
+    cudaStreamSynchronize(ctx->stream);
+    int rc = 0;
+    ctx->server = swg::Server::create(db_params(ctx), ctx->cfg.device, ctx->serve_opt, &msg, &rc);
+    if (!ctx->server) return fail(ctx, rc ? rc : SW_E_OOM, msg);
+  }
+  const int rc = ctx->server->submit(q_concat, q_offsets, nq, out, ld_out, ticket, &msg);
+  return rc ? fail(ctx, rc, msg) : SW_OK;
+}
+
+int sw_poll(sw_ctx* ctx, int64_t ticket, int32_t timeout_ms, int32_t* done, sw_job_info* info) {
+  if (!ctx || !done) return SW_E_ARG;
+  if (!ctx->server) return fail(ctx, SW_E_ARG, "unknown ticket");
+  int d = 0;
+  const int rc = ctx->server->poll(ticket, std::max(0, timeout_ms), &d, info);
+  *done = d;
+  if (rc == SW_E_ARG) return fail(ctx, rc, "unknown ticket");
+  if (rc) return fail(ctx, rc, "job failed");
+  return SW_OK;
+}
+
+int sw_serve_stats(sw_ctx* ctx, sw_serve_counters* stats) {
+  if (!ctx || !stats) return SW_E_ARG;
+  std::memset(stats, 0, sizeof(*stats));
+  if (ctx->server) ctx->server->stats(stats);
+  return SW_OK;
+}
+
+int sw_serve_drain(sw_ctx* ctx) {
+  if (!ctx) return SW_E_ARG;
+  if (!ctx->server) return SW_OK;
+  ctx->server->drain();
+  delete ctx->server;
+  ctx->server = nullptr;
   return SW_OK;
 }
 

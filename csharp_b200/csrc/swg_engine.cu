@@ -68,6 +68,15 @@ struct EngineJob {
   int rerun_cap;
   int mpad;                 // profile rows staged (passes * 32 * K of the bin)
   unsigned long long* stats; // [0] items taken, [1] pairs finished in 16-bit lanes, [2] tripped
+  // Query mode (serving): s1 is query slot q of a separate set, s2 every database entry of the
+  // chunk, the distance goes to qout[q][d].  Raw residue bytes index qtab/qflag (row 127 = pad).
+  int qmode;
+  const uint8_t* qseq;
+  const int64_t* qoff;
+  const int32_t* qlen;
+  int16_t* const* qout;
+  const int32_t* qtab;      // [128 * (A+1)] S(x, letter c) + o; pad row/column -bias + o
+  const uint32_t* qflag;    // [128 * (A+1)]
 };
 
 // Rank owning a global row index under RangePartitioner (Program.cs:791-802).
@@ -76,7 +85,7 @@ __device__ __forceinline__ int block_of(int x, int a, int b) {
 }
 
 __device__ __forceinline__ bool oriented(const EngineJob& J, int q, int d) {
-  if (J.mode == kModeSwgMs) return true;
+  if (J.qmode || J.mode == kModeSwgMs) return true;
   if (q == d) return false;
   const int bq = block_of(q, J.rb_a, J.rb_b), bd = block_of(d, J.rb_a, J.rb_b);
   if (bq == bd) return q > d;
@@ -269,6 +278,10 @@ __device__ __forceinline__ void warp_best(int& best, int& row, uint32_t& cnt) {
 }
 
 __device__ __forceinline__ void emit(const EngineJob& J, int q, int d, int16_t dist) {
+  if (J.qmode) {
+    J.qout[q][d] = dist;
+    return;
+  }
   J.out[(long long)q * J.ld + d] = dist;
   if (J.mode != kModeSwgMs) J.out[(long long)d * J.ld + q] = dist;
 }
@@ -297,25 +310,28 @@ __global__ void __launch_bounds__(warps_of(K) * 32, ctas_of(K)) engine_kernel(En
     const int4 item = J.items[it];
     const int q = item.x, c0 = item.y, c1 = item.z, passes = item.w;
     if (threadIdx.x == 0) atomicAdd(J.stats, 1ull);
-    const int m = (int)(J.off[q + 1] - J.off[q]);
+    const int m = J.qmode ? J.qlen[q] : (int)(J.off[q + 1] - J.off[q]);
     const int mrows = passes * 32 * K;
     // query profile (rows beyond m and the pad column score -bias, count nothing)
     const bool rebuild = (q != s_q);
     __syncthreads();
     if (rebuild) {
-      const uint8_t* qc = J.code + J.off[q];
+      const uint8_t* qc = J.qmode ? J.qseq + J.qoff[q] : J.code + J.off[q];
+      const int32_t* ptab = J.qmode ? J.qtab : J.lettab;
+      const uint32_t* ftab = J.qmode ? J.qflag : J.flagtab;
+      const int pad = J.qmode ? kPadCode : J.A;
       for (int idx = threadIdx.x; idx < A1 * mrows; idx += blockDim.x) {
         const int c = idx / mrows, i = idx - c * mrows;
         const int pp = i / (32 * K), rem = i - pp * 32 * K, t = rem / K, rr = rem - t * K;
         // rows in groups of four per lane (lane-interleaved), then a group of two when K % 4 == 2
         const int pos = pp * 32 * K + (rr < (K & ~3) ? ((rr >> 2) * 32 + t) * 4 + (rr & 3)
                                                      : (K & ~3) * 32 + t * 2 + (rr & 1));
-        const int a = (i < m) ? (int)qc[i] : J.A;
-        const int v = J.lettab[a * A1 + c];
+        const int a = (i < m) ? (int)qc[i] : pad;
+        const int v = ptab[a * A1 + c];
         uint32_t* pc = prof + (size_t)c * 3 * J.mpad;
         pc[pos] = (uint32_t)v;
         pc[J.mpad + pos] = (uint32_t)v << 16;
-        pc[2 * J.mpad + pos] = J.flagtab[a * A1 + c];
+        pc[2 * J.mpad + pos] = ftab[a * A1 + c];
       }
     }
     if (threadIdx.x == 0) { s_q = q; s_count = 0; s_next = 0; }
@@ -513,7 +529,7 @@ int upload_vec(T** dst, const std::vector<T>& v, std::string* msg, const char* w
 // State of one sequence set shared by every plan: residue codes, length order, tables.
 struct Base {
   int alpha = 0, bias = 1, max_s = 0, maxcol = 1;
-  std::vector<int> len, sorted_h;
+  std::vector<int> len, sorted_h, letters;
   uint8_t* d_code = nullptr;
   int32_t* d_sorted = nullptr;
   int32_t* d_lettab = nullptr;
@@ -527,6 +543,66 @@ struct Base {
     cudaFree(d_scratch); cudaFree(d_carry);
   }
 };
+
+// Residue codes of the sequence set, its length order and the dense score/flag tables of the
+// 16-bit lanes (alphabets of up to 8 letters), plus the 32-bit lanes' scratch.
+int build_base(Base& B, const EngineParams& P, std::string* msg) {
+  const int N = P.nseq;
+  const int64_t total = P.h_off[N];
+  int code_of[128];
+  std::fill(code_of, code_of + 128, -1);
+  std::vector<int> letters;
+  for (int64_t k = 0; k < total; k++) {
+    const int b = P.h_seq[k];
+    if (code_of[b] < 0) { code_of[b] = (int)letters.size(); letters.push_back(b); }
+  }
+  B.alpha = (int)letters.size();
+  B.letters = letters;
+  B.len.resize(N);
+  for (int i = 0; i < N; i++) B.len[i] = (int)(P.h_off[i + 1] - P.h_off[i]);
+  B.maxcol = std::max(P.maxlen, 1);
+  B.sorted_h.resize(N);
+  std::iota(B.sorted_h.begin(), B.sorted_h.end(), 0);
+  std::stable_sort(B.sorted_h.begin(), B.sorted_h.end(), [&](int a, int b) { return B.len[a] < B.len[b]; });
+  int rc;
+  // the 32-bit lanes (reruns, NW, large alphabets) need the plain kernel's scratch
+  B.carry_threads = (long)P.sms * 8 * 128;
+  if (cudaMalloc(&B.d_carry, plain_carry_bytes(P.mode == kModeNw ? kModeNw : kModeSwgMpi, B.carry_threads, B.maxcol)) != cudaSuccess) {
+    cudaGetLastError(); B.d_carry = nullptr; *msg = "cudaMalloc 32-bit lane scratch"; return SW_E_OOM;
+  }
+  if (B.alpha > 8 || P.mode == kModeNw || P.lanes == SW_LANES_32) return SW_OK;
+  const int A = B.alpha, A1 = A + 1;
+  int maxS = 0, minS = 0;
+  for (int a : letters)
+    for (int b : letters) {
+      const int s = P.h_scores[a * 128 + b];
+      maxS = std::max(maxS, s);
+      minS = std::min(minS, s);
+    }
+  B.bias = std::max(std::max(P.o + 2 * P.e, -minS), 1);
+  B.max_s = maxS;
+  std::vector<int32_t> lettab((size_t)A1 * A1);
+  std::vector<uint32_t> flagtab((size_t)A1 * A1, 0u);
+  for (int a = 0; a < A1; a++)
+    for (int c = 0; c < A1; c++) {
+      int s;
+      uint32_t f = 0;
+      if (a == A || c == A) s = -B.bias;
+      else {
+        s = P.h_scores[letters[a] * 128 + letters[c]];
+        f = P.h_flags[letters[a] * 128 + letters[c]] & kFlagCount;
+      }
+      lettab[(size_t)a * A1 + c] = s + P.o;
+      flagtab[(size_t)a * A1 + c] = f;
+    }
+  std::vector<uint8_t> code((size_t)total + 64, (uint8_t)A);
+  for (int64_t k = 0; k < total; k++) code[(size_t)k] = (uint8_t)code_of[P.h_seq[k]];
+  if ((rc = upload_vec(&B.d_code, code, msg, "codes"))) return rc;
+  if ((rc = upload_vec(&B.d_sorted, B.sorted_h, msg, "order"))) return rc;
+  if ((rc = upload_vec(&B.d_lettab, lettab, msg, "score table"))) return rc;
+  if ((rc = upload_vec(&B.d_flagtab, flagtab, msg, "flag table"))) return rc;
+  return SW_OK;
+}
 
 // One job (mode, world size, query range): its work items, 32-bit pair list and CUDA graph.
 struct Plan {
@@ -631,7 +707,7 @@ class EngineImpl : public Engine {
     int rc;
     if (!base_) {
       base_.reset(new Base());
-      if ((rc = build_base(P, msg))) { base_.reset(); return rc; }
+      if ((rc = build_base(*base_, P, msg))) { base_.reset(); return rc; }
     }
     const int N = P.nseq;
     PlanKey key{P.mode, P.ranks, std::max(0, P.row_lo), P.row_hi < 0 ? N - 1 : std::min(N - 1, P.row_hi)};
@@ -676,64 +752,6 @@ class EngineImpl : public Engine {
   }
 
  private:
-  int build_base(const EngineParams& P, std::string* msg) {
-    Base& B = *base_;
-    const int N = P.nseq;
-    const int64_t total = P.h_off[N];
-    int code_of[128];
-    std::fill(code_of, code_of + 128, -1);
-    std::vector<int> letters;
-    for (int64_t k = 0; k < total; k++) {
-      const int b = P.h_seq[k];
-      if (code_of[b] < 0) { code_of[b] = (int)letters.size(); letters.push_back(b); }
-    }
-    B.alpha = (int)letters.size();
-    B.len.resize(N);
-    for (int i = 0; i < N; i++) B.len[i] = (int)(P.h_off[i + 1] - P.h_off[i]);
-    B.maxcol = std::max(P.maxlen, 1);
-    int rc;
-    // the 32-bit lanes (reruns, NW, large alphabets) need the plain kernel's scratch
-    B.carry_threads = (long)P.sms * 8 * 128;
-    if (cudaMalloc(&B.d_carry, plain_carry_bytes(P.mode == kModeNw ? kModeNw : kModeSwgMpi, B.carry_threads, B.maxcol)) != cudaSuccess) {
-      cudaGetLastError(); B.d_carry = nullptr; *msg = "cudaMalloc 32-bit lane scratch"; return SW_E_OOM;
-    }
-    if (B.alpha > 8 || P.mode == kModeNw || P.lanes == SW_LANES_32) return SW_OK;
-    const int A = B.alpha, A1 = A + 1;
-    int maxS = 0, minS = 0;
-    for (int a : letters)
-      for (int b : letters) {
-        const int s = P.h_scores[a * 128 + b];
-        maxS = std::max(maxS, s);
-        minS = std::min(minS, s);
-      }
-    B.bias = std::max(std::max(P.o + 2 * P.e, -minS), 1);
-    B.max_s = maxS;
-    std::vector<int32_t> lettab((size_t)A1 * A1);
-    std::vector<uint32_t> flagtab((size_t)A1 * A1, 0u);
-    for (int a = 0; a < A1; a++)
-      for (int c = 0; c < A1; c++) {
-        int s;
-        uint32_t f = 0;
-        if (a == A || c == A) s = -B.bias;
-        else {
-          s = P.h_scores[letters[a] * 128 + letters[c]];
-          f = P.h_flags[letters[a] * 128 + letters[c]] & kFlagCount;
-        }
-        lettab[(size_t)a * A1 + c] = s + P.o;
-        flagtab[(size_t)a * A1 + c] = f;
-      }
-    std::vector<uint8_t> code((size_t)total + 64, (uint8_t)A);
-    for (int64_t k = 0; k < total; k++) code[(size_t)k] = (uint8_t)code_of[P.h_seq[k]];
-    B.sorted_h.resize(N);
-    std::iota(B.sorted_h.begin(), B.sorted_h.end(), 0);
-    std::stable_sort(B.sorted_h.begin(), B.sorted_h.end(), [&](int a, int b) { return B.len[a] < B.len[b]; });
-    if ((rc = upload_vec(&B.d_code, code, msg, "codes"))) return rc;
-    if ((rc = upload_vec(&B.d_sorted, B.sorted_h, msg, "order"))) return rc;
-    if ((rc = upload_vec(&B.d_lettab, lettab, msg, "score table"))) return rc;
-    if ((rc = upload_vec(&B.d_flagtab, flagtab, msg, "flag table"))) return rc;
-    return SW_OK;
-  }
-
   int build_plan(const EngineParams& P, const PlanKey& key, Plan& pl, std::string* msg) {
     Base& B = *base_;
     const int N = P.nseq;
@@ -961,8 +979,301 @@ class EngineImpl : public Engine {
   Plan* last_ = nullptr;
 };
 
+// ---- query mode ---------------------------------------------------------------------------------
+// Nominal rates of the cost model (GPU seconds of an item): row-padded cells per second of the
+// 16-bit lanes at 16 rows per lane, and cells per second of the 32-bit lanes, on B200.
+constexpr double kRate16 = 1.45e12;
+constexpr double kRate32 = 1.4e11;
+constexpr int kQueryChunk = 512;
+
+class QueryRunnerImpl : public QueryRunner {
+ public:
+  ~QueryRunnerImpl() override {
+    cudaFree(d_qtab_); cudaFree(d_qflag_); cudaFree(d_scratch_);
+    for (auto& w : wb_) {
+      cudaFree(w.d_items); cudaFree(w.d_counters); cudaFree(w.d_stats); cudaFree(w.d_rerun);
+      cudaFree(w.d_rerun_count); cudaFreeHost(w.h_items); cudaFreeHost(w.h_rerun);
+    }
+    if (fork_) cudaEventDestroy(fork_);
+    for (int x = 0; x < kNumK; x++) {
+      if (side_[x]) cudaStreamDestroy(side_[x]);
+      if (join_[x]) cudaEventDestroy(join_[x]);
+    }
+  }
+
+  int init(const EngineParams& P, std::string* msg) {
+    P_ = P;
+    int rc = build_base(B_, P, msg);
+    if (rc) return rc;
+    N_ = P.nseq;
+    lanes16_ = !(B_.alpha > 8 || P.mode == kModeNw || P.lanes == SW_LANES_32 || B_.alpha == 0);
+    // database chunks in length order
+    for (int c0 = 0; c0 < N_; c0 += kQueryChunk) {
+      const int c1 = std::min(N_, c0 + kQueryChunk);
+      int64_t sum = 0;
+      int mx = 0;
+      for (int k = c0; k < c1; k++) { sum += B_.len[B_.sorted_h[k]]; mx = std::max(mx, B_.len[B_.sorted_h[k]]); }
+      chunk_lo_.push_back(c0); chunk_hi_.push_back(c1); chunk_sum_.push_back(sum); chunk_max_.push_back(mx);
+      total_len_ += sum;
+    }
+    if (fork_ == nullptr) {
+      if (cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming) != cudaSuccess) { *msg = "event create"; return SW_E_CUDA; }
+      for (int x = 0; x < kNumK; x++)
+        if (cudaStreamCreateWithFlags(&side_[x], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&join_[x], cudaEventDisableTiming) != cudaSuccess) {
+          cudaGetLastError(); *msg = "stream create"; return SW_E_CUDA;
+        }
+    }
+    if (!lanes16_) return SW_OK;
+    // query-side tables: any residue byte (rows) against the database letters (columns)
+    const int A = B_.alpha, A1 = A + 1;
+    int maxS = 0, minS = 0;
+    for (int x = 0; x < 127; x++)
+      for (int b : B_.letters) {
+        const int v = P.h_scores[x * 128 + b];
+        maxS = std::max(maxS, v);
+        minS = std::min(minS, v);
+      }
+    bias_ = std::max(std::max(P.o + 2 * P.e, -minS), 1);
+    max_s_ = maxS;
+    thresh_ = 32767 - bias_ - max_s_;
+    std::vector<int32_t> qtab((size_t)128 * A1);
+    std::vector<uint32_t> qflag((size_t)128 * A1, 0u);
+    for (int x = 0; x < 128; x++)
+      for (int c = 0; c < A1; c++) {
+        int v = -bias_;
+        uint32_t f = 0;
+        if (x != kPadCode && c != A) {
+          v = P.h_scores[x * 128 + B_.letters[c]];
+          f = P.h_flags[x * 128 + B_.letters[c]] & kFlagCount;
+        }
+        qtab[(size_t)x * A1 + c] = v + P.o;
+        qflag[(size_t)x * A1 + c] = f;
+      }
+    if ((rc = upload_vec(&d_qtab_, qtab, msg, "query score table"))) return rc;
+    if ((rc = upload_vec(&d_qflag_, qflag, msg, "query flag table"))) return rc;
+    return SW_OK;
+  }
+
+  int db_count() const override { return N_; }
+
+  int64_t query_cells(int m) const override { return (int64_t)m * total_len_; }
+
+  void plan_query(int slot, int m, std::vector<QueryItem>* items) const override {
+    int K = 0, passes = 0;
+    bool fits = lanes16_;
+    if (fits) {
+      choose_k(m, 0, &K, &passes);
+      // a profile beyond shared memory (queries of several thousand residues): 32-bit lanes
+      fits = engine_smem(B_.alpha, passes * 32 * K, B_.maxcol, K) <= 227 * 1024;
+    }
+    for (size_t c = 0; c < chunk_lo_.size(); c++) {
+      QueryItem it;
+      it.slot = slot;
+      it.c0 = chunk_lo_[c];
+      it.c1 = chunk_hi_[c];
+      const int cnt = it.c1 - it.c0;
+      const int mn = std::min(m, chunk_max_[c]);
+      if (fits && (long)max_s_ * (mn + 1) + bias_ <= 32767) {
+        it.K = K;
+        it.passes = passes;
+        it.cost = (double)passes * 32 * K * ((double)chunk_sum_[c] + 31.0 * cnt) * k_weight(K) / 100.0 / kRate16;
+      } else {
+        // 16-bit lanes cannot hold these scores (or are not available): 32-bit lanes
+        it.K = 0;
+        it.passes = 0;
+        it.cost = (double)std::max(m, 1) * ((double)chunk_sum_[c] + cnt) / kRate32;
+      }
+      items->push_back(it);
+    }
+  }
+
+  int enqueue(int buf, const std::vector<QueryItem>& items, const QueryTables& T, cudaStream_t st,
+              std::string* msg) override {
+    WaveBuf& W = wb_[buf & 1];
+    // bins by rows per lane, longest first inside each; 32-bit items become explicit pairs
+    std::vector<std::vector<const QueryItem*>> bins(kNumK);
+    std::vector<double> bin_cost(kNumK, 0.0);
+    size_t n16 = 0, nbig = 0;
+    long long pairs16 = 0;
+    for (const QueryItem& it : items) {
+      if (it.K == 0) { nbig += (size_t)(it.c1 - it.c0); continue; }
+      const int b = (int)(std::find(std::begin(kKs), std::end(kKs), it.K) - std::begin(kKs));
+      bins[b].push_back(&it);
+      bin_cost[b] += it.cost;
+      n16++;
+      pairs16 += it.c1 - it.c0;
+    }
+    const size_t rerun_cap = std::max<size_t>(nbig + (size_t)pairs16, 1);
+    int rc;
+    if ((rc = grow(W, std::max<size_t>(n16, 1), rerun_cap, msg))) return rc;
+    size_t big = 0;
+    for (const QueryItem& it : items)
+      if (it.K == 0)
+        for (int k = it.c0; k < it.c1; k++) W.h_rerun[big++] = make_int2(it.slot, B_.sorted_h[k]);
+    struct Launch { int K, b, offset, count, mpad, max_passes; };
+    std::vector<Launch> ls;
+    size_t pos = 0;
+    for (int b = 0; b < kNumK; b++) {
+      if (bins[b].empty()) continue;
+      std::stable_sort(bins[b].begin(), bins[b].end(), [](const QueryItem* x, const QueryItem* y) { return x->cost > y->cost; });
+      Launch L{kKs[b], b, (int)pos, (int)bins[b].size(), 0, 0};
+      for (const QueryItem* it : bins[b]) {
+        W.h_items[pos++] = make_int4(it->slot, it->c0, it->c1, it->passes);
+        L.mpad = std::max(L.mpad, it->passes * 32 * L.K);
+        L.max_passes = std::max(L.max_passes, it->passes);
+      }
+      ls.push_back(L);
+    }
+    std::stable_sort(ls.begin(), ls.end(), [&](const Launch& x, const Launch& y) { return bin_cost[x.b] > bin_cost[y.b]; });
+    // per-bin launch shape and scratch (bins run concurrently, each multi-pass bin has its own)
+    const int A = B_.alpha;
+    std::vector<size_t> smem(ls.size()), scr_off(ls.size());
+    std::vector<int> grid(ls.size());
+    size_t scr_words = 0;
+    for (size_t x = 0; x < ls.size(); x++) {
+      smem[x] = engine_smem(A, ls[x].mpad, B_.maxcol, ls[x].K);
+      if (smem[x] > 227 * 1024) { *msg = "query profile exceeds shared memory"; return SW_E_UNSUPPORTED; }
+      if (allow_smem_k(ls[x].K, smem[x]) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
+      const int occ = std::max(1, occupancy_k(ls[x].K, smem[x]));
+      grid[x] = std::min(P_.sms * occ, ls[x].count);
+      scr_off[x] = scr_words;
+      if (ls[x].max_passes > 1) scr_words += (size_t)grid[x] * warps_of(ls[x].K) * B_.maxcol * kScrWords;
+    }
+    if (scr_words * 4 > scratch_bytes_) {
+      // earlier waves may still use the old scratch: cudaFree waits for the device
+      cudaFree(d_scratch_);
+      d_scratch_ = nullptr;
+      scratch_bytes_ = 0;
+      if (cudaMalloc(&d_scratch_, scr_words * 4) != cudaSuccess) { cudaGetLastError(); *msg = "cudaMalloc pass scratch"; return SW_E_OOM; }
+      scratch_bytes_ = scr_words * 4;
+    }
+    cudaError_t e;
+    if (n16 && (e = cudaMemcpyAsync(W.d_items, W.h_items, n16 * sizeof(int4), cudaMemcpyHostToDevice, st)) != cudaSuccess) return cuda_err(e, msg);
+    if (big && (e = cudaMemcpyAsync(W.d_rerun, W.h_rerun, big * sizeof(int2), cudaMemcpyHostToDevice, st)) != cudaSuccess) return cuda_err(e, msg);
+    if ((e = cudaMemsetAsync(W.d_counters, 0, sizeof(int) * kNumK, st)) != cudaSuccess) return cuda_err(e, msg);
+    if ((e = cudaMemsetAsync(W.d_stats, 0, sizeof(unsigned long long) * 4, st)) != cudaSuccess) return cuda_err(e, msg);
+    set_int_kernel<<<1, 1, 0, st>>>(W.d_rerun_count, (int)big);
+    if (!ls.empty()) {
+      EngineJob J;
+      std::memset(&J, 0, sizeof(J));
+      J.code = B_.d_code; J.off = P_.off; J.sorted = B_.d_sorted;
+      J.A = A; J.o = P_.o; J.e = P_.e; J.bias = bias_; J.thresh = thresh_;
+      J.mode = P_.mode; J.ranks = 1; J.nseq = N_;
+      J.maxcol = B_.maxcol;
+      J.rerun = W.d_rerun; J.rerun_count = W.d_rerun_count; J.rerun_cap = (int)rerun_cap;
+      J.stats = W.d_stats;
+      J.qmode = 1; J.qseq = T.qseq; J.qoff = T.qoff; J.qlen = T.qlen; J.qout = T.qout;
+      J.qtab = d_qtab_; J.qflag = d_qflag_;
+      const bool fork = ls.size() > 1;
+      if (fork && (e = cudaEventRecord(fork_, st)) != cudaSuccess) return cuda_err(e, msg);
+      for (size_t x = 0; x < ls.size(); x++) {
+        cudaStream_t s2 = fork ? side_[x] : st;
+        if (fork && (e = cudaStreamWaitEvent(s2, fork_, 0)) != cudaSuccess) return cuda_err(e, msg);
+        J.items = W.d_items + ls[x].offset;
+        J.nitems = ls[x].count;
+        J.counter = W.d_counters + ls[x].b;
+        J.mpad = ls[x].mpad;
+        J.scratch = d_scratch_ + scr_off[x];
+        if ((e = launch_engine_k(ls[x].K, J, grid[x], smem[x], s2)) != cudaSuccess) return cuda_err(e, msg);
+        if (fork) {
+          if ((e = cudaEventRecord(join_[x], s2)) != cudaSuccess) return cuda_err(e, msg);
+          if ((e = cudaStreamWaitEvent(st, join_[x], 0)) != cudaSuccess) return cuda_err(e, msg);
+        }
+      }
+    }
+    // 32-bit lanes: pairs routed there by the static guard and 16-bit lanes that tripped
+    PlainJob R;
+    std::memset(&R, 0, sizeof(R));
+    R.seq = P_.seq; R.off = P_.off;
+    R.list = W.d_rerun; R.list_count = W.d_rerun_count;
+    R.npairs = (long long)rerun_cap;
+    R.scores = P_.scores; R.flags = P_.flags;
+    R.o = P_.o; R.e = P_.e; R.mode = P_.mode; R.protein = P_.protein;
+    R.carry = B_.d_carry;
+    R.qseq = T.qseq; R.qoff = T.qoff; R.qlen = T.qlen; R.qout = T.qout;
+    const int g = big > 0 ? (int)(B_.carry_threads / 128) : P_.sms;
+    if ((e = launch_plain_block(R, g, 128, st)) != cudaSuccess) return cuda_err(e, msg);
+    return SW_OK;
+  }
+
+ private:
+  struct WaveBuf {
+    int4* d_items = nullptr;
+    int4* h_items = nullptr;
+    size_t cap_items = 0;
+    int2* d_rerun = nullptr;
+    int2* h_rerun = nullptr;
+    size_t cap_rerun = 0;
+    int* d_counters = nullptr;
+    int* d_rerun_count = nullptr;
+    unsigned long long* d_stats = nullptr;
+  };
+
+  static int cuda_err(cudaError_t e, std::string* msg) {
+    *msg = std::string("query wave: ") + cudaGetErrorString(e);
+    return SW_E_CUDA;
+  }
+
+  // Wave buffers grow geometrically; a buffer is only regrown when its earlier wave is done.
+  int grow(WaveBuf& W, size_t items, size_t rerun, std::string* msg) {
+    if (!W.d_counters) {
+      if (cudaMalloc(&W.d_counters, sizeof(int) * kNumK) != cudaSuccess ||
+          cudaMalloc(&W.d_rerun_count, sizeof(int)) != cudaSuccess ||
+          cudaMalloc(&W.d_stats, sizeof(unsigned long long) * 4) != cudaSuccess) {
+        cudaGetLastError(); *msg = "cudaMalloc wave counters"; return SW_E_OOM;
+      }
+    }
+    if (items > W.cap_items) {
+      const size_t cap = std::max(items, W.cap_items * 2);
+      cudaFree(W.d_items); cudaFreeHost(W.h_items);
+      W.d_items = nullptr; W.h_items = nullptr; W.cap_items = 0;
+      if (cudaMalloc(&W.d_items, cap * sizeof(int4)) != cudaSuccess ||
+          cudaMallocHost(&W.h_items, cap * sizeof(int4)) != cudaSuccess) {
+        cudaGetLastError(); *msg = "wave item buffers"; return SW_E_OOM;
+      }
+      W.cap_items = cap;
+    }
+    if (rerun > W.cap_rerun) {
+      const size_t cap = std::max(rerun, W.cap_rerun * 2);
+      cudaFree(W.d_rerun); cudaFreeHost(W.h_rerun);
+      W.d_rerun = nullptr; W.h_rerun = nullptr; W.cap_rerun = 0;
+      if (cudaMalloc(&W.d_rerun, cap * sizeof(int2)) != cudaSuccess ||
+          cudaMallocHost(&W.h_rerun, cap * sizeof(int2)) != cudaSuccess) {
+        cudaGetLastError(); *msg = "wave pair buffers"; return SW_E_OOM;
+      }
+      W.cap_rerun = cap;
+    }
+    return SW_OK;
+  }
+
+  EngineParams P_;
+  Base B_;
+  int N_ = 0;
+  bool lanes16_ = false;
+  int bias_ = 1, max_s_ = 0, thresh_ = 0;
+  int64_t total_len_ = 0;
+  std::vector<int> chunk_lo_, chunk_hi_, chunk_max_;
+  std::vector<int64_t> chunk_sum_;
+  int32_t* d_qtab_ = nullptr;
+  uint32_t* d_qflag_ = nullptr;
+  uint32_t* d_scratch_ = nullptr;
+  size_t scratch_bytes_ = 0;
+  WaveBuf wb_[2];
+  cudaEvent_t fork_ = nullptr;
+  cudaStream_t side_[kNumK] = {};
+  cudaEvent_t join_[kNumK] = {};
+};
+
 }  // namespace
 
 Engine* Engine::create() { return new (std::nothrow) EngineImpl(); }
+
+QueryRunner* QueryRunner::create(const EngineParams& db, std::string* msg, int* rc) {
+  QueryRunnerImpl* q = new (std::nothrow) QueryRunnerImpl();
+  if (!q) { *rc = SW_E_OOM; *msg = "query runner"; return nullptr; }
+  if ((*rc = q->init(db, msg))) { delete q; return nullptr; }
+  return q;
+}
 
 }  // namespace swg

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 namespace swg {
 
@@ -49,6 +50,41 @@ class Engine {
   virtual int64_t stat(const char* key) const = 0;
   // Pairs the last run gave to 32-bit lanes (static guard plus tripped lanes); waits on st.
   virtual int rerun_count(cudaStream_t st, int64_t* count, std::string* msg) = 0;
+};
+
+// ---- query mode (serving) ---------------------------------------------------------------------
+// A query batch is aligned (query = s1) against every sequence of the set, which serves as the
+// database.  Work is cut into items (query slot, chunk of the database in length order) that
+// waves of the same persistent kernels execute; the caller (the server) decides which items go
+// into which wave.
+
+struct QueryItem {
+  int slot;       // query slot (row of the device query tables)
+  int c0, c1;     // database chunk: positions [c0, c1) of the length order
+  int K, passes;  // rows per lane and passes (16-bit lanes); K = 0: 32-bit lanes
+  double cost;    // estimated GPU seconds
+};
+
+struct QueryTables {   // device, indexed by slot
+  const uint8_t* qseq;
+  const int64_t* qoff;
+  const int32_t* qlen;
+  int16_t* const* qout;  // each a row of database-count distances
+};
+
+class QueryRunner {
+ public:
+  // db describes the database (the context's uploaded sequences, scores and penalties).
+  static QueryRunner* create(const EngineParams& db, std::string* msg, int* rc);
+  virtual ~QueryRunner() {}
+  virtual int db_count() const = 0;
+  // Appends the items of one query of m residues held in `slot`.
+  virtual void plan_query(int slot, int m, std::vector<QueryItem>* items) const = 0;
+  // Useful cells of one query of m residues against the whole database.
+  virtual int64_t query_cells(int m) const = 0;
+  // Enqueues one wave on st (wave buffer `buf`, 0 or 1, reused once its earlier wave is done).
+  virtual int enqueue(int buf, const std::vector<QueryItem>& items, const QueryTables& T,
+                      cudaStream_t st, std::string* msg) = 0;
 };
 
 }  // namespace swg

@@ -27,6 +27,11 @@ struct PlainJob {
   void* carry;             // device scratch, plain_carry_bytes(mode, threads, maxlen)
   const int2* list;        // optional explicit pairs (s1 index, s2 index); replaces the block
   const int* list_count;   // device count of list entries (at most npairs are read)
+  // optional query set (serving; list mode only): s1 index = query slot, distance to qout[slot][j]
+  const uint8_t* qseq;
+  const int64_t* qoff;
+  const int32_t* qlen;
+  int16_t* const* qout;
 };
 
 struct sw_pair_result_dev {

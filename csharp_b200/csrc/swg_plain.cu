@@ -174,9 +174,10 @@ __global__ void __launch_bounds__(128) plain_block_kernel(PlainJob J) {
     } else {
       pair_of(p, J, i, j);
     }
-    const uint8_t* s1 = J.seq + J.off[i];
+    const uint8_t* s1 = J.qoff ? J.qseq + J.qoff[i] : J.seq + J.off[i];
     const uint8_t* s2 = J.seq + J.off[j];
-    const int m = (int)(J.off[i + 1] - J.off[i]), n = (int)(J.off[j + 1] - J.off[j]);
+    const int m = J.qoff ? J.qlen[i] : (int)(J.off[i + 1] - J.off[i]);
+    const int n = (int)(J.off[j + 1] - J.off[j]);
     int16_t d;
     if (LOCAL) {
       if (m == 0 || n == 0) {
@@ -196,6 +197,10 @@ __global__ void __launch_bounds__(128) plain_block_kernel(PlainJob J) {
         c = *reinterpret_cast<const NwCnt::T*>(&r.c);
       }
       d = nw_distance(c, m, n, J.protein);
+    }
+    if (J.qoff) {
+      J.qout[i][j] = d;
+      continue;
     }
     J.out[(long long)(i - J.out_r0) * J.ld + (j - J.out_c0)] = d;
     if (J.mirror) J.out[(long long)(j - J.out_r0) * J.ld + (i - J.out_c0)] = d;

@@ -29,7 +29,7 @@ EXPORTS = [
     "sw_builtin_scoring_matrix", "sw_parse_fasta", "sw_partition_ranges", "sw_block_is_computed",
     "sw_write_full_matrix", "sw_write_ms_block", "sw_read_ms_block_dims", "sw_read_ms_block_values",
     "sw_measure_int_peak", "sw_set_option", "sw_compute_rank_blocks", "sw_query",
-    "sw_compute_block_static",
+    "sw_compute_block_static", "sw_submit_job", "sw_poll", "sw_serve_stats", "sw_serve_drain",
 ]
 
 
@@ -50,6 +50,17 @@ class sw_pair_result(C.Structure):
                 ("start1", C.c_int32), ("start2", C.c_int32), ("identity", C.c_int32),
                 ("similarity", C.c_int32), ("gaps", C.c_int32), ("length", C.c_int32),
                 ("distance", C.c_int16), ("reserved", C.c_int16)]
+
+
+class sw_job_info(C.Structure):
+    _fields_ = [("status", C.c_int32), ("queries", C.c_int32), ("pairs", C.c_int64), ("cells", C.c_int64),
+                ("submit_s", C.c_double), ("admit_s", C.c_double), ("done_s", C.c_double),
+                ("waves", C.c_int32), ("reserved", C.c_int32)]
+
+
+class sw_serve_counters(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("waves", C.c_int64), ("cells", C.c_int64),
+                ("active", C.c_int32), ("pending", C.c_int32), ("max_active", C.c_int32), ("reserved", C.c_int32)]
 
 
 class sw_ms_block_header(C.Structure):
@@ -101,6 +112,10 @@ def load():
         "sw_query": ([P, C.c_char_p, C.POINTER(I64)], I32),
         "sw_compute_block_static": ([C.POINTER(sw_config), P, P, I32, I32, I32, I32, I32, I32, P, I64,
                                      C.POINTER(I64), P], I32),
+        "sw_submit_job": ([P, P, P, I32, P, I64, C.POINTER(I64)], I32),
+        "sw_poll": ([P, I64, I32, C.POINTER(I32), C.POINTER(sw_job_info)], I32),
+        "sw_serve_stats": ([P, C.POINTER(sw_serve_counters)], I32),
+        "sw_serve_drain": ([P], I32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

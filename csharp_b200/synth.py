@@ -31,23 +31,21 @@ def _mutate(root, p_sub, p_indel, rng, alphabet, sub_cdf=None):
     ev = np.nonzero(rng.random(n) < p_indel)[0]
     if len(ev) == 0:
         return s
-    lens = rng.geometric(0.5, len(ev))
-    ins = rng.random(len(ev)) < 0.5
-    keep = np.ones(n, dtype=bool)
+    lens = rng.geometric(0.5, len(ev)).tolist()
+    ins = (rng.random(len(ev)) < 0.5).tolist()
+    # events inside a deletion are dropped; inserted codes are drawn event by event, in order
     pieces, last = [], 0
-    for p, ln, isi in zip(ev, lens, ins):
+    for p, ln, isi in zip(ev.tolist(), lens, ins):
         if p < last:
             continue
-        pieces.append(np.nonzero(keep[last:p])[0] + last)
+        pieces.append(s[last:p])
         if isi:
-            pieces.append(-1 - rng.integers(0, len(alphabet), ln))  # inserted codes, marked negative
+            pieces.append(rng.integers(0, len(alphabet), ln).astype(s.dtype))
             last = p
         else:
             last = min(n, p + ln)
-    pieces.append(np.arange(last, n))
-    idx = np.concatenate(pieces)
-    out = np.where(idx >= 0, s[np.clip(idx, 0, n - 1)], -1 - idx)
-    return out.astype(s.dtype)
+    pieces.append(s[last:n])
+    return np.concatenate(pieces)
 
 
 def _fit(seq, L, rng, alphabet_size):

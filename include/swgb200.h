@@ -190,6 +190,49 @@ int sw_compute_block_static(const sw_config* cfg, const uint8_t* d_residues,
                             int32_t is_diagonal, int16_t* d_out, int64_t ld_out,
                             int64_t* pairs_computed, void* stream);
 
+/* ---- serving: query batches against a device-resident database --------------------------- */
+/* No single reference call: the reference aligns one sequence set against itself.  Here the
+ * sequences uploaded with sw_upload_sequences form the database, and a job is a batch of queries
+ * each aligned (query = s1, database entry = s2, every entry) with the context's mode, distance
+ * rule and penalties, as the MS block handler aligns one row sequence against a column range
+ * (Salsa.SmithWatermanMS/Program.cs:341-375).  Jobs run asynchronously on one host scheduler
+ * thread per context: a job is admitted once query slots, query-arena bytes and device memory
+ * for its result are free ("serve_slots", "serve_arena_mb", "serve_memory_mb"), and every wave
+ * of kernels ("serve_wave_us" of estimated GPU time) takes a fair share of the work items of
+ * every admitted job, so jobs that arrive while others run join the next wave.  The options are
+ * read when the first job of a database is submitted. */
+typedef struct {
+  int32_t status;   /* SW_OK, or the error that ended the job */
+  int32_t queries;
+  int64_t pairs;    /* queries x database entries */
+  int64_t cells;    /* sum of query length x entry length */
+  double submit_s;  /* the scheduler's clock (seconds since it started) at submission, */
+  double admit_s;   /* at admission, */
+  double done_s;    /* and when the result was in the caller's buffer */
+  int32_t waves;    /* kernel waves the job's work took part in */
+  int32_t reserved;
+} sw_job_info;
+
+typedef struct {
+  int64_t submitted, completed, waves, cells;
+  int32_t active;      /* jobs admitted and not yet complete */
+  int32_t pending;     /* jobs waiting for admission */
+  int32_t max_active;  /* the most jobs admitted at once so far */
+  int32_t reserved;
+} sw_serve_counters;
+
+/* Submits nq queries (concatenated residues, nq + 1 offsets).  The queries are copied before the
+ * call returns; out (host, nq x ld_out Int16, ld_out >= database count) must stay valid until
+ * sw_poll reports the job done.  out[i * ld_out + j] = distance(align(query i, entry j)). */
+int sw_submit_job(sw_ctx* ctx, const uint8_t* q_concat, const int64_t* q_offsets, int32_t nq,
+                  int16_t* out, int64_t ld_out, int64_t* ticket);
+/* Waits up to timeout_ms (0 = just look) for the job; done = 1 once out holds every distance.
+ * info (optional) is filled when done; a ticket is forgotten after it was reported done. */
+int sw_poll(sw_ctx* ctx, int64_t ticket, int32_t timeout_ms, int32_t* done, sw_job_info* info);
+int sw_serve_stats(sw_ctx* ctx, sw_serve_counters* stats);
+/* Waits for every submitted job, then stops the scheduler (the next submit starts it again). */
+int sw_serve_drain(sw_ctx* ctx);
+
 /* ---- host-side library (formats the reference reads and writes) --------------------------- */
 /* ScoringMatrix.Load (Salsa.CoreTPL/Bio/Algorithms/ScoringMatrix.cs:145-196) over the matrix
  * text (header of column letters, then one "<letter> <scores...>" line per row; '#' comment
