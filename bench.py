@@ -35,6 +35,7 @@ WORKLOAD = dict(n=20000, median=400, sigma=0.6, lo=50, hi=1500, roots=200, seed=
 OPS_PER_CELL = 11      # algorithmic integer ops of one SW-Gotoh cell (E, F, H, running best)
 LANES_PER_OP = 2       # the engine's score registers hold two 16-bit lanes
 SHARES = 8             # steps per whole job: the shares of an 8-rank run
+SERVE = dict(db=100000, qmin=1, qmax=512, load=0.7, seconds=40.0, seed=6)
 
 
 def workload_sequences(n):
@@ -167,6 +168,63 @@ def run_reference_arm(a):
     return 0
 
 
+def serving(cs, device, seconds, load):
+    """Serving workload: a device-resident database of 100,000 DNA sequences (lognormal median
+    500, sigma 0.6, clipped 50-2,000), a Poisson stream of query batches (sizes log-uniform in
+    1-512, query lengths from the same distribution) aligned SW-Gotoh against the whole database.
+    The arrival rate is set from a calibration job so that the offered load is `load` of the GPU.
+    Latency of a job = its completion (results in host memory) minus its submission."""
+    from csharp_b200 import pack_sequences, synth
+    db = synth.config5_db(SERVE["db"])
+    concat, off = pack_sequences(db)
+    dblen = float(off[-1])
+    rng = np.random.default_rng(SERVE["seed"])
+    pool = synth.dna_family(4000, 40, synth.lognormal_lengths(4000, 500, 0.6, 50, 2000, rng), SERVE["seed"])
+    eng = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4, device=device)
+    eng.upload(concat=concat, offsets=off)
+    # calibration (also builds the database state): 64 queries alone
+    cal = [pool[k].tobytes() for k in range(64)]
+    r = eng.wait(eng.submit(cal))
+    cal_rate = r["cells"] / max(r["done_s"] - r["admit_s"], 1e-9)
+    mean_q = (SERVE["qmax"] - SERVE["qmin"]) / np.log(SERVE["qmax"] / SERVE["qmin"])
+    mean_cells = mean_q * float(np.mean([len(p) for p in pool])) * dblen
+    lam = load * cal_rate / mean_cells           # batches per second
+    arrivals = np.cumsum(rng.exponential(1.0 / lam, 10000))
+    arrivals = arrivals[arrivals < seconds]
+    sizes = np.exp(rng.uniform(np.log(SERVE["qmin"]), np.log(SERVE["qmax"] + 1), len(arrivals))).astype(int)
+    sizes = np.clip(sizes, SERVE["qmin"], SERVE["qmax"])
+    batches = [[pool[k].tobytes() for k in rng.integers(0, len(pool), n)] for n in sizes]
+    outstanding, results = {}, []
+    t0 = time.monotonic()
+    for at, b in zip(arrivals, batches):
+        while True:
+            now = time.monotonic() - t0
+            if now >= at:
+                break
+            time.sleep(min(0.005, at - now))
+        outstanding[eng.submit(b)] = len(b)
+        for t in list(outstanding):
+            x = eng.poll(t, 0)
+            if x is not None:
+                results.append(x)
+                del outstanding[t]
+    for t in list(outstanding):
+        results.append(eng.wait(t))
+    st = eng.serve_stats()
+    lat = np.array([x["done_s"] - x["submit_s"] for x in results]) * 1e3
+    cells = float(sum(x["cells"] for x in results))
+    span = max(x["done_s"] for x in results) - min(x["submit_s"] for x in results)
+    ok = all(x["status"] == 0 for x in results)
+    eng.close()
+    return {"workload": "cfg5 serving: 100,000 DNA database lognormal(median 500, sigma 0.6) clipped 50-2000, "
+                        "Poisson batches of 1-512 queries (log-uniform sizes), EDNAFULL, open 16 / extend 4",
+            "jobs": len(results), "queries": int(sizes.sum()), "offered_load": load,
+            "arrival_rate_per_s": round(lam, 3), "p50_ms": round(float(np.percentile(lat, 50)), 1),
+            "p99_ms": round(float(np.percentile(lat, 99)), 1), "mean_ms": round(float(lat.mean()), 1),
+            "gcups": round(cells / span / 1e9, 1), "calibration_gcups": round(cal_rate / 1e9, 1),
+            "max_admitted": st["max_active"], "waves": st["waves"], "all_ok": ok}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -178,7 +236,13 @@ def main():
     ap.add_argument("--ref-step-seconds", type=float, default=6.0)
     ap.add_argument("--skip-extras", action="store_true", help="headline only (profiling runs)")
     ap.add_argument("--rows-per-lane", type=int, default=0, help="engine rows per lane (0 = per query)")
+    ap.add_argument("--serving-only", action="store_true", help="only the serving workload (one JSON line)")
+    ap.add_argument("--serve-seconds", type=float, default=SERVE["seconds"])
     a = ap.parse_args()
+    if a.serving_only:
+        import csharp_b200 as cs
+        print(json.dumps({"serving": serving(cs, 0, a.serve_seconds, SERVE["load"])}))
+        return 0
     if a.impl == "reference":
         return run_reference_arm(a)
 
@@ -356,6 +420,7 @@ def main():
                                       "speedup": round(times["plain"] / times["batched"], 2),
                                       "identical": bool(np.array_equal(a2[offd], a3[offd]))}
         sub.close()
+        result["serving"] = serving(cs, local, a.serve_seconds, SERVE["load"])
     if rank == 0:
         print(json.dumps(result))
     if world > 1:

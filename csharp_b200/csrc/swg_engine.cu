@@ -984,20 +984,21 @@ class EngineImpl : public Engine {
 // 16-bit lanes at 16 rows per lane, and cells per second of the 32-bit lanes, on B200.
 constexpr double kRate16 = 1.45e12;
 constexpr double kRate32 = 1.4e11;
-constexpr int kQueryChunk = 512;
+constexpr int kQueryChunk = 256;
 
 class QueryRunnerImpl : public QueryRunner {
  public:
   ~QueryRunnerImpl() override {
-    cudaFree(d_qtab_); cudaFree(d_qflag_); cudaFree(d_scratch_);
+    cudaFree(d_qtab_); cudaFree(d_qflag_);
     for (auto& w : wb_) {
       cudaFree(w.d_items); cudaFree(w.d_counters); cudaFree(w.d_stats); cudaFree(w.d_rerun);
-      cudaFree(w.d_rerun_count); cudaFreeHost(w.h_items); cudaFreeHost(w.h_rerun);
-    }
-    if (fork_) cudaEventDestroy(fork_);
-    for (int x = 0; x < kNumK; x++) {
-      if (side_[x]) cudaStreamDestroy(side_[x]);
-      if (join_[x]) cudaEventDestroy(join_[x]);
+      cudaFree(w.d_rerun_count); cudaFreeHost(w.h_items); cudaFreeHost(w.h_rerun); cudaFree(w.d_scratch);
+      if (w.fork) cudaEventDestroy(w.fork);
+      if (w.plain_done) cudaEventDestroy(w.plain_done);
+      for (int x = 0; x < kNumK; x++) {
+        if (w.side[x]) cudaStreamDestroy(w.side[x]);
+        if (w.join[x]) cudaEventDestroy(w.join[x]);
+      }
     }
   }
 
@@ -1016,11 +1017,14 @@ class QueryRunnerImpl : public QueryRunner {
       chunk_lo_.push_back(c0); chunk_hi_.push_back(c1); chunk_sum_.push_back(sum); chunk_max_.push_back(mx);
       total_len_ += sum;
     }
-    if (fork_ == nullptr) {
-      if (cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming) != cudaSuccess) { *msg = "event create"; return SW_E_CUDA; }
+    for (auto& w : wb_) {
+      if (cudaEventCreateWithFlags(&w.fork, cudaEventDisableTiming) != cudaSuccess ||
+          cudaEventCreateWithFlags(&w.plain_done, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError(); *msg = "event create"; return SW_E_CUDA;
+      }
       for (int x = 0; x < kNumK; x++)
-        if (cudaStreamCreateWithFlags(&side_[x], cudaStreamNonBlocking) != cudaSuccess ||
-            cudaEventCreateWithFlags(&join_[x], cudaEventDisableTiming) != cudaSuccess) {
+        if (cudaStreamCreateWithFlags(&w.side[x], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&w.join[x], cudaEventDisableTiming) != cudaSuccess) {
           cudaGetLastError(); *msg = "stream create"; return SW_E_CUDA;
         }
     }
@@ -1140,13 +1144,13 @@ class QueryRunnerImpl : public QueryRunner {
       scr_off[x] = scr_words;
       if (ls[x].max_passes > 1) scr_words += (size_t)grid[x] * warps_of(ls[x].K) * B_.maxcol * kScrWords;
     }
-    if (scr_words * 4 > scratch_bytes_) {
-      // earlier waves may still use the old scratch: cudaFree waits for the device
-      cudaFree(d_scratch_);
-      d_scratch_ = nullptr;
-      scratch_bytes_ = 0;
-      if (cudaMalloc(&d_scratch_, scr_words * 4) != cudaSuccess) { cudaGetLastError(); *msg = "cudaMalloc pass scratch"; return SW_E_OOM; }
-      scratch_bytes_ = scr_words * 4;
+    if (scr_words * 4 > W.scratch_bytes) {
+      // the earlier wave of this buffer is done; the other buffer's wave may run (own scratch)
+      cudaFree(W.d_scratch);
+      W.d_scratch = nullptr;
+      W.scratch_bytes = 0;
+      if (cudaMalloc(&W.d_scratch, scr_words * 4) != cudaSuccess) { cudaGetLastError(); *msg = "cudaMalloc pass scratch"; return SW_E_OOM; }
+      W.scratch_bytes = scr_words * 4;
     }
     cudaError_t e;
     if (n16 && (e = cudaMemcpyAsync(W.d_items, W.h_items, n16 * sizeof(int4), cudaMemcpyHostToDevice, st)) != cudaSuccess) return cuda_err(e, msg);
@@ -1166,19 +1170,19 @@ class QueryRunnerImpl : public QueryRunner {
       J.qmode = 1; J.qseq = T.qseq; J.qoff = T.qoff; J.qlen = T.qlen; J.qout = T.qout;
       J.qtab = d_qtab_; J.qflag = d_qflag_;
       const bool fork = ls.size() > 1;
-      if (fork && (e = cudaEventRecord(fork_, st)) != cudaSuccess) return cuda_err(e, msg);
+      if (fork && (e = cudaEventRecord(W.fork, st)) != cudaSuccess) return cuda_err(e, msg);
       for (size_t x = 0; x < ls.size(); x++) {
-        cudaStream_t s2 = fork ? side_[x] : st;
-        if (fork && (e = cudaStreamWaitEvent(s2, fork_, 0)) != cudaSuccess) return cuda_err(e, msg);
+        cudaStream_t s2 = fork ? W.side[x] : st;
+        if (fork && (e = cudaStreamWaitEvent(s2, W.fork, 0)) != cudaSuccess) return cuda_err(e, msg);
         J.items = W.d_items + ls[x].offset;
         J.nitems = ls[x].count;
         J.counter = W.d_counters + ls[x].b;
         J.mpad = ls[x].mpad;
-        J.scratch = d_scratch_ + scr_off[x];
+        J.scratch = W.d_scratch + scr_off[x];
         if ((e = launch_engine_k(ls[x].K, J, grid[x], smem[x], s2)) != cudaSuccess) return cuda_err(e, msg);
         if (fork) {
-          if ((e = cudaEventRecord(join_[x], s2)) != cudaSuccess) return cuda_err(e, msg);
-          if ((e = cudaStreamWaitEvent(st, join_[x], 0)) != cudaSuccess) return cuda_err(e, msg);
+          if ((e = cudaEventRecord(W.join[x], s2)) != cudaSuccess) return cuda_err(e, msg);
+          if ((e = cudaStreamWaitEvent(st, W.join[x], 0)) != cudaSuccess) return cuda_err(e, msg);
         }
       }
     }
@@ -1193,7 +1197,12 @@ class QueryRunnerImpl : public QueryRunner {
     R.carry = B_.d_carry;
     R.qseq = T.qseq; R.qoff = T.qoff; R.qlen = T.qlen; R.qout = T.qout;
     const int g = big > 0 ? (int)(B_.carry_threads / 128) : P_.sms;
+    // the 32-bit lanes' scratch is shared: after the other buffer's 32-bit kernel
+    WaveBuf& other = wb_[(buf & 1) ^ 1];
+    if (other.plain_used && (e = cudaStreamWaitEvent(st, other.plain_done, 0)) != cudaSuccess) return cuda_err(e, msg);
     if ((e = launch_plain_block(R, g, 128, st)) != cudaSuccess) return cuda_err(e, msg);
+    if ((e = cudaEventRecord(W.plain_done, st)) != cudaSuccess) return cuda_err(e, msg);
+    W.plain_used = true;
     return SW_OK;
   }
 
@@ -1208,6 +1217,13 @@ class QueryRunnerImpl : public QueryRunner {
     int* d_counters = nullptr;
     int* d_rerun_count = nullptr;
     unsigned long long* d_stats = nullptr;
+    // waves of the two buffers may run at once: each has its own scratch, streams and events
+    uint32_t* d_scratch = nullptr;
+    size_t scratch_bytes = 0;
+    cudaEvent_t fork = nullptr, plain_done = nullptr;
+    bool plain_used = false;
+    cudaStream_t side[kNumK] = {};
+    cudaEvent_t join[kNumK] = {};
   };
 
   static int cuda_err(cudaError_t e, std::string* msg) {
@@ -1257,12 +1273,7 @@ class QueryRunnerImpl : public QueryRunner {
   std::vector<int64_t> chunk_sum_;
   int32_t* d_qtab_ = nullptr;
   uint32_t* d_qflag_ = nullptr;
-  uint32_t* d_scratch_ = nullptr;
-  size_t scratch_bytes_ = 0;
   WaveBuf wb_[2];
-  cudaEvent_t fork_ = nullptr;
-  cudaStream_t side_[kNumK] = {};
-  cudaEvent_t join_[kNumK] = {};
 };
 
 }  // namespace

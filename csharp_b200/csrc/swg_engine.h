@@ -83,6 +83,7 @@ class QueryRunner {
   // Useful cells of one query of m residues against the whole database.
   virtual int64_t query_cells(int m) const = 0;
   // Enqueues one wave on st (wave buffer `buf`, 0 or 1, reused once its earlier wave is done).
+  // Waves of the two buffers may be enqueued on different streams and overlap on the GPU.
   virtual int enqueue(int buf, const std::vector<QueryItem>& items, const QueryTables& T,
                       cudaStream_t st, std::string* msg) = 0;
 };

@@ -8,8 +8,9 @@
 //               enqueue of the persistent per-K kernels over items of every admitted job: each
 //               job gets an equal share of the wave's time budget, the rest goes to whoever still
 //               has items, so a small job admitted while a large one runs finishes in its first
-//               wave or two instead of queueing behind it.  Two waves are in flight at a time so
-//               the GPU never idles between them;
+//               wave or two instead of queueing behind it.  Two waves are in flight at a time,
+//               on two streams with their own scratch, so the next wave's CTAs take the SMs
+//               that the current wave's tail leaves idle;
 //   copying  -> its last wave finished: a second thread copies the result to the caller's buffer
 //               and frees the job's device memory, slots and arena bytes;
 //   done     -> sw_poll reports it and forgets the ticket.
@@ -82,7 +83,8 @@ class ServerImpl : public Server {
     cudaMemGetInfo(&free_b, &total_b);
     budget_ = opt.memory_bytes ? opt.memory_bytes : free_b / 2;
     const int S = std::max(1, opt.slots);
-    if (cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking) != cudaSuccess ||
+    if (cudaStreamCreateWithFlags(&st_[0], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&st_[1], cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&copy_st_, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&up_st_, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&d_arena_, std::max<size_t>(opt.arena_bytes, 64) + 64) != cudaSuccess ||
@@ -244,7 +246,8 @@ class ServerImpl : public Server {
       if (a->second > need) arena_free_[a->first + need] = a->second - need;
       arena_free_.erase(a);
       j->out_bytes = std::max<size_t>((size_t)j->nq * db_count_ * 2, 2);
-      if (cudaMallocAsync(reinterpret_cast<void**>(&j->d_out), j->out_bytes, st_) != cudaSuccess) {
+      // allocated on the upload stream, which is synchronized below: usable by both wave streams
+      if (cudaMallocAsync(reinterpret_cast<void**>(&j->d_out), j->out_bytes, up_st_) != cudaSuccess) {
         cudaGetLastError();
         release_locked(j);
         j->info.status = SW_E_OOM;
@@ -346,9 +349,9 @@ class ServerImpl : public Server {
     T.qout = d_qout_;
     std::vector<QueryItem> items;
     items.swap(wave_items_);
-    int rc = runner_->enqueue(w.buf, items, T, st_, msg);
+    int rc = runner_->enqueue(w.buf, items, T, st_[w.buf], msg);
     if (rc) return rc;
-    if (cudaEventRecord(w.ev, st_) != cudaSuccess) { *msg = "wave event"; return SW_E_CUDA; }
+    if (cudaEventRecord(w.ev, st_[w.buf]) != cudaSuccess) { *msg = "wave event"; return SW_E_CUDA; }
     return SW_OK;
   }
 
@@ -421,7 +424,8 @@ class ServerImpl : public Server {
 
   void fail_all(int rc, const std::string& msg) {
     cudaGetLastError();
-    cudaStreamSynchronize(st_);  // nothing may still use the memory the copy thread frees
+    cudaStreamSynchronize(st_[0]);  // nothing may still use the memory the copy thread frees
+    cudaStreamSynchronize(st_[1]);
     cudaGetLastError();
     std::lock_guard<std::mutex> lk(mu_);
     error_ = rc;
@@ -460,16 +464,16 @@ class ServerImpl : public Server {
     }
     if (copier_.joinable()) copier_.join();
     cudaSetDevice(device_);
-    if (st_) cudaStreamSynchronize(st_);
+    for (cudaStream_t s : st_) if (s) cudaStreamSynchronize(s);
     if (copy_st_) cudaStreamSynchronize(copy_st_);
     runner_.reset();
     for (int b = 0; b < 2; b++) if (wave_ev_[b]) cudaEventDestroy(wave_ev_[b]);
     cudaFree(d_arena_); cudaFree(d_qoff_); cudaFree(d_qlen_); cudaFree(d_qout_);
     cudaFreeHost(h_qoff_); cudaFreeHost(h_qlen_); cudaFreeHost(h_qout_);
-    if (st_) cudaStreamDestroy(st_);
+    for (cudaStream_t& s : st_) { if (s) cudaStreamDestroy(s); s = nullptr; }
     if (copy_st_) cudaStreamDestroy(copy_st_);
     if (up_st_) cudaStreamDestroy(up_st_);
-    st_ = copy_st_ = up_st_ = nullptr;
+    copy_st_ = up_st_ = nullptr;
   }
 
   int device_ = 0;
@@ -478,7 +482,8 @@ class ServerImpl : public Server {
   size_t budget_ = 0, in_use_ = 0;
   std::chrono::steady_clock::time_point t0_;
   std::unique_ptr<QueryRunner> runner_;
-  cudaStream_t st_ = nullptr, copy_st_ = nullptr, up_st_ = nullptr;
+  cudaStream_t st_[2] = {nullptr, nullptr};  // wave streams: the two buffers' waves overlap
+  cudaStream_t copy_st_ = nullptr, up_st_ = nullptr;
   cudaEvent_t wave_ev_[2] = {nullptr, nullptr};
   uint8_t* d_arena_ = nullptr;
   int64_t* d_qoff_ = nullptr;

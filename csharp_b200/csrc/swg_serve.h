@@ -13,7 +13,7 @@ struct ServeOptions {
   size_t memory_bytes = 0;          // device bytes for admitted jobs' results (0: half the free memory)
   size_t arena_bytes = 64u << 20;   // device bytes for admitted jobs' query residues
   int slots = 8192;                 // queries admitted at once
-  double wave_seconds = 0.04;       // estimated GPU time of one wave
+  double wave_seconds = 0.1;        // estimated GPU time of one wave
 };
 
 class Server {
