@@ -117,11 +117,20 @@ __device__ __forceinline__ uint32_t vmax2(uint32_t a, uint32_t b, bool& hi, bool
   return r;
 }
 
+// x * 65536 + y as one multiply-add (the FMA pipe has room; the ALU pipe is the bound).
+__device__ __forceinline__ uint32_t mad_hi16(uint32_t x, uint32_t y) {
+  uint32_t r;
+  asm("mad.lo.u32 %0, %1, 65536, %2;" : "=r"(r) : "r"(x), "r"(y));
+  return r;
+}
+
 // One warp, query rows in registers, two database sequences (lanes A/B) in lockstep.
-// prof: shared-memory profile planes, plane(c, kind) at ((c*3+kind) * mpad) words, rows stored
+// prof: shared-memory profile planes, plane(c, kind) at ((c*NP+kind) * mpad) words, rows stored
 // per pass in lane-interleaved groups of 4 so each lane's 128-bit load hits distinct banks.
+// NP = 3: score + o, (score + o) << 16, counted flag; NP = 2 (large alphabets, where three
+// planes would not fit shared memory): score + o and flag, lane B's word shifted by a multiply-add.
 // ca/cb: shared-memory code buffers with 32 pad entries before column 0.
-template <int K>
+template <int K, int NP>
 __device__ __forceinline__ void align_two(const uint32_t* __restrict__ prof, int mpad, int passes,
                                           const uint8_t* __restrict__ ca,
                                           const uint8_t* __restrict__ cb, int ncols,
@@ -133,7 +142,7 @@ __device__ __forceinline__ void align_two(const uint32_t* __restrict__ prof, int
   const uint32_t sent2 = (uint32_t)(J.bias - J.o - J.e) * 0x10001u;  // -infinity + bias
   const uint32_t best0 = (uint32_t)(J.bias - 1) * 0x10001u;          // below any V
   const uint32_t vo_top = (uint32_t)(J.bias - J.o) * 0x10001u;        // V(0,j) - o + bias
-  const int plane = 3 * mpad;
+  const int plane = NP * mpad;
   bestA = bestB = -1;
   rowA = rowB = 0;
   cntA = cntB = 0u;
@@ -186,13 +195,13 @@ __device__ __forceinline__ void align_two(const uint32_t* __restrict__ prof, int
         xa = ca[col]; xb = cb[col];
       }
       const uint32_t* pla = pl + xa * plane;
-      const uint32_t* phb = pl + xb * plane + mpad;
-      const uint32_t* pma = pl + xa * plane + 2 * mpad;
-      const uint32_t* pmb = pl + xb * plane + 2 * mpad;
+      const uint32_t* phb = pl + xb * plane + (NP == 3 ? mpad : 0);
+      const uint32_t* pma = pl + xa * plane + (NP - 1) * mpad;
+      const uint32_t* pmb = pl + xb * plane + (NP - 1) * mpad;
       // one row of the lane's block: the cell (row r, column col) of both pairs
       auto cell = [&](const int r, const uint32_t pl_r, const uint32_t ph_r, const uint32_t ma_r,
                       const uint32_t mb_r) {
-        const uint32_t F = VOD + pl_r + ph_r;
+        const uint32_t F = (NP == 3) ? VOD + pl_r + ph_r : mad_hi16(ph_r, VOD + pl_r);
         const uint32_t cfA = cdA + ma_r + 0x10000u;
         const uint32_t cfB = cdB + mb_r + 0x10000u;
         bool hiB, loA;
@@ -286,13 +295,13 @@ __device__ __forceinline__ void emit(const EngineJob& J, int q, int d, int16_t d
   if (J.mode != kModeSwgMs) J.out[(long long)d * J.ld + q] = dist;
 }
 
-template <int K>
+template <int K, int NP>
 __global__ void __launch_bounds__(warps_of(K) * 32, ctas_of(K)) engine_kernel(EngineJob J) {
   constexpr int kEngWarps = warps_of(K);
   extern __shared__ __align__(16) uint8_t smem[];
   uint32_t* prof = reinterpret_cast<uint32_t*>(smem);
   const int A1 = J.A + 1;
-  int* list = reinterpret_cast<int*>(smem + (size_t)A1 * 3 * J.mpad * 4);
+  int* list = reinterpret_cast<int*>(smem + (size_t)A1 * NP * J.mpad * 4);
   uint8_t* codes = reinterpret_cast<uint8_t*>(list + kMaxChunk);
   const int cbuf = 64 + ((J.maxcol + 31) / 32) * 32;
   __shared__ int s_item, s_count, s_next, s_q;
@@ -328,10 +337,10 @@ __global__ void __launch_bounds__(warps_of(K) * 32, ctas_of(K)) engine_kernel(En
                                                      : (K & ~3) * 32 + t * 2 + (rr & 1));
         const int a = (i < m) ? (int)qc[i] : pad;
         const int v = ptab[a * A1 + c];
-        uint32_t* pc = prof + (size_t)c * 3 * J.mpad;
+        uint32_t* pc = prof + (size_t)c * NP * J.mpad;
         pc[pos] = (uint32_t)v;
-        pc[J.mpad + pos] = (uint32_t)v << 16;
-        pc[2 * J.mpad + pos] = ftab[a * A1 + c];
+        if (NP == 3) pc[J.mpad + pos] = (uint32_t)v << 16;
+        pc[(NP - 1) * J.mpad + pos] = ftab[a * A1 + c];
       }
     }
     if (threadIdx.x == 0) { s_q = q; s_count = 0; s_next = 0; }
@@ -378,7 +387,7 @@ __global__ void __launch_bounds__(warps_of(K) * 32, ctas_of(K)) engine_kernel(En
       int bA, rA, bB, rB;
       uint32_t cA, cB;
       if (m > 0 && ncols > 0) {
-        align_two<K>(prof, J.mpad, passes, ca, cb, ncols, J, scr, lane, bA, rA, cA, bB, rB, cB);
+        align_two<K, NP>(prof, J.mpad, passes, ca, cb, ncols, J, scr, lane, bA, rA, cA, bB, rB, cB);
       } else {
         bA = bB = 0; rA = rB = 0; cA = cB = 0u;
       }
@@ -423,9 +432,13 @@ namespace {
 constexpr int kNumK = 7;
 constexpr int kKs[kNumK] = {4, 6, 8, 10, 12, 14, 16};
 
+// Largest alphabet of the 16-bit lanes (two-plane profiles beyond 8 letters).
+constexpr int kMaxAlpha16 = 32;
+int planes_of(int A) { return A > 8 ? 2 : 3; }
+
 size_t engine_smem(int A, int mpad, int maxcol, int K) {
   const int cbuf = 64 + ((maxcol + 31) / 32) * 32;
-  return (size_t)(A + 1) * 3 * mpad * 4 + kMaxChunk * 4 + (size_t)warps_of(K) * 2 * cbuf;
+  return (size_t)(A + 1) * planes_of(A) * mpad * 4 + kMaxChunk * 4 + (size_t)warps_of(K) * 2 * cbuf;
 }
 
 __global__ void set_int_kernel(int* p, int v) { *p = v; }
@@ -444,25 +457,32 @@ auto with_k(int K, Fn fn) {
   }
 }
 
-cudaError_t allow_smem_k(int K, size_t smem) {
+// The kernel instantiation for K rows per lane and the planes of alphabet A.
+template <class Fn>
+auto with_kp(int K, int A, Fn fn) {
   return with_k(K, [&](auto k) {
-    return cudaFuncSetAttribute(engine_kernel<decltype(k)::value>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (planes_of(A) == 3) return fn(engine_kernel<decltype(k)::value, 3>, warps_of(decltype(k)::value) * 32);
+    return fn(engine_kernel<decltype(k)::value, 2>, warps_of(decltype(k)::value) * 32);
+  });
+}
+
+cudaError_t allow_smem_k(int K, int A, size_t smem) {
+  return with_kp(K, A, [&](auto kern, int) {
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   });
 }
 
 cudaError_t launch_engine_k(int K, const EngineJob& J, int grid, size_t smem, cudaStream_t st) {
-  return with_k(K, [&](auto k) {
-    engine_kernel<decltype(k)::value><<<grid, warps_of(decltype(k)::value) * 32, smem, st>>>(J);
+  return with_kp(K, J.A, [&](auto kern, int threads) {
+    kern<<<grid, threads, smem, st>>>(J);
     return cudaGetLastError();
   });
 }
 
-int occupancy_k(int K, size_t smem) {
-  return with_k(K, [&](auto k) {
+int occupancy_k(int K, int A, size_t smem) {
+  return with_kp(K, A, [&](auto kern, int threads) {
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel<decltype(k)::value>,
-                                                  warps_of(decltype(k)::value) * 32, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem);
     return n;
   });
 }
@@ -570,7 +590,7 @@ int build_base(Base& B, const EngineParams& P, std::string* msg) {
   if (cudaMalloc(&B.d_carry, plain_carry_bytes(P.mode == kModeNw ? kModeNw : kModeSwgMpi, B.carry_threads, B.maxcol)) != cudaSuccess) {
     cudaGetLastError(); B.d_carry = nullptr; *msg = "cudaMalloc 32-bit lane scratch"; return SW_E_OOM;
   }
-  if (B.alpha > 8 || P.mode == kModeNw || P.lanes == SW_LANES_32) return SW_OK;
+  if (B.alpha > kMaxAlpha16 || P.mode == kModeNw || P.lanes == SW_LANES_32) return SW_OK;
   const int A = B.alpha, A1 = A + 1;
   int maxS = 0, minS = 0;
   for (int a : letters)
@@ -760,7 +780,7 @@ class EngineImpl : public Engine {
     for (int r = 0; r < P.ranks; r++)
       for (int x = starts[r]; x <= ends[r]; x++) blk[x] = r;
     int rc;
-    pl.plain_only = B.alpha > 8 || P.mode == kModeNw || P.lanes == SW_LANES_32;
+    pl.plain_only = B.alpha > kMaxAlpha16 || P.mode == kModeNw || P.lanes == SW_LANES_32;
     std::vector<int2> big;
     if (pl.plain_only) {
       for (int q = key.row_lo; q <= key.row_hi; q++)
@@ -798,6 +818,8 @@ class EngineImpl : public Engine {
       const int m = B.len[q];
       int K, passes;
       choose_k(m, opt_.k_override, &K, &passes);
+      // a profile beyond shared memory (long queries, large alphabets): 32-bit lanes
+      const bool fits = engine_smem(A, passes * 32 * K, B.maxcol, K) <= 227 * 1024;
       const int bi = (int)(std::find(std::begin(kKs), std::end(kKs), K) - std::begin(kKs));
       const int bq = blk[q];
       for (int c = 0; c < nchunks; c++) {
@@ -826,7 +848,7 @@ class EngineImpl : public Engine {
         pl.npairs += cnt;
         pl.ncells += (int64_t)((double)m * lsum);
         const int mn = std::min(m, cmaxlen[c]);
-        if ((long)B.max_s * (mn + 1) + B.bias > 32767) {
+        if (!fits || (long)B.max_s * (mn + 1) + B.bias > 32767) {
           // 16-bit lanes cannot hold this item's scores: its pairs go to 32-bit lanes
           for (int k = c * chunk; k < std::min(N, (c + 1) * chunk); k++) {
             const int d = B.sorted_h[k];
@@ -861,8 +883,8 @@ class EngineImpl : public Engine {
       if (bn.items.empty()) continue;
       bn.smem = engine_smem(A, bn.mpad, B.maxcol, bn.K);
       if (bn.smem > 227 * 1024) { *msg = "query profile exceeds shared memory"; return SW_E_UNSUPPORTED; }
-      if (allow_smem_k(bn.K, bn.smem) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
-      const int occ = std::max(1, occupancy_k(bn.K, bn.smem));
+      if (allow_smem_k(bn.K, A, bn.smem) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
+      const int occ = std::max(1, occupancy_k(bn.K, A, bn.smem));
       bn.grid = (int)std::min<long>((long)P.sms * occ, (long)bn.items.size());
       bn.scratch_off = scr_words;
       if (bn.max_passes > 1) scr_words += (size_t)bn.grid * warps_of(bn.K) * B.maxcol * kScrWords;
@@ -1007,7 +1029,7 @@ class QueryRunnerImpl : public QueryRunner {
     int rc = build_base(B_, P, msg);
     if (rc) return rc;
     N_ = P.nseq;
-    lanes16_ = !(B_.alpha > 8 || P.mode == kModeNw || P.lanes == SW_LANES_32 || B_.alpha == 0);
+    lanes16_ = !(B_.alpha > kMaxAlpha16 || P.mode == kModeNw || P.lanes == SW_LANES_32 || B_.alpha == 0);
     // database chunks in length order
     for (int c0 = 0; c0 < N_; c0 += kQueryChunk) {
       const int c1 = std::min(N_, c0 + kQueryChunk);
@@ -1138,8 +1160,8 @@ class QueryRunnerImpl : public QueryRunner {
     for (size_t x = 0; x < ls.size(); x++) {
       smem[x] = engine_smem(A, ls[x].mpad, B_.maxcol, ls[x].K);
       if (smem[x] > 227 * 1024) { *msg = "query profile exceeds shared memory"; return SW_E_UNSUPPORTED; }
-      if (allow_smem_k(ls[x].K, smem[x]) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
-      const int occ = std::max(1, occupancy_k(ls[x].K, smem[x]));
+      if (allow_smem_k(ls[x].K, A, smem[x]) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
+      const int occ = std::max(1, occupancy_k(ls[x].K, A, smem[x]));
       grid[x] = std::min(P_.sms * occ, ls[x].count);
       scr_off[x] = scr_words;
       if (ls[x].max_passes > 1) scr_words += (size_t)grid[x] * warps_of(ls[x].K) * B_.maxcol * kScrWords;

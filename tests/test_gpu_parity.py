@@ -239,3 +239,21 @@ def test_engine_accounts_for_every_pair(cs):
     _, pairs, _ = eng.all_pairs(1)
     assert eng.query("items") == eng.query("planned_items") > 0
     assert eng.query("lane16_pairs") + eng.rerun_count() == pairs
+
+
+def test_protein_engine_uses_16bit_lanes_and_matches_oracle(cs, oracle_mod):
+    """20-letter alphabet: two-plane profiles in the 16-bit lanes; a 2,500-residue query whose
+    profile exceeds shared memory goes to 32-bit lanes.  Every pair against the oracle."""
+    from csharp_b200 import synth
+    sc = cs.ScoringMatrix.Load("BLOSUM62").Scores
+    rng = np.random.default_rng(44)
+    lens = np.concatenate([rng.integers(100, 1001, 70), [0, 1, 2500]])
+    seqs = [s.tobytes() for s in synth.protein_family(len(lens), 6, lens, 44, sc)]
+    eng = cs.Engine(cs.ScoringMatrix.Load("BLOSUM62"), 10, 1, alignment_type=0).upload(seqs)
+    full, pairs, _ = eng.all_pairs(1)
+    assert eng.query("alphabet") > 8 and eng.query("lane16_pairs") > 0
+    assert eng.rerun_count() >= len(seqs) - 1  # the long query's pairs (it is s1 of every pair j < i)
+    N = len(seqs)
+    pr = np.array([(i, j) for i in range(N) for j in range(i)], dtype=np.int32)
+    want = _oracle_distances(oracle_mod, seqs, pr, "BLOSUM62", 10.0, 1.0, atype=0)
+    np.testing.assert_array_equal(full[pr[:, 0], pr[:, 1]], want)
