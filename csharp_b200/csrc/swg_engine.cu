@@ -42,11 +42,14 @@ namespace swg {
 // SM): up to 8 rows fit 128 registers (2 CTAs of 8 warps), 10-12 rows fit 168 (1 CTA of 12
 // warps), 14-16 rows need up to 255 (1 CTA of 8 warps).  Measured on B200, 12 warps run the
 // 10- and 12-row kernels 16% faster than 8.
+// NW carries twice the counter words and spills a little at these register caps; measured on
+// B200, the occupancy still pays more than the spills cost (8 warps with no spill: -9 %).
 constexpr int kMaxWarps = 12;
-__host__ __device__ constexpr int warps_of(int K) { return K <= 8 ? 8 : K <= 12 ? 12 : 8; }
-__host__ __device__ constexpr int ctas_of(int K) { return K <= 8 ? 2 : 1; }
+__host__ __device__ constexpr int warps_of(int K, bool nw = false) { return K <= 8 ? 8 : K <= 12 ? 12 : 8; }
+__host__ __device__ constexpr int ctas_of(int K, bool nw = false) { return K <= 8 ? 2 : 1; }
 constexpr int kMaxChunk = 1024;
-constexpr int kScrWords = 8;  // words of carried state per column in the pass scratch
+constexpr int kScrWords = 8;    // words of carried state per column in the pass scratch (SW)
+constexpr int kScrWordsNw = 12; // NW: V, G and two counter words per state and lane
 
 struct EngineJob {
   const uint8_t* code;      // dense residue codes (pad code = A), same offsets as the residues
@@ -61,12 +64,13 @@ struct EngineJob {
   int mode, ranks, nseq, rb_a, rb_b;
   int16_t* out;
   long long ld;
-  uint32_t* scratch;        // per (CTA, warp) slot: maxcol * kScrWords words
+  uint32_t* scratch;        // per (CTA, warp) slot: maxcol * (kScrWords or kScrWordsNw) words
   int maxcol;               // longest database sequence
   int2* rerun;              // pairs to redo with 32-bit lanes
   int* rerun_count;
   int rerun_cap;
   int mpad;                 // profile rows staged (passes * 32 * K of the bin)
+  int protein;              // NW distance rule: similarity over the full length
   unsigned long long* stats; // [0] items taken, [1] pairs finished in 16-bit lanes, [2] tripped
   // Query mode (serving): s1 is query slot q of a separate set, s2 every database entry of the
   // chunk, the distance goes to qout[q][d].  Raw residue bytes index qtab/qflag (row 127 = pad).
@@ -275,6 +279,193 @@ __device__ __forceinline__ void align_two(const uint32_t* __restrict__ prof, int
   }
 }
 
+// NW (global) counterpart of align_two: V = max(F, G, H) without the 0 floor, boundaries
+// V(i,0) = -o-(i-1)e and V(0,j) = -o-(j-1)e reached through the gap chains, the result taken at
+// (m, n) of each pair.  Every state carries two counter words per lane (NwCnt): w0 = aligned
+// columns << 16 | counted columns, w1 = leading gap run << 16 | signed trailing gap run.
+// Lanes hold value + bias with a bias that covers the all-gap lower bound of every cell a pass
+// touches (padding rows and columns score 0, so they stay inside the same bounds); lanes start
+// at their own column 0, so steps before it change nothing.
+template <int K, int NP>
+__device__ __forceinline__ void align_two_nw(const uint32_t* __restrict__ prof, int mpad, int passes,
+                                             int m, const uint8_t* __restrict__ ca,
+                                             const uint8_t* __restrict__ cb, int ncols, int nA, int nB,
+                                             const EngineJob& J, uint32_t* __restrict__ scr, int lane,
+                                             uint32_t& capA0, uint32_t& capA1, uint32_t& capB0,
+                                             uint32_t& capB1) {
+  const int B = J.bias, o = J.o, e = J.e;
+  const uint32_t O2 = (uint32_t)o * 0x10001u, E2 = (uint32_t)e * 0x10001u;
+  const uint32_t sent2 = (uint32_t)e * 0x10001u;  // -infinity: loses to any opening, minus e is 0
+  const int plane = NP * mpad;
+  // the cell (m, n) of each pair: its pass, lane, row in the lane, and the step that reaches it
+  const int pm = (m - 1) / (32 * K), tm = ((m - 1) % (32 * K)) / K, rm = (m - 1) % K;
+  const int sA = nA - 1 + tm, sB = nB - 1 + tm;
+  capA0 = capA1 = capB0 = capB1 = 0u;
+  for (int p = 0; p < passes; p++) {
+    const int pbase = p * 32 * K;
+    uint32_t VOL[K], H[K], clA0[K], clA1[K], clB0[K], clB1[K], chA0[K], chA1[K], chB0[K], chB1[K];
+#pragma unroll
+    for (int r = 0; r < K; r++) {
+      const int i = pbase + lane * K + r + 1;  // V(i, 0) = -o - (i-1)e, counters of i UP columns
+      VOL[r] = (uint32_t)(B - 2 * o - (i - 1) * e) * 0x10001u;
+      H[r] = sent2;
+      clA0[r] = clB0[r] = (uint32_t)i << 16;
+      clA1[r] = clB1[r] = ((uint32_t)i << 16) | (uint32_t)(i & 0xFFFF);
+      chA0[r] = chA1[r] = chB0[r] = chB1[r] = 0u;
+    }
+    // the row above the lane's first row, at column 0 (the first step's diagonal)
+    const int i0 = pbase + lane * K;
+    uint32_t dVO = (uint32_t)(i0 == 0 ? B - o : B - 2 * o - (i0 - 1) * e) * 0x10001u;
+    uint32_t dcA0 = (uint32_t)i0 << 16, dcA1 = ((uint32_t)i0 << 16) | (uint32_t)(i0 & 0xFFFF);
+    uint32_t dcB0 = dcA0, dcB1 = dcA1;
+    uint32_t uVO = 0, uG = 0, ucvA0 = 0, ucvA1 = 0, ucvB0 = 0, ucvB1 = 0, ucgA0 = 0, ucgA1 = 0,
+             ucgB0 = 0, ucgB1 = 0;
+    const uint32_t* pl = prof + pbase + lane * 4;
+    const int nsteps = ncols + 31;
+    for (int s = 0; s < nsteps; s++) {
+      const uint32_t bVO = __shfl_up_sync(0xffffffffu, uVO, 1);
+      const uint32_t bG = __shfl_up_sync(0xffffffffu, uG, 1);
+      const uint32_t bcvA0 = __shfl_up_sync(0xffffffffu, ucvA0, 1);
+      const uint32_t bcvA1 = __shfl_up_sync(0xffffffffu, ucvA1, 1);
+      const uint32_t bcvB0 = __shfl_up_sync(0xffffffffu, ucvB0, 1);
+      const uint32_t bcvB1 = __shfl_up_sync(0xffffffffu, ucvB1, 1);
+      const uint32_t bcgA0 = __shfl_up_sync(0xffffffffu, ucgA0, 1);
+      const uint32_t bcgA1 = __shfl_up_sync(0xffffffffu, ucgA1, 1);
+      const uint32_t bcgB0 = __shfl_up_sync(0xffffffffu, ucgB0, 1);
+      const uint32_t bcgB1 = __shfl_up_sync(0xffffffffu, ucgB1, 1);
+      if (s >= lane) {  // the lane's columns start at step `lane`
+        uint32_t VOU, GU, cvuA0, cvuA1, cvuB0, cvuB1, cguA0, cguA1, cguB0, cguB1;
+        if (lane == 0) {
+          if (p == 0) {
+            // row 0: V(0, j) = -o - (j-1)e for column j = s + 1 (past the end: clamped)
+            const int j = min(s, ncols - 1) + 1;
+            VOU = (uint32_t)(B - 2 * o - (j - 1) * e) * 0x10001u;
+            GU = sent2;
+            cvuA0 = cvuB0 = (uint32_t)j << 16;
+            cvuA1 = cvuB1 = ((uint32_t)j << 16) | (uint32_t)((-j) & 0xFFFF);
+            cguA0 = cguA1 = cguB0 = cguB1 = 0u;
+          } else {
+            const int js = min(s, ncols - 1);
+            const uint4 x = *reinterpret_cast<const uint4*>(scr + (long)js * kScrWordsNw);
+            const uint4 y = *reinterpret_cast<const uint4*>(scr + (long)js * kScrWordsNw + 4);
+            const uint4 z = *reinterpret_cast<const uint4*>(scr + (long)js * kScrWordsNw + 8);
+            VOU = x.x; GU = x.y; cvuA0 = x.z; cvuA1 = x.w;
+            cvuB0 = y.x; cvuB1 = y.y; cguA0 = y.z; cguA1 = y.w;
+            cguB0 = z.x; cguB1 = z.y;
+          }
+        } else {
+          VOU = bVO; GU = bG; cvuA0 = bcvA0; cvuA1 = bcvA1; cvuB0 = bcvB0; cvuB1 = bcvB1;
+          cguA0 = bcgA0; cguA1 = bcgA1; cguB0 = bcgB0; cguB1 = bcgB1;
+        }
+        uint32_t VOD = dVO, cdA0 = dcA0, cdA1 = dcA1, cdB0 = dcB0, cdB1 = dcB1;
+        dVO = VOU; dcA0 = cvuA0; dcA1 = cvuA1; dcB0 = cvuB0; dcB1 = cvuB1;
+        const int col = 32 + s - lane;
+        const int xa = ca[col], xb = cb[col];
+        const uint32_t* pla = pl + xa * plane;
+        const uint32_t* phb = pl + xb * plane + (NP == 3 ? mpad : 0);
+        const uint32_t* pma = pl + xa * plane + (NP - 1) * mpad;
+        const uint32_t* pmb = pl + xb * plane + (NP - 1) * mpad;
+        auto cell = [&](const int r, const uint32_t pl_r, const uint32_t ph_r, const uint32_t ma_r,
+                        const uint32_t mb_r) {
+          const uint32_t F = (NP == 3) ? VOD + pl_r + ph_r : mad_hi16(ph_r, VOD + pl_r);
+          const uint32_t cfA0 = cdA0 + ma_r + 0x10000u, cfA1 = cdA1 & 0xFFFF0000u;
+          const uint32_t cfB0 = cdB0 + mb_r + 0x10000u, cfB1 = cdB1 & 0xFFFF0000u;
+          bool hiB, loA;
+          // vertical gap: opening wins ties (extend only if strictly better)
+          const uint32_t G = vmax2(VOU, GU - E2, hiB, loA);
+          const uint32_t cgA0 = (loA ? cvuA0 : cguA0) + 0x10000u;
+          const uint32_t cgA1 = loA ? ((cvuA1 & 0xFFFF0000u) | 1u) : cguA1 + 1u;
+          const uint32_t cgB0 = (hiB ? cvuB0 : cguB0) + 0x10000u;
+          const uint32_t cgB1 = hiB ? ((cvuB1 & 0xFFFF0000u) | 1u) : cguB1 + 1u;
+          // horizontal gap
+          H[r] = vmax2(VOL[r], H[r] - E2, hiB, loA);
+          chA0[r] = (loA ? clA0[r] : chA0[r]) + 0x10000u;
+          chA1[r] = loA ? ((clA1[r] & 0xFFFF0000u) | 0xFFFFu) : chA1[r] - 1u;
+          chB0[r] = (hiB ? clB0[r] : chB0[r]) + 0x10000u;
+          chB1[r] = hiB ? ((clB1[r] & 0xFFFF0000u) | 0xFFFFu) : chB1[r] - 1u;
+          // V = max(F, G, H) with DIAGONAL > UP > LEFT on ties
+          const uint32_t GHv = vmax2(G, H[r], hiB, loA);
+          const uint32_t cghA0 = loA ? cgA0 : chA0[r], cghA1 = loA ? cgA1 : chA1[r];
+          const uint32_t cghB0 = hiB ? cgB0 : chB0[r], cghB1 = hiB ? cgB1 : chB1[r];
+          const uint32_t V = vmax2(F, GHv, hiB, loA);
+          const uint32_t cvA0 = loA ? cfA0 : cghA0, cvA1 = loA ? cfA1 : cghA1;
+          const uint32_t cvB0 = hiB ? cfB0 : cghB0, cvB1 = hiB ? cfB1 : cghB1;
+          const uint32_t VO = V - O2;
+          VOD = VOL[r]; cdA0 = clA0[r]; cdA1 = clA1[r]; cdB0 = clB0[r]; cdB1 = clB1[r];
+          VOL[r] = VO; clA0[r] = cvA0; clA1[r] = cvA1; clB0[r] = cvB0; clB1[r] = cvB1;
+          VOU = VO; GU = G;
+          cvuA0 = cvA0; cvuA1 = cvA1; cvuB0 = cvB0; cvuB1 = cvB1;
+          cguA0 = cgA0; cguA1 = cgA1; cguB0 = cgB0; cguB1 = cgB1;
+        };
+#pragma unroll
+        for (int g = 0; g < K / 4; g++) {
+          const uint4 PL = *reinterpret_cast<const uint4*>(pla + g * 128);
+          const uint4 PH = *reinterpret_cast<const uint4*>(phb + g * 128);
+          const uint4 MA = *reinterpret_cast<const uint4*>(pma + g * 128);
+          const uint4 MB = *reinterpret_cast<const uint4*>(pmb + g * 128);
+          cell(g * 4 + 0, PL.x, PH.x, MA.x, MB.x);
+          cell(g * 4 + 1, PL.y, PH.y, MA.y, MB.y);
+          cell(g * 4 + 2, PL.z, PH.z, MA.z, MB.z);
+          cell(g * 4 + 3, PL.w, PH.w, MA.w, MB.w);
+        }
+        if (K % 4 == 2) {
+          const int t2 = (K / 4) * 128 - lane * 2;
+          const uint2 PL = *reinterpret_cast<const uint2*>(pla + t2);
+          const uint2 PH = *reinterpret_cast<const uint2*>(phb + t2);
+          const uint2 MA = *reinterpret_cast<const uint2*>(pma + t2);
+          const uint2 MB = *reinterpret_cast<const uint2*>(pmb + t2);
+          cell(K - 2, PL.x, PH.x, MA.x, MB.x);
+          cell(K - 1, PL.y, PH.y, MA.y, MB.y);
+        }
+        uVO = VOU; uG = GU; ucvA0 = cvuA0; ucvA1 = cvuA1; ucvB0 = cvuB0; ucvB1 = cvuB1;
+        ucgA0 = cguA0; ucgA1 = cguA1; ucgB0 = cguB0; ucgB1 = cguB1;
+        // the (m, n) cells: lane tm of pass pm holds them after steps sA / sB
+        if (p == pm && lane == tm && (s == sA || s == sB)) {
+#pragma unroll
+          for (int r = 0; r < K; r++)
+            if (r == rm) {
+              if (s == sA) { capA0 = clA0[r]; capA1 = clA1[r]; }
+              if (s == sB) { capB0 = clB0[r]; capB1 = clB1[r]; }
+            }
+        }
+        if (lane == 31 && p + 1 < passes) {
+          const int j = s - 31;
+          if (j >= 0 && j < ncols) {
+            uint32_t* w = scr + (long)j * kScrWordsNw;
+            *reinterpret_cast<uint4*>(w) = make_uint4(uVO, uG, ucvA0, ucvA1);
+            *reinterpret_cast<uint4*>(w + 4) = make_uint4(ucvB0, ucvB1, ucgA0, ucgA1);
+            *reinterpret_cast<uint4*>(w + 8) = make_uint4(ucgB0, ucgB1, 0u, 0u);
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+  // the holder of (m, n) is lane tm: everyone gets its counters
+  capA0 = __shfl_sync(0xffffffffu, capA0, tm);
+  capA1 = __shfl_sync(0xffffffffu, capA1, tm);
+  capB0 = __shfl_sync(0xffffffffu, capB0, tm);
+  capB1 = __shfl_sync(0xffffffffu, capB1, tm);
+}
+
+// NW distance (Salsa.NeedlemanWunschTPL/Program.cs:547-571, :583-604) from the counters of (m, n).
+__device__ __forceinline__ int16_t engine_nw_distance(uint32_t w0, uint32_t w1, int m, int n, int protein) {
+  const int count = (int)(w0 & 0xFFFFu), len = (int)(w0 >> 16);
+  if (protein) return fraction_distance(count, len);
+  const int lead = (int)(w1 >> 16);
+  const int run = (int)(int16_t)(w1 & 0xFFFFu);
+  int trimmed = len - lead - (run < 0 ? -run : run);
+  if (m == 0 || n == 0) trimmed = 0;
+  return fraction_distance(count, trimmed);
+}
+
+// Counters of a pair with an empty side: all of it one gap run along the boundary.
+__device__ __forceinline__ void nw_boundary(int m, int n, uint32_t& w0, uint32_t& w1) {
+  if (m == 0 && n == 0) { w0 = 0u; w1 = 0u; }
+  else if (m == 0) { w0 = (uint32_t)n << 16; w1 = ((uint32_t)n << 16) | (uint32_t)((-n) & 0xFFFF); }
+  else { w0 = (uint32_t)m << 16; w1 = ((uint32_t)m << 16) | (uint32_t)(m & 0xFFFF); }
+}
+
 // Lexicographic (max score, min row) over the warp; lane 0 ends with the winner.
 __device__ __forceinline__ void warp_best(int& best, int& row, uint32_t& cnt) {
 #pragma unroll
@@ -295,9 +486,10 @@ __device__ __forceinline__ void emit(const EngineJob& J, int q, int d, int16_t d
   if (J.mode != kModeSwgMs) J.out[(long long)d * J.ld + q] = dist;
 }
 
-template <int K, int NP>
-__global__ void __launch_bounds__(warps_of(K) * 32, ctas_of(K)) engine_kernel(EngineJob J) {
-  constexpr int kEngWarps = warps_of(K);
+template <int K, int NP, bool NW>
+__global__ void __launch_bounds__(warps_of(K, NW) * 32, ctas_of(K, NW)) engine_kernel(EngineJob J) {
+  constexpr int kEngWarps = warps_of(K, NW);
+  constexpr int kScr = NW ? kScrWordsNw : kScrWords;
   extern __shared__ __align__(16) uint8_t smem[];
   uint32_t* prof = reinterpret_cast<uint32_t*>(smem);
   const int A1 = J.A + 1;
@@ -309,7 +501,7 @@ __global__ void __launch_bounds__(warps_of(K) * 32, ctas_of(K)) engine_kernel(En
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint8_t* ca = codes + (size_t)warp * 2 * cbuf;
   uint8_t* cb = ca + cbuf;
-  uint32_t* scr = J.scratch + ((long)blockIdx.x * kEngWarps + warp) * (long)J.maxcol * kScrWords;
+  uint32_t* scr = J.scratch + ((long)blockIdx.x * kEngWarps + warp) * (long)J.maxcol * kScr;
   if (threadIdx.x == 0) s_q = -1;
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(J.counter, 1);
@@ -384,6 +576,22 @@ __global__ void __launch_bounds__(warps_of(K) * 32, ctas_of(K)) engine_kernel(En
       }
       for (int k = 32 + ncols + lane; k < 64 + ncols; k += 32) { ca[k] = (uint8_t)J.A; cb[k] = (uint8_t)J.A; }
       __syncwarp();
+      if constexpr (NW) {
+        uint32_t a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+        if (m > 0 && ncols > 0)
+          align_two_nw<K, NP>(prof, J.mpad, passes, m, ca, cb, ncols, nA, nB, J, scr, lane, a0, a1, b0, b1);
+        if (lane == 0) {
+          if (m == 0 || nA == 0) nw_boundary(m, nA, a0, a1);
+          emit(J, q, dA, engine_nw_distance(a0, a1, m, nA, J.protein));
+          if (dB >= 0) {
+            if (m == 0 || nB == 0) nw_boundary(m, nB, b0, b1);
+            emit(J, q, dB, engine_nw_distance(b0, b1, m, nB, J.protein));
+          }
+          atomicAdd(J.stats + 1, (unsigned long long)(1 + (dB >= 0)));
+        }
+        __syncwarp();
+        continue;
+      }
       int bA, rA, bB, rB;
       uint32_t cA, cB;
       if (m > 0 && ncols > 0) {
@@ -436,9 +644,9 @@ constexpr int kKs[kNumK] = {4, 6, 8, 10, 12, 14, 16};
 constexpr int kMaxAlpha16 = 32;
 int planes_of(int A) { return A > 8 ? 2 : 3; }
 
-size_t engine_smem(int A, int mpad, int maxcol, int K) {
+size_t engine_smem(int A, int mpad, int maxcol, int K, bool nw = false) {
   const int cbuf = 64 + ((maxcol + 31) / 32) * 32;
-  return (size_t)(A + 1) * planes_of(A) * mpad * 4 + kMaxChunk * 4 + (size_t)warps_of(K) * 2 * cbuf;
+  return (size_t)(A + 1) * planes_of(A) * mpad * 4 + kMaxChunk * 4 + (size_t)warps_of(K, nw) * 2 * cbuf;
 }
 
 __global__ void set_int_kernel(int* p, int v) { *p = v; }
@@ -457,38 +665,55 @@ auto with_k(int K, Fn fn) {
   }
 }
 
-// The kernel instantiation for K rows per lane and the planes of alphabet A.
+// The kernel instantiation for K rows per lane, the planes of alphabet A and the DP kind.
 template <class Fn>
-auto with_kp(int K, int A, Fn fn) {
+auto with_kp(int K, int A, bool nw, Fn fn) {
   return with_k(K, [&](auto k) {
-    if (planes_of(A) == 3) return fn(engine_kernel<decltype(k)::value, 3>, warps_of(decltype(k)::value) * 32);
-    return fn(engine_kernel<decltype(k)::value, 2>, warps_of(decltype(k)::value) * 32);
+    constexpr int kk = decltype(k)::value;
+    if (nw) {
+      if (planes_of(A) == 3) return fn(engine_kernel<kk, 3, true>, warps_of(kk, true) * 32);
+      return fn(engine_kernel<kk, 2, true>, warps_of(kk, true) * 32);
+    }
+    if (planes_of(A) == 3) return fn(engine_kernel<kk, 3, false>, warps_of(kk) * 32);
+    return fn(engine_kernel<kk, 2, false>, warps_of(kk) * 32);
   });
 }
 
-cudaError_t allow_smem_k(int K, int A, size_t smem) {
-  return with_kp(K, A, [&](auto kern, int) {
+cudaError_t allow_smem_k(int K, int A, bool nw, size_t smem) {
+  return with_kp(K, A, nw, [&](auto kern, int) {
     return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   });
 }
 
 cudaError_t launch_engine_k(int K, const EngineJob& J, int grid, size_t smem, cudaStream_t st) {
-  return with_kp(K, J.A, [&](auto kern, int threads) {
+  return with_kp(K, J.A, J.mode == kModeNw, [&](auto kern, int threads) {
     kern<<<grid, threads, smem, st>>>(J);
     return cudaGetLastError();
   });
 }
 
-int occupancy_k(int K, int A, size_t smem) {
-  return with_kp(K, A, [&](auto kern, int threads) {
+int occupancy_k(int K, int A, bool nw, size_t smem) {
+  return with_kp(K, A, nw, [&](auto kern, int threads) {
     int n = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem);
     return n;
   });
 }
 
-// Relative cost of one computed row at K rows per lane (100 = 16 rows): B200 row-padded cell
-// rates of the uneven 3,000-sequence DNA job with K forced for every query.
+// Relative cost of one computed row at K rows per lane (100 = the cheapest), from B200 row-padded
+// cell rates with K forced for every query: SW on the uneven 3,000-sequence DNA job, NW on the
+// 3,000-sequence uniform 300-500 DNA job.
+long k_weight_nw(int k) {
+  switch (k) {
+    case 4: return 120;
+    case 6: return 103;
+    case 8: return 105;
+    case 10: return 106;
+    case 12: return 106;
+    default: return 100;
+  }
+}
+
 long k_weight(int k) {
   switch (k) {
     case 4: return 188;
@@ -502,16 +727,17 @@ long k_weight(int k) {
 }
 
 // Rows per lane and passes for a query of m rows: fewest padded rows, then fewest passes.
-void choose_k(int m, int kov, int* K, int* passes) {
+void choose_k(int m, int kov, int* K, int* passes, bool nw = false) {
+  if (nw && kov > 14) kov = 14;  // NW kernels stop at 14 rows per lane
   if (kov) { *K = kov; *passes = std::max(1, (m + 32 * kov - 1) / (32 * kov)); return; }
   long best = -1;
   for (int k : kKs) {
+    if (nw && k > 14) continue;
     const int p = std::max(1, (m + 32 * k - 1) / (32 * k));
-    // rows computed (padding included) times the per-row cost of that K, measured on B200 for
-    // the uneven 3,000-sequence job with K forced: 4 rows per lane cost 1.55x a row at 8-16
-    // (too few rows to amortise the per-step shuffles, loads and column bookkeeping); ties go to
-    // fewer passes (each pass adds a wavefront fill and a scratch round trip)
-    const long weight = k_weight(k);
+    // rows computed (padding included) times the per-row cost of that K (few rows per lane do
+    // not amortise the per-step shuffles, loads and column bookkeeping); ties go to fewer passes
+    // (each pass adds a wavefront fill and a scratch round trip)
+    const long weight = nw ? k_weight_nw(k) : k_weight(k);
     const long cost = (long)p * 32 * k * weight * 16 + p;
     if (best < 0 || cost < best) { best = cost; *K = k; *passes = p; }
   }
@@ -549,6 +775,7 @@ int upload_vec(T** dst, const std::vector<T>& v, std::string* msg, const char* w
 // State of one sequence set shared by every plan: residue codes, length order, tables.
 struct Base {
   int alpha = 0, bias = 1, max_s = 0, maxcol = 1;
+  bool nw16 = false;  // NW fits the 16-bit lanes
   std::vector<int> len, sorted_h, letters;
   uint8_t* d_code = nullptr;
   int32_t* d_sorted = nullptr;
@@ -590,7 +817,7 @@ int build_base(Base& B, const EngineParams& P, std::string* msg) {
   if (cudaMalloc(&B.d_carry, plain_carry_bytes(P.mode == kModeNw ? kModeNw : kModeSwgMpi, B.carry_threads, B.maxcol)) != cudaSuccess) {
     cudaGetLastError(); B.d_carry = nullptr; *msg = "cudaMalloc 32-bit lane scratch"; return SW_E_OOM;
   }
-  if (B.alpha > kMaxAlpha16 || P.mode == kModeNw || P.lanes == SW_LANES_32) return SW_OK;
+  if (B.alpha > kMaxAlpha16 || P.lanes == SW_LANES_32) return SW_OK;
   const int A = B.alpha, A1 = A + 1;
   int maxS = 0, minS = 0;
   for (int a : letters)
@@ -599,7 +826,20 @@ int build_base(Base& B, const EngineParams& P, std::string* msg) {
       maxS = std::max(maxS, s);
       minS = std::min(minS, s);
     }
-  B.bias = std::max(std::max(P.o + 2 * P.e, -minS), 1);
+  const bool nw = P.mode == kModeNw;
+  if (nw) {
+    // Global alignment has no floor: the bias covers the all-gap lower bound of every cell a
+    // pass touches (rows padded by up to 32 x 16 - 1, columns by up to 63), minus the most
+    // negative score and a gap open + extend of intermediate values.  The lanes hold the
+    // scores only if the highest possible V still fits: otherwise 32-bit lanes.
+    const long span = (long)B.maxcol + 512 + (long)B.maxcol + 64;
+    const long bias = 3L * P.o + 2L * P.e + span * P.e - minS;
+    if (bias + (long)maxS * (B.maxcol + 1) > 32767) return SW_OK;
+    B.bias = (int)bias;
+    B.nw16 = true;
+  } else {
+    B.bias = std::max(std::max(P.o + 2 * P.e, -minS), 1);
+  }
   B.max_s = maxS;
   std::vector<int32_t> lettab((size_t)A1 * A1);
   std::vector<uint32_t> flagtab((size_t)A1 * A1, 0u);
@@ -607,7 +847,7 @@ int build_base(Base& B, const EngineParams& P, std::string* msg) {
     for (int c = 0; c < A1; c++) {
       int s;
       uint32_t f = 0;
-      if (a == A || c == A) s = -B.bias;
+      if (a == A || c == A) s = nw ? 0 : -B.bias;  // padding: NW keeps its values bounded
       else {
         s = P.h_scores[letters[a] * 128 + letters[c]];
         f = P.h_flags[letters[a] * 128 + letters[c]] & kFlagCount;
@@ -780,7 +1020,8 @@ class EngineImpl : public Engine {
     for (int r = 0; r < P.ranks; r++)
       for (int x = starts[r]; x <= ends[r]; x++) blk[x] = r;
     int rc;
-    pl.plain_only = B.alpha > kMaxAlpha16 || P.mode == kModeNw || P.lanes == SW_LANES_32;
+    const bool nw = P.mode == kModeNw;
+    pl.plain_only = B.alpha > kMaxAlpha16 || (nw && !B.nw16) || P.lanes == SW_LANES_32;
     std::vector<int2> big;
     if (pl.plain_only) {
       for (int q = key.row_lo; q <= key.row_hi; q++)
@@ -817,9 +1058,9 @@ class EngineImpl : public Engine {
     for (int q = key.row_lo; q <= key.row_hi; q++) {
       const int m = B.len[q];
       int K, passes;
-      choose_k(m, opt_.k_override, &K, &passes);
+      choose_k(m, opt_.k_override, &K, &passes, nw);
       // a profile beyond shared memory (long queries, large alphabets): 32-bit lanes
-      const bool fits = engine_smem(A, passes * 32 * K, B.maxcol, K) <= 227 * 1024;
+      const bool fits = engine_smem(A, passes * 32 * K, B.maxcol, K, nw) <= 227 * 1024;
       const int bi = (int)(std::find(std::begin(kKs), std::end(kKs), K) - std::begin(kKs));
       const int bq = blk[q];
       for (int c = 0; c < nchunks; c++) {
@@ -881,13 +1122,13 @@ class EngineImpl : public Engine {
     size_t scr_words = 0;
     for (auto& bn : pl.bins) {
       if (bn.items.empty()) continue;
-      bn.smem = engine_smem(A, bn.mpad, B.maxcol, bn.K);
+      bn.smem = engine_smem(A, bn.mpad, B.maxcol, bn.K, nw);
       if (bn.smem > 227 * 1024) { *msg = "query profile exceeds shared memory"; return SW_E_UNSUPPORTED; }
-      if (allow_smem_k(bn.K, A, bn.smem) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
-      const int occ = std::max(1, occupancy_k(bn.K, A, bn.smem));
+      if (allow_smem_k(bn.K, A, nw, bn.smem) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
+      const int occ = std::max(1, occupancy_k(bn.K, A, nw, bn.smem));
       bn.grid = (int)std::min<long>((long)P.sms * occ, (long)bn.items.size());
       bn.scratch_off = scr_words;
-      if (bn.max_passes > 1) scr_words += (size_t)bn.grid * warps_of(bn.K) * B.maxcol * kScrWords;
+      if (bn.max_passes > 1) scr_words += (size_t)bn.grid * warps_of(bn.K, nw) * B.maxcol * (nw ? kScrWordsNw : kScrWords);
     }
     pl.order.clear();
     for (size_t b = 0; b < pl.bins.size(); b++)
@@ -929,7 +1170,7 @@ class EngineImpl : public Engine {
       J.code = B.d_code; J.off = P.off; J.sorted = B.d_sorted;
       J.lettab = B.d_lettab; J.flagtab = B.d_flagtab;
       J.A = B.alpha; J.o = P.o; J.e = P.e; J.bias = B.bias; J.thresh = pl.thresh;
-      J.mode = P.mode; J.ranks = P.ranks; J.nseq = P.nseq;
+      J.mode = P.mode; J.ranks = P.ranks; J.nseq = P.nseq; J.protein = P.protein;
       J.rb_a = P.nseq / P.ranks; J.rb_b = P.nseq % P.ranks;
       J.out = P.out; J.ld = P.ld;
       J.scratch = B.d_scratch; J.maxcol = B.maxcol;
@@ -1160,8 +1401,8 @@ class QueryRunnerImpl : public QueryRunner {
     for (size_t x = 0; x < ls.size(); x++) {
       smem[x] = engine_smem(A, ls[x].mpad, B_.maxcol, ls[x].K);
       if (smem[x] > 227 * 1024) { *msg = "query profile exceeds shared memory"; return SW_E_UNSUPPORTED; }
-      if (allow_smem_k(ls[x].K, A, smem[x]) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
-      const int occ = std::max(1, occupancy_k(ls[x].K, A, smem[x]));
+      if (allow_smem_k(ls[x].K, A, false, smem[x]) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
+      const int occ = std::max(1, occupancy_k(ls[x].K, A, false, smem[x]));
       grid[x] = std::min(P_.sms * occ, ls[x].count);
       scr_off[x] = scr_words;
       if (ls[x].max_passes > 1) scr_words += (size_t)grid[x] * warps_of(ls[x].K) * B_.maxcol * kScrWords;

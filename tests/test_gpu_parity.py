@@ -257,3 +257,29 @@ def test_protein_engine_uses_16bit_lanes_and_matches_oracle(cs, oracle_mod):
     pr = np.array([(i, j) for i in range(N) for j in range(i)], dtype=np.int32)
     want = _oracle_distances(oracle_mod, seqs, pr, "BLOSUM62", 10.0, 1.0, atype=0)
     np.testing.assert_array_equal(full[pr[:, 0], pr[:, 1]], want)
+
+
+@pytest.mark.parametrize("matrix,o,e,atype", [("EDNAFULL", 16, 4, 1), ("BLOSUM62", 10, 1, 0)])
+def test_nw_engine_matches_plain_kernel(cs, matrix, o, e, atype):
+    """NW on the 16-bit lanes (every rows-per-lane bin, multi-pass queries, empty and 1-residue
+    sequences) equals the 32-bit plain kernel, which the NW restatement fixtures pin."""
+    from csharp_b200 import synth
+    rng = np.random.default_rng(61)
+    lens = np.concatenate([rng.integers(1, 900, 110), [0, 1, 1, 1400]])
+    if atype == 1:
+        seqs = [s.tobytes() for s in synth.dna_family(len(lens), 5, lens, seed=61)]
+    else:
+        seqs = [s.tobytes() for s in synth.protein_family(len(lens), 5, lens, 61, cs.ScoringMatrix.Load(matrix).Scores)]
+    eng = cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=cs.NW, alignment_type=atype).upload(seqs)
+    full, pairs, _ = eng.all_pairs(1)
+    # all but the 1,400-residue protein query's pairs (its profile exceeds shared memory)
+    assert eng.query("lane16_pairs") + eng.rerun_count() == pairs
+    assert eng.query("lane16_pairs") >= pairs - (len(seqs) if atype == 0 else 0)
+    ref = cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=cs.NW, alignment_type=atype, lanes=32).upload(seqs)
+    want, _, _ = ref.all_pairs(1)
+    np.testing.assert_array_equal(full, want)
+    for k in (4, 10, 16):  # forced rows per lane
+        eng.set_option("rows_per_lane", k)
+        got, _, _ = eng.all_pairs(3)
+        want3, _, _ = ref.all_pairs(3)
+        np.testing.assert_array_equal(got, want3)
