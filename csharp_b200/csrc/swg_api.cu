@@ -41,6 +41,7 @@ struct sw_ctx {
   int64_t last_reruns = 0;
   cudaStream_t own_stream = nullptr;  // the context's stream while a caller's stream is in use
   int64_t last_pairs = 0, last_cells = 0;
+  int* d_throws = nullptr;  // set by a SWG-MPI JukesCantor pair whose log argument is <= 0
   // serving (query batches against the uploaded sequences)
   swg::Server* server = nullptr;
   swg::ServeOptions serve_opt;
@@ -89,7 +90,18 @@ void build_flags(sw_ctx* c) {
       if (a == b) f |= swg::kFlagIdent;
       if (a == b || s > 0) f |= swg::kFlagSimNA;
       bool count;
-      if (!protein) count = (a == b);                 // identity (all three apps)
+      if (!protein) {
+        count = (a == b);                             // identity (all three apps)
+        // Kimura2 / JukesCantor read the aligned strings (Alignment.cs:254-348)
+        const bool transition = (a == 'A' && b == 'G') || (a == 'G' && b == 'A') ||
+                                (a == 'C' && b == 'T') || (a == 'T' && b == 'C');
+        if (c->cfg.distance_fn == SW_DIST_KIMURA2) {
+          if (transition) f |= swg::kFlagCntA;
+          else if (a != b) f |= swg::kFlagCntB;
+        } else if (c->cfg.distance_fn == SW_DIST_JUKES_CANTOR) {
+          if (a == b) f |= swg::kFlagCntA;
+        }
+      }
       else if (mode == SW_MODE_SWG_MPI) count = (a == b || s > 0);  // NAligner similarity
       else count = (s > 0);                           // MBF: non-gap pairs with positive score
       if (count) f |= swg::kFlagCount;
@@ -113,8 +125,10 @@ int sw_create(const sw_config* cfg, sw_ctx** out) {
   if (cfg->alignment_type != SW_PROTEIN && cfg->alignment_type != SW_NUCLEIC) return SW_E_ARG;
   if (cfg->distance_fn < 0 || cfg->distance_fn > 2) return SW_E_ARG;
   if (cfg->lanes != SW_LANES_AUTO && cfg->lanes != SW_LANES_16 && cfg->lanes != SW_LANES_32) return SW_E_ARG;
-  // Kimura2 / JukesCantor need the aligned strings' transition counts: not in this engine.
-  if (cfg->distance_fn != SW_DIST_PERCENT_IDENTITY && cfg->alignment_type == SW_NUCLEIC) return SW_E_UNSUPPORTED;
+  // Kimura2 / JukesCantor of NW alignments are not restated here (SWG-MPI and SWG-MS are).
+  if (cfg->distance_fn != SW_DIST_PERCENT_IDENTITY && cfg->alignment_type == SW_NUCLEIC &&
+      cfg->mode == SW_MODE_NW)
+    return SW_E_UNSUPPORTED;
   const float o = cfg->gap_open, e = cfg->gap_extension;
   if (!(std::isfinite(o) && std::isfinite(e))) return SW_E_ARG;
   if (o != std::floor(o) || e != std::floor(e)) return SW_E_UNSUPPORTED;
@@ -143,6 +157,8 @@ int sw_create(const sw_config* cfg, sw_ctx** out) {
   if ((err = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
       (err = cudaMalloc(&ctx->d_scores, sizeof(ctx->h_scores))) != cudaSuccess ||
       (err = cudaMalloc(&ctx->d_flags, sizeof(ctx->h_flags))) != cudaSuccess ||
+      (err = cudaMalloc(&ctx->d_throws, sizeof(int))) != cudaSuccess ||
+      (err = cudaMemset(ctx->d_throws, 0, sizeof(int))) != cudaSuccess ||
       (err = cudaMemcpy(ctx->d_scores, ctx->h_scores, sizeof(ctx->h_scores), cudaMemcpyHostToDevice)) != cudaSuccess ||
       (err = cudaMemcpy(ctx->d_flags, ctx->h_flags, sizeof(ctx->h_flags), cudaMemcpyHostToDevice)) != cudaSuccess) {
     cudaGetLastError();
@@ -164,6 +180,7 @@ int sw_destroy(sw_ctx* ctx) {
   cudaFree(ctx->d_off);
   cudaFree(ctx->d_scores);
   cudaFree(ctx->d_flags);
+  cudaFree(ctx->d_throws);
   cudaFree(ctx->d_carry);
   cudaFree(ctx->d_stage);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -236,7 +253,20 @@ static int block_job(sw_ctx* ctx, int32_t rs, int32_t re, int32_t cs, int32_t ce
   J->e = ctx->e;
   J->mode = ctx->cfg.mode;
   J->protein = ctx->cfg.alignment_type == SW_PROTEIN;
+  J->dist_fn = ctx->cfg.distance_fn;
+  J->throws = ctx->d_throws;
   return SW_OK;
+}
+
+// After the context's stream is idle: SW_E_THROWS if a pair since the last check met the
+// reference's JukesCantor Log(Zero) (its entry holds 0), and the flag is cleared.
+static int check_throws(sw_ctx* ctx) {
+  if (ctx->cfg.distance_fn != SW_DIST_JUKES_CANTOR) return SW_OK;
+  int h = 0;
+  CK(cudaMemcpy(&h, ctx->d_throws, sizeof(int), cudaMemcpyDeviceToHost), "read throw flag");
+  if (!h) return SW_OK;
+  CK(cudaMemset(ctx->d_throws, 0, sizeof(int)), "clear throw flag");
+  return fail(ctx, SW_E_THROWS, "JukesCantor: the reference throws for Log(Zero) on a pair of this job");
 }
 
 static int run_plain(sw_ctx* ctx, swg::PlainJob& J) {
@@ -246,7 +276,7 @@ static int run_plain(sw_ctx* ctx, swg::PlainJob& J) {
   if (threads < block) threads = block;
   const int grid = (int)(threads / block);
   int rc = ensure(ctx, &ctx->d_carry, &ctx->carry_bytes,
-                  swg::plain_carry_bytes(J.mode, threads, ctx->maxlen), "carry scratch");
+                  swg::plain_carry_bytes(J.mode, threads, ctx->maxlen, J.dist_fn), "carry scratch");
   if (rc) return rc;
   J.carry = ctx->d_carry;
   CK(swg::launch_plain_block(J, grid, block, ctx->stream), "plain block kernel launch");
@@ -295,7 +325,7 @@ int sw_compute_block(sw_ctx* ctx, int32_t rs, int32_t re, int32_t cs, int32_t ce
   CK(cudaMemcpy2DAsync(out, (size_t)ld * 2, ctx->d_stage, Cc * 2, Cc * 2, R, cudaMemcpyDeviceToHost, ctx->stream), "copy block out");
   CK(cudaStreamSynchronize(ctx->stream), "compute block");
   if (pairs) *pairs = J.npairs;
-  return SW_OK;
+  return check_throws(ctx);
 }
 
 int sw_align_pair(sw_ctx* ctx, const uint8_t* s1, int32_t m, const uint8_t* s2, int32_t n,
@@ -334,6 +364,40 @@ int sw_align_pair(sw_ctx* ctx, const uint8_t* s1, int32_t m, const uint8_t* s2, 
   out->start1 = r.start1; out->start2 = r.start2;
   out->identity = r.identity; out->similarity = r.similarity;
   out->gaps = r.gaps; out->length = r.length;
+  out->reserved = 0;
+  if (ctx->cfg.alignment_type == SW_NUCLEIC && ctx->cfg.distance_fn != SW_DIST_PERCENT_IDENTITY) {
+    // Kimura2 / JukesCantor (Alignment.cs:254-348) in binary64, as the device epilogue
+    const double eps = 4.9406564584124654e-324;  // System.Double.Epsilon
+    const bool ms = ctx->cfg.mode == SW_MODE_SWG_MS;
+    const double length = r.length, gapc = (double)(r.length - r.diag);
+    double v;
+    if (ctx->cfg.distance_fn == SW_DIST_KIMURA2) {
+      volatile double P = (double)r.transitions / (length - gapc), Q = (double)r.transversions / (length - gapc);
+      volatile double t1 = 1.0 - (2.0 * P + Q), t2 = 1.0 - 2.0 * Q;
+      if (t1 <= eps || t2 <= eps) v = 10.0;
+      else {
+        volatile double a = 1.0 - 2.0 * P - Q;
+        volatile double l1 = -0.5 * std::log(a), l2 = 0.25 * std::log(t2);
+        v = l1 - l2;
+      }
+      if (ms && v > 10.0) v = 10.0;
+    } else {
+      volatile double frac = (double)(r.diag - r.identity) / (length - gapc);
+      volatile double d = 1.0 - (4.0 / 3.0) * frac;
+      if (d <= eps) {
+        if (!ms) {
+          out->distance = 0;
+          return fail(ctx, SW_E_THROWS, "JukesCantor: the reference throws for Log(Zero)");
+        }
+        v = 10.0;
+      } else {
+        v = -0.75 * std::log(d);
+      }
+    }
+    volatile double x = v * 32767.0;
+    out->distance = (x > -2147483649.0 && x < 2147483648.0) ? (int16_t)(uint16_t)(uint32_t)(int32_t)x : 0;
+    return SW_OK;
+  }
   // ComputeDistance for this pair on the host, in binary32 like the device epilogue.
   int count;
   if (ctx->cfg.alignment_type == SW_NUCLEIC) count = r.identity;
@@ -350,7 +414,7 @@ int sw_synchronize(sw_ctx* ctx) {
   if (!ctx) return SW_E_ARG;
   cudaSetDevice(ctx->cfg.device);
   CK(cudaStreamSynchronize(ctx->stream), "synchronize");
-  return SW_OK;
+  return check_throws(ctx);
 }
 
 int sw_last_rerun_count(const sw_ctx* ctx_, int64_t* count) {
@@ -384,6 +448,8 @@ static int run_engine(sw_ctx* ctx, int32_t ranks, int row_lo, int row_hi, int16_
   P.mode = ctx->cfg.mode;
   P.protein = ctx->cfg.alignment_type == SW_PROTEIN;
   P.lanes = ctx->cfg.lanes;
+  P.dist_fn = ctx->cfg.distance_fn;
+  P.throws = ctx->d_throws;
   P.ranks = ranks;
   P.row_lo = row_lo;
   P.row_hi = row_hi;
@@ -489,7 +555,7 @@ int sw_all_pairs(sw_ctx* ctx, int32_t ranks, int16_t* out, int64_t ld, int64_t* 
   if ((rc = sw_all_pairs_device(ctx, ranks, ctx->d_stage, (int64_t)N, pairs, cells))) return rc;
   if (N) CK(cudaMemcpy2DAsync(out, (size_t)ld * 2, ctx->d_stage, N * 2, N * 2, N, cudaMemcpyDeviceToHost, ctx->stream), "copy result");
   CK(cudaStreamSynchronize(ctx->stream), "all pairs");
-  return SW_OK;
+  return check_throws(ctx);
 }
 
 static swg::EngineParams db_params(sw_ctx* ctx) {
@@ -504,6 +570,8 @@ static swg::EngineParams db_params(sw_ctx* ctx) {
   P.mode = ctx->cfg.mode;
   P.protein = ctx->cfg.alignment_type == SW_PROTEIN;
   P.lanes = ctx->cfg.lanes;
+  P.dist_fn = ctx->cfg.distance_fn;
+  P.throws = ctx->d_throws;
   P.ranks = 1;
   P.out = nullptr; P.ld = 0;
   P.sms = ctx->sms;

@@ -30,6 +30,8 @@ constexpr int kTable = 128;          // substitution tables are [128][128]
 constexpr uint32_t kFlagCount = 1u;  // the context's counted column (identity or similarity)
 constexpr uint32_t kFlagIdent = 2u;  // c1 == c2
 constexpr uint32_t kFlagSimNA = 4u;  // NAligner similarity: c1 == c2 or S > 0
+constexpr uint32_t kFlagCntA = 8u;   // Kimura2: transition (A<->G, C<->T); JukesCantor: c1 == c2
+constexpr uint32_t kFlagCntB = 16u;  // Kimura2: transversion (any other mismatch)
 
 // ---- counter policies --------------------------------------------------------------------------
 // SwCnt: one 32-bit word, aligned columns in bits 16..31, counted columns in bits 0..15.
@@ -64,15 +66,36 @@ struct NwCnt {
   __device__ __forceinline__ static T left_open(T c) { return T{c.w0 + 0x10000u, (c.w1 & 0xFFFF0000u) | 0xFFFFu}; }
 };
 
-// FullCnt: every PairwiseAlignment field the path reads, for the single-pair aligner.
-struct FullCnt {
-  struct T { int id, sim, len, si, sj; };
-  __device__ __forceinline__ static T stop(int i, int j) { return T{0, 0, 0, i, j}; }
-  __device__ __forceinline__ static T origin() { return T{0, 0, 0, 0, 0}; }
-  __device__ __forceinline__ static T row0(int j) { return T{0, 0, 0, 0, j}; }
-  __device__ __forceinline__ static T col0(int i) { return T{0, 0, 0, i, 0}; }
+// KimCnt: the Kimura2 / JukesCantor counts of the aligned strings (Alignment.cs:254-348).
+// w0 = aligned columns << 16 | A-flagged columns, w1 = diagonal (non-gap) columns << 16 |
+// B-flagged columns, with A/B = transitions/transversions (Kimura2) or identical/none
+// (JukesCantor), as the flag table marks them.
+struct KimCnt {
+  struct T { uint32_t w0, w1; };
+  __device__ __forceinline__ static T origin() { return T{0u, 0u}; }
+  __device__ __forceinline__ static T stop(int, int) { return T{0u, 0u}; }
+  __device__ __forceinline__ static T row0(int) { return T{0u, 0u}; }
+  __device__ __forceinline__ static T col0(int) { return T{0u, 0u}; }
   __device__ __forceinline__ static T diag(T c, uint32_t fl) {
-    return T{c.id + (int)((fl >> 1) & 1u), c.sim + (int)((fl >> 2) & 1u), c.len + 1, c.si, c.sj};
+    return T{c.w0 + 0x10000u + ((fl >> 3) & 1u), c.w1 + 0x10000u + ((fl >> 4) & 1u)};
+  }
+  __device__ __forceinline__ static T up_ext(T c) { return T{c.w0 + 0x10000u, c.w1}; }
+  __device__ __forceinline__ static T up_open(T c) { return T{c.w0 + 0x10000u, c.w1}; }
+  __device__ __forceinline__ static T left_ext(T c) { return T{c.w0 + 0x10000u, c.w1}; }
+  __device__ __forceinline__ static T left_open(T c) { return T{c.w0 + 0x10000u, c.w1}; }
+};
+
+// FullCnt: every PairwiseAlignment field the path reads, for the single-pair aligner, plus the
+// transition / transversion counts of Kimura2.
+struct FullCnt {
+  struct T { int id, sim, len, si, sj, diag, ts, tv; };
+  __device__ __forceinline__ static T stop(int i, int j) { return T{0, 0, 0, i, j, 0, 0, 0}; }
+  __device__ __forceinline__ static T origin() { return T{0, 0, 0, 0, 0, 0, 0, 0}; }
+  __device__ __forceinline__ static T row0(int j) { return T{0, 0, 0, 0, j, 0, 0, 0}; }
+  __device__ __forceinline__ static T col0(int i) { return T{0, 0, 0, i, 0, 0, 0, 0}; }
+  __device__ __forceinline__ static T diag(T c, uint32_t fl) {
+    return T{c.id + (int)((fl >> 1) & 1u), c.sim + (int)((fl >> 2) & 1u), c.len + 1, c.si, c.sj,
+             c.diag + 1, c.ts + (int)((fl >> 3) & 1u), c.tv + (int)((fl >> 4) & 1u)};
   }
   __device__ __forceinline__ static T up_ext(T c) { c.len++; return c; }
   __device__ __forceinline__ static T up_open(T c) { c.len++; return c; }
@@ -118,6 +141,56 @@ __device__ __forceinline__ int16_t cs_conv_i2(float x) {
 __device__ __forceinline__ int16_t fraction_distance(int count, int len) {
   const float p = __fdiv_rn(__int2float_rn(count), __int2float_rn(len));
   return cs_conv_i2(__fmul_rn(__fsub_rn(1.0f, p), 32767.0f));
+}
+
+// .NET x64 conv.i2 of a double (cvttsd2si to int32, then the low 16 bits).
+__device__ __forceinline__ int16_t cs_conv_i2_d(double x) {
+  if (!(x > -2147483649.0 && x < 2147483648.0)) return 0;
+  return (int16_t)(uint16_t)(uint32_t)__double2int_rz(x);
+}
+
+constexpr double kDoubleEpsilon = 4.9406564584124654e-324;  // System.Double.Epsilon
+
+// Kimura2 (Alignment.cs:254-302) of an alignment with len columns, diag of them non-gap, ts
+// transitions and tv transversions; in binary64 without contraction, like the reference.
+__device__ __forceinline__ double kimura2_value(int len, int diag, int ts, int tv) {
+  const double length = (double)len, gapc = (double)(len - diag);
+  const double P = __ddiv_rn((double)ts, __dsub_rn(length, gapc));
+  const double Q = __ddiv_rn((double)tv, __dsub_rn(length, gapc));
+  if (__dsub_rn(1.0, __dadd_rn(__dmul_rn(2.0, P), Q)) <= kDoubleEpsilon) return 10.0;
+  if (__dsub_rn(1.0, __dmul_rn(2.0, Q)) <= kDoubleEpsilon) return 10.0;
+  return __dsub_rn(__dmul_rn(-0.5, log(__dsub_rn(__dsub_rn(1.0, __dmul_rn(2.0, P)), Q))),
+                   __dmul_rn(0.25, log(__dsub_rn(1.0, __dmul_rn(2.0, Q)))));
+}
+
+// JukesCantor (Alignment.cs:314-348): 1 - (4/3)(diff / non-gap columns); false where the
+// reference's log would see a value <= Double.Epsilon (it throws "Log(Zero)").
+__device__ __forceinline__ bool jukes_cantor_value(int len, int diag, int identical, double* out) {
+  const double length = (double)len, gapc = (double)(len - diag);
+  const double d = __dsub_rn(1.0, __dmul_rn(4.0 / 3.0, __ddiv_rn((double)(diag - identical), __dsub_rn(length, gapc))));
+  if (d <= kDoubleEpsilon) return false;
+  *out = __dmul_rn(-0.75, log(d));
+  return true;
+}
+
+// Int16 distance of KimCnt counters: SWG-MPI ComputeDistance (Program.cs:271-276) or, with
+// ms, the SWG-MS rules (Program.cs:555-668: Kimura2 capped at 10, undefined JukesCantor = 10).
+// A JukesCantor that SWG-MPI would throw on sets *throws and gives 0.
+__device__ __forceinline__ int16_t kim_distance(const KimCnt::T& c, int dist_fn, bool ms, int* throws) {
+  const int len = (int)(c.w0 >> 16), a = (int)(c.w0 & 0xFFFFu);
+  const int diag = (int)(c.w1 >> 16), b = (int)(c.w1 & 0xFFFFu);
+  double v;
+  if (dist_fn == 1) {
+    v = kimura2_value(len, diag, a, b);
+    if (ms && v > 10.0) v = 10.0;
+  } else if (!jukes_cantor_value(len, diag, a, &v)) {
+    if (!ms) {
+      if (throws) atomicExch(throws, 1);
+      return 0;
+    }
+    v = 10.0;
+  }
+  return cs_conv_i2_d(__dmul_rn(v, 32767.0));
 }
 
 }  // namespace swg

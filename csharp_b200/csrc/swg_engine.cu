@@ -814,7 +814,7 @@ int build_base(Base& B, const EngineParams& P, std::string* msg) {
   int rc;
   // the 32-bit lanes (reruns, NW, large alphabets) need the plain kernel's scratch
   B.carry_threads = (long)P.sms * 8 * 128;
-  if (cudaMalloc(&B.d_carry, plain_carry_bytes(P.mode == kModeNw ? kModeNw : kModeSwgMpi, B.carry_threads, B.maxcol)) != cudaSuccess) {
+  if (cudaMalloc(&B.d_carry, plain_carry_bytes(P.mode == kModeNw ? kModeNw : kModeSwgMpi, B.carry_threads, B.maxcol, P.protein ? 0 : P.dist_fn)) != cudaSuccess) {
     cudaGetLastError(); B.d_carry = nullptr; *msg = "cudaMalloc 32-bit lane scratch"; return SW_E_OOM;
   }
   if (B.alpha > kMaxAlpha16 || P.lanes == SW_LANES_32) return SW_OK;
@@ -1021,7 +1021,8 @@ class EngineImpl : public Engine {
       for (int x = starts[r]; x <= ends[r]; x++) blk[x] = r;
     int rc;
     const bool nw = P.mode == kModeNw;
-    pl.plain_only = B.alpha > kMaxAlpha16 || (nw && !B.nw16) || P.lanes == SW_LANES_32;
+    const bool kim = P.dist_fn != 0 && !P.protein;  // Kimura2 / JukesCantor: 32-bit lanes
+    pl.plain_only = B.alpha > kMaxAlpha16 || (nw && !B.nw16) || kim || P.lanes == SW_LANES_32;
     std::vector<int2> big;
     if (pl.plain_only) {
       for (int q = key.row_lo; q <= key.row_hi; q++)
@@ -1206,6 +1207,7 @@ class EngineImpl : public Engine {
     R.mirror = P.mode != kModeSwgMs;
     R.scores = P.scores; R.flags = P.flags;
     R.o = P.o; R.e = P.e; R.mode = P.mode; R.protein = P.protein;
+    R.dist_fn = P.dist_fn; R.throws = P.throws;
     R.carry = B.d_carry;
     const int grid = pl.big_count > 0 ? (int)(B.carry_threads / 128) : P.sms;
     return launch_plain_block(R, grid, 128, P.stream);
@@ -1270,7 +1272,8 @@ class QueryRunnerImpl : public QueryRunner {
     int rc = build_base(B_, P, msg);
     if (rc) return rc;
     N_ = P.nseq;
-    lanes16_ = !(B_.alpha > kMaxAlpha16 || P.mode == kModeNw || P.lanes == SW_LANES_32 || B_.alpha == 0);
+    lanes16_ = !(B_.alpha > kMaxAlpha16 || P.mode == kModeNw || P.lanes == SW_LANES_32 || B_.alpha == 0 ||
+                 (P.dist_fn != 0 && !P.protein));
     // database chunks in length order
     for (int c0 = 0; c0 < N_; c0 += kQueryChunk) {
       const int c1 = std::min(N_, c0 + kQueryChunk);
@@ -1457,6 +1460,7 @@ class QueryRunnerImpl : public QueryRunner {
     R.npairs = (long long)rerun_cap;
     R.scores = P_.scores; R.flags = P_.flags;
     R.o = P_.o; R.e = P_.e; R.mode = P_.mode; R.protein = P_.protein;
+    R.dist_fn = P_.dist_fn; R.throws = P_.throws;
     R.carry = B_.d_carry;
     R.qseq = T.qseq; R.qoff = T.qoff; R.qlen = T.qlen; R.qout = T.qout;
     const int g = big > 0 ? (int)(B_.carry_threads / 128) : P_.sms;

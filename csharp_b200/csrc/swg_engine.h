@@ -20,6 +20,8 @@ struct EngineParams {
   int max_score, max_abs_score;
   int o, e;
   int mode, protein, lanes;
+  int dist_fn = 0;         // SW_DIST_*: Kimura2 / JukesCantor run on 32-bit lanes
+  int* throws = nullptr;   // device flag: SWG-MPI JukesCantor met log(0)
   int ranks;
   int row_lo = 0, row_hi = -1;  // queries (s1 indices) aligned; row_hi < 0: all
   int16_t* out;

@@ -24,7 +24,7 @@ struct PlainJob {
   int o, e;
   int mode;
   int protein;
-  void* carry;             // device scratch, plain_carry_bytes(mode, threads, maxlen)
+  void* carry;             // device scratch, plain_carry_bytes(mode, threads, maxlen, dist_fn)
   const int2* list;        // optional explicit pairs (s1 index, s2 index); replaces the block
   const int* list_count;   // device count of list entries (at most npairs are read)
   // optional query set (serving; list mode only): s1 index = query slot, distance to qout[slot][j]
@@ -32,11 +32,14 @@ struct PlainJob {
   const int64_t* qoff;
   const int32_t* qlen;
   int16_t* const* qout;
+  int dist_fn;             // SW_DIST_*: Kimura2 / JukesCantor count transitions on the path
+  int* throws;             // set when SWG-MPI JukesCantor meets log(0) (the reference throws)
 };
 
 struct sw_pair_result_dev {
   int score, score_is_neg_inf;
   int end1, end2, start1, start2, identity, similarity, gaps, length;
+  int diag, transitions, transversions;  // for Kimura2 / JukesCantor
 };
 
 struct PairJob {
@@ -50,7 +53,7 @@ struct PairJob {
   sw_pair_result_dev* out;
 };
 
-size_t plain_carry_bytes(int mode, long threads, int maxlen);
+size_t plain_carry_bytes(int mode, long threads, int maxlen, int dist_fn = 0);
 cudaError_t launch_plain_block(const PlainJob& J, int grid, int block, cudaStream_t st);
 size_t pair_carry_bytes(int n);
 cudaError_t launch_align_pair(const PairJob& J, cudaStream_t st);

@@ -7,6 +7,7 @@
 // Substitution scores and column flags are staged in shared memory.
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
 #include "swg_device.cuh"
 #include "swg_internal.h"
 
@@ -180,14 +181,18 @@ __global__ void __launch_bounds__(128) plain_block_kernel(PlainJob J) {
     const int n = (int)(J.off[j + 1] - J.off[j]);
     int16_t d;
     if (LOCAL) {
-      if (m == 0 || n == 0) {
+      if constexpr (std::is_same<CP, KimCnt>::value) {
+        KimCnt::T c = KimCnt::origin();
+        if (m > 0 && n > 0) c = dp_pair<LOCAL, CP, K, false>(s1, m, s2, n, sc, fl, J.o, J.e, carry, stride).c;
+        d = kim_distance(c, J.dist_fn, J.mode == kModeSwgMs, J.throws);
+      } else if (m == 0 || n == 0) {
         d = fraction_distance(0, 0);
       } else {
         DpResult<CP> r = dp_pair<LOCAL, CP, K, false>(s1, m, s2, n, sc, fl, J.o, J.e, carry, stride);
         const uint32_t w = *reinterpret_cast<const uint32_t*>(&r.c);
         d = fraction_distance((int)(w & 0xFFFFu), (int)(w >> 16));
       }
-    } else {
+    } else if constexpr (std::is_same<CP, NwCnt>::value) {
       NwCnt::T c;
       if (m == 0 && n == 0) c = NwCnt::origin();
       else if (m == 0) c = NwCnt::row0(n);
@@ -223,6 +228,7 @@ __global__ void __launch_bounds__(32) align_pair_kernel(PairJob J) {
     out.score = 0;
     out.end1 = out.end2 = out.start1 = out.start2 = 0;
     out.identity = out.similarity = out.gaps = out.length = 0;
+    out.diag = out.transitions = out.transversions = 0;
   } else {
     DpResult<FullCnt> r = dp_pair<true, FullCnt, 4, true>(J.s1, J.m, J.s2, J.n, sc, fl, J.o, J.e,
                                                           reinterpret_cast<Carry<FullCnt>*>(J.carry), 1);
@@ -235,20 +241,25 @@ __global__ void __launch_bounds__(32) align_pair_kernel(PairJob J) {
     out.identity = r.c.id;
     out.similarity = r.c.sim;
     out.length = r.c.len;
+    out.diag = r.c.diag;
+    out.transitions = r.c.ts;
+    out.transversions = r.c.tv;
     out.gaps = r.c.len - ((r.bi - r.c.si) + (r.bj - r.c.sj) - r.c.len);
   }
   *J.out = out;
 }
 
 // ---- launchers -----------------------------------------------------------------------------
-size_t plain_carry_bytes(int mode, long threads, int maxlen) {
-  const size_t per = (mode == kModeNw) ? sizeof(Carry<NwCnt>) : sizeof(Carry<SwCnt>);
+size_t plain_carry_bytes(int mode, long threads, int maxlen, int dist_fn) {
+  const size_t per = (mode == kModeNw) ? sizeof(Carry<NwCnt>)
+                     : dist_fn ? sizeof(Carry<KimCnt>) : sizeof(Carry<SwCnt>);
   return per * (size_t)threads * (size_t)(maxlen + 1);
 }
 
 cudaError_t launch_plain_block(const PlainJob& J, int grid, int block, cudaStream_t st) {
   if (J.npairs == 0) return cudaSuccess;
   if (J.mode == kModeNw) plain_block_kernel<false, NwCnt, 8><<<grid, block, 0, st>>>(J);
+  else if (J.dist_fn && !J.protein) plain_block_kernel<true, KimCnt, 8><<<grid, block, 0, st>>>(J);
   else plain_block_kernel<true, SwCnt, 8><<<grid, block, 0, st>>>(J);
   return cudaGetLastError();
 }

@@ -94,7 +94,7 @@ def kat_pairs():
     return len(out)
 
 
-def mpi_job(name, seqs, matrix, atype, o, e, ranks):
+def mpi_job(name, seqs, matrix, atype, o, e, ranks, dist_fn=0):
     """The reference's block driver for `ranks` ranks: every rank's ComputeBlock calls plus the
     Scatter mirror, assembled into the full N x N matrix."""
     concat, off = pack(seqs)
@@ -113,7 +113,7 @@ def mpi_job(name, seqs, matrix, atype, o, e, ranks):
             computed = diag or (r > c and (r + c) % 2 == 0) or (r < c and (r + c) % 2 == 1)
             if not computed or bounds[r][0] > bounds[r][1] or bounds[c][0] > bounds[c][1]:
                 continue
-            got, n = oracle.ref_compute_block(matrix, atype, 0, o, e, concat, off, bounds[r][0],
+            got, n = oracle.ref_compute_block(matrix, atype, dist_fn, o, e, concat, off, bounds[r][0],
                                               bounds[r][1], bounds[c][0], bounds[c][1], diag)
             pairs += n
             rs, re_ = bounds[r]
@@ -122,11 +122,12 @@ def mpi_job(name, seqs, matrix, atype, o, e, ranks):
             if not diag:  # Scatter: the transposed block lands in rank c's rows
                 full[cs:ce + 1, rs:re_ + 1] = got[rs:re_ + 1, cs:ce + 1].T
     np.savez_compressed(HERE / name, concat=concat, offsets=off, matrix=np.frombuffer(matrix.encode(), np.uint8),
-                        alignment_type=atype, o=o, e=e, ranks=ranks, distances=full, pairs=pairs)
+                        alignment_type=atype, o=o, e=e, ranks=ranks, distances=full, pairs=pairs,
+                        dist_fn=dist_fn)
     return pairs
 
 
-def restated_job(name, seqs, matrix, mode, atype, o, e):
+def restated_job(name, seqs, matrix, mode, atype, o, e, dist_fn=0):
     """NW (mode 2) and SWG-MS (mode 1) from the oracle restatement (unpinned)."""
     concat, off = pack(seqs)
     N = len(seqs)
@@ -143,19 +144,32 @@ def restated_job(name, seqs, matrix, mode, atype, o, e):
                 full[i, j] = full[j, i] = d
             else:
                 r = oracle.align(s1, s2, sc, o, e, with_strings=True)
-                full[i, j] = oracle.ms_distance_i16(r["aln1"], r["aln2"], sc, protein=(atype == 0))
+                full[i, j] = oracle.ms_distance_i16(r["aln1"], r["aln2"], sc, protein=(atype == 0),
+                                                    dist_fn=dist_fn)
     np.savez_compressed(HERE / name, concat=concat, offsets=off, matrix=np.frombuffer(matrix.encode(), np.uint8),
-                        alignment_type=atype, o=o, e=e, mode=mode, distances=full)
+                        alignment_type=atype, o=o, e=e, mode=mode, distances=full, dist_fn=dist_fn)
+
+
+def distance_function_jobs(dna):
+    """Kimura2 / JukesCantor (Alignment.cs:254-348): SWG-MPI from the reference's own driver,
+    SWG-MS from the restatement."""
+    print("mpi kimura p3", mpi_job("mpi_kimura_p3.npz", dna, "EDNAFULL", 1, 16, 4, 3, dist_fn=1))
+    print("mpi jukes-cantor p1", mpi_job("mpi_jc_p1.npz", dna, "EDNAFULL", 1, 16, 4, 1, dist_fn=2))
+    restated_job("ms_kimura_restated.npz", dna[:24], "EDNAFULL", 1, 1, 16, 4, dist_fn=1)
+    restated_job("ms_jc_restated.npz", dna[:24], "EDNAFULL", 1, 1, 16, 4, dist_fn=2)
 
 
 def main():
     oracle.build()
     if not oracle.ref_available():
         raise SystemExit("oracle/_ref could not be built (reference sources missing)")
-    print("kat pairs", kat_pairs())
     rng = np.random.default_rng(7)
     dna = [s.tobytes() for s in synth.dna_family(46, 4, rng.integers(20, 160, 46), seed=11)]
     dna = dna[:20] + [b"", b"A", b"ACGTNNACGT"] + dna[20:]
+    if "--distance-functions" in sys.argv:  # only the Kimura2 / JukesCantor fixtures
+        distance_function_jobs(dna)
+        return
+    print("kat pairs", kat_pairs())
     print("mpi p1", mpi_job("mpi_p1.npz", dna, "EDNAFULL", 1, 16, 4, 1))
     print("mpi p3", mpi_job("mpi_p3.npz", dna, "EDNAFULL", 1, 16, 4, 3))
     print("mpi p4", mpi_job("mpi_p4.npz", dna, "EDNAFULL", 1, 14, 4, 4))
@@ -169,6 +183,7 @@ def main():
     restated_job("ms_restated.npz", dna[:24], "EDNAFULL", 1, 1, 16, 4)
     restated_job("ms_protein_restated.npz", pro[:20], "BLOSUM62", 1, 0, 10, 1)
     restated_job("nw_protein_restated.npz", pro[:20], "BLOSUM62", 2, 0, 10, 1)
+    distance_function_jobs(dna)
     del ScoringMatrix
 
 

@@ -283,3 +283,83 @@ def test_nw_engine_matches_plain_kernel(cs, matrix, o, e, atype):
         got, _, _ = eng.all_pairs(3)
         want3, _, _ = ref.all_pairs(3)
         np.testing.assert_array_equal(got, want3)
+
+
+@pytest.mark.parametrize("name", ["mpi_kimura_p3.npz", "mpi_jc_p1.npz"])
+def test_kimura_and_jukes_cantor_match_reference_driver(cs, name):
+    """Kimura2 / JukesCantor distances of the reference's own block driver (Alignment.cs:254-348)."""
+    z = load_npz(name)
+    eng = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), float(z["o"]), float(z["e"]),
+                    distance_fn=int(z["dist_fn"]))
+    eng.upload(concat=z["concat"], offsets=z["offsets"])
+    full, pairs, _ = eng.all_pairs(int(z["ranks"]))
+    assert pairs == int(z["pairs"])
+    np.testing.assert_array_equal(full, z["distances"])
+    N = len(z["offsets"]) - 1
+    blk, _ = eng.compute_block(0, N - 1, 0, N - 1, True)
+    off = ~np.eye(N, dtype=bool)
+    if int(z["ranks"]) == 1:
+        np.testing.assert_array_equal(blk[off], z["distances"][off])
+
+
+@pytest.mark.parametrize("name", ["ms_kimura_restated.npz", "ms_jc_restated.npz"])
+def test_ms_kimura_and_jukes_cantor_match_restatement(cs, name):
+    z = load_npz(name)
+    eng = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), float(z["o"]), float(z["e"]), mode=cs.SWG_MS,
+                    distance_fn=int(z["dist_fn"]))
+    eng.upload(concat=z["concat"], offsets=z["offsets"])
+    full, _, _ = eng.all_pairs(1)
+    np.testing.assert_array_equal(full, z["distances"])
+
+
+def test_kimura_single_pair_matches_reference_kats(cs, kats):
+    eng = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4, distance_fn=cs.KIMURA2)
+    n = 0
+    for k in kats:
+        if k["matrix"] != "EDNAFULL" or k.get("kimura2") is None or (k["o"], k["e"]) != (16, 4):
+            continue
+        assert eng.align(k["s1"], k["s2"]).Distance == k["kimura2"], k
+        n += 1
+    assert n > 50
+
+
+@pytest.mark.parametrize("dist_fn,mode", [(1, 0), (2, 0), (1, 1), (2, 1)])
+def test_kimura_and_jukes_cantor_against_oracle(cs, oracle_mod, dist_fn, mode):
+    """Uneven lengths up to 700 and multi-strip pairs: every pair against the oracle."""
+    from csharp_b200 import synth
+    rng = np.random.default_rng(90 + dist_fn)
+    lens = np.concatenate([rng.integers(1, 700, 60), [0, 1]])
+    seqs = [s.tobytes() for s in synth.dna_family(len(lens), 3, lens, seed=91)]
+    sm = cs.ScoringMatrix.Load("EDNAFULL")
+    eng = cs.Engine(sm, 16, 4, mode=mode, distance_fn=dist_fn).upload(seqs)
+    full, _, _ = eng.all_pairs(1)
+    concat, off = cs.pack_sequences(seqs)
+    N = len(seqs)
+    want, _ = oracle_mod.block(concat, off, 0, N - 1, 0, N - 1, True, mode, sm.Scores[:127, :127].astype(np.float32),
+                               16.0, 4.0, 1, dist_fn)
+    if mode == 0:
+        tri = np.tril(np.ones((N, N), dtype=bool), -1)
+        np.testing.assert_array_equal(full[tri], want[tri])
+        np.testing.assert_array_equal(full.T[tri], want[tri])
+    else:
+        np.testing.assert_array_equal(full, want)
+
+
+def test_jukes_cantor_log_zero_is_reported(cs, oracle_mod):
+    """A matrix whose mismatches score above zero aligns AAAA with CCCC: 1 - 4/3 < 0, where
+    SWG-MPI's JukesCantor throws (SW_E_THROWS) and SWG-MS gives 10."""
+    txt = "   A C\nA 1 2\nC 2 1\n"
+    m = cs.ScoringMatrix.Parse(txt, "POSMISMATCH")
+    seqs = [b"AAAA", b"CCCC"]
+    eng = cs.Engine(m, 16, 4, distance_fn=cs.JUKES_CANTOR).upload(seqs)
+    with pytest.raises(cs.SwError) as ex:
+        eng.all_pairs(1)
+    assert ex.value.status == 8
+    with pytest.raises(cs.SwError):
+        eng.compute_block(0, 1, 0, 1, True)
+    ms = cs.Engine(m, 16, 4, mode=cs.SWG_MS, distance_fn=cs.JUKES_CANTOR).upload(seqs)
+    full, _, _ = ms.all_pairs(1)
+    concat, off = cs.pack_sequences(seqs)
+    want, _ = oracle_mod.block(concat, off, 0, 1, 0, 1, False, 1, m.Scores[:127, :127].astype(np.float32), 16.0, 4.0, 1, 2)
+    np.testing.assert_array_equal(full, want)
+    assert full[1, 0] == -10  # (short)(int)(10 * 32767): 327670 keeps its low 16 bits

@@ -51,7 +51,7 @@ def test_indp_formulation_matches_reference_kats(kats, oracle_mod):
 
 
 @pytest.mark.parametrize("name", ["mpi_p1.npz", "mpi_p3.npz", "mpi_p4.npz", "protein_mpi.npz",
-                                  "identity_mpi.npz"])
+                                  "identity_mpi.npz", "mpi_kimura_p3.npz", "mpi_jc_p1.npz"])
 def test_restatement_block_driver_matches_reference(name, oracle_mod):
     z = load_npz(name)
     seqs = unpack(z)
@@ -70,7 +70,8 @@ def test_restatement_block_driver_matches_reference(name, oracle_mod):
                 continue
             (rs, re_), (cs, ce) = bounds[r], bounds[c]
             blk, _ = oracle_mod.block(z["concat"], z["offsets"], rs, re_, cs, ce, diag, 0, sc,
-                                      float(z["o"]), float(z["e"]), int(z["alignment_type"]))
+                                      float(z["o"]), float(z["e"]), int(z["alignment_type"]),
+                                      int(z.get("dist_fn", 0)))
             if diag:
                 full[rs:re_ + 1, cs:ce + 1] = blk
             else:
