@@ -225,6 +225,65 @@ def serving(cs, device, seconds, load):
             "max_admitted": st["max_active"], "waves": st["waves"], "all_ok": ok}
 
 
+def other_configs(cs, device, stream, flush):
+    """The other benchmark configurations, each timed with inputs resident (CUDA events, L2
+    flushed): the 16-bit engine on the whole job and, on a subset, the same pairs on 32-bit
+    lanes (results compared entry by entry; parity with the reference is the tests' job)."""
+    import torch
+    from csharp_b200 import pack_sequences, synth
+    out = {}
+    specs = [
+        ("cfg1", "plain SW-Gotoh: 1,000 DNA, 20 roots of 500 nt, lengths 200-600, EDNAFULL 16/4",
+         lambda: synth.config1(), "EDNAFULL", 16, 4, cs.SWG_MPI, cs.NUCLEIC, 1000),
+        ("cfg2", "NW global: 10,000 DNA, lengths uniform 300-500, 100 roots, EDNAFULL 16/4",
+         lambda: synth.config2(), "EDNAFULL", 16, 4, cs.NW, cs.NUCLEIC, 1500),
+        ("cfg4", "protein SW-Gotoh: 5,000 of the 20,000-sequence set (20 amino acids, lengths 100-1000, "
+                 "500 roots), BLOSUM62 10/1",
+         lambda: synth.config4(cs.ScoringMatrix.Load("BLOSUM62").Scores, n=5000), "BLOSUM62", 10, 1,
+         cs.SWG_MPI, cs.PROTEIN, 1000),
+    ]
+
+    def timed(eng, n, dst):
+        eng.all_pairs_device(dst.data_ptr(), n, 1)
+        torch.cuda.synchronize()
+        flush.zero_()
+        b, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b.record(stream)
+        eng.all_pairs_device(dst.data_ptr(), n, 1)
+        e.record(stream)
+        torch.cuda.synchronize()
+        return b.elapsed_time(e), eng.query("cells")
+
+    for name, desc, gen, matrix, o, e, mode, atype, sub in specs:
+        seqs = gen()
+        concat, off = pack_sequences(seqs)
+        n = len(seqs)
+        eng = cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=mode, alignment_type=atype, device=device)
+        eng.upload(concat=concat, offsets=off)
+        eng.use_stream(stream.cuda_stream)
+        full = torch.zeros((n, n), dtype=torch.int16, device="cuda")
+        ms, cells = timed(eng, n, full)
+        m = min(sub, n)
+        a16 = cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=mode, alignment_type=atype, device=device)
+        a32 = cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=mode, alignment_type=atype, device=device, lanes=32)
+        r = {}
+        for tag, x in (("lanes16", a16), ("lanes32", a32)):
+            x.upload(concat=concat[: off[m]], offsets=off[: m + 1])
+            x.use_stream(stream.cuda_stream)
+            d = torch.zeros((m, m), dtype=torch.int16, device="cuda")
+            t, c = timed(x, m, d)
+            r[tag] = (t, c, d)
+        out[name] = {"workload": desc, "gcups": round(cells / (ms * 1e-3) / 1e9, 1), "ms": round(ms, 1),
+                     "cells": int(cells), "pairs": n * (n - 1) // 2,
+                     "subset": f"first {m} sequences: 16-bit lanes {r['lanes16'][1] / (r['lanes16'][0] * 1e-3) / 1e9:.1f}"
+                               f" vs 32-bit lanes {r['lanes32'][1] / (r['lanes32'][0] * 1e-3) / 1e9:.1f} GCUPS",
+                     "subset_identical": bool(torch.equal(r["lanes16"][2], r["lanes32"][2]))}
+        for x in (eng, a16, a32):
+            x.close()
+        del full
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -237,11 +296,20 @@ def main():
     ap.add_argument("--skip-extras", action="store_true", help="headline only (profiling runs)")
     ap.add_argument("--rows-per-lane", type=int, default=0, help="engine rows per lane (0 = per query)")
     ap.add_argument("--serving-only", action="store_true", help="only the serving workload (one JSON line)")
+    ap.add_argument("--configs-only", action="store_true", help="only configurations 1, 2 and 4 (one JSON line)")
     ap.add_argument("--serve-seconds", type=float, default=SERVE["seconds"])
     a = ap.parse_args()
     if a.serving_only:
         import csharp_b200 as cs
         print(json.dumps({"serving": serving(cs, 0, a.serve_seconds, SERVE["load"])}))
+        return 0
+    if a.configs_only:
+        import torch
+        import csharp_b200 as cs
+        st = torch.cuda.Stream()
+        torch.cuda.set_stream(st)
+        fl = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        print(json.dumps({"configs": other_configs(cs, 0, st, fl)}))
         return 0
     if a.impl == "reference":
         return run_reference_arm(a)
@@ -420,6 +488,7 @@ def main():
                                       "speedup": round(times["plain"] / times["batched"], 2),
                                       "identical": bool(np.array_equal(a2[offd], a3[offd]))}
         sub.close()
+        result["configs"] = other_configs(cs, local, stream, flush)
         result["serving"] = serving(cs, local, a.serve_seconds, SERVE["load"])
     if rank == 0:
         print(json.dumps(result))
