@@ -295,6 +295,7 @@ def main():
     ap.add_argument("--ref-step-seconds", type=float, default=6.0)
     ap.add_argument("--skip-extras", action="store_true", help="headline only (profiling runs)")
     ap.add_argument("--rows-per-lane", type=int, default=0, help="engine rows per lane (0 = per query)")
+    ap.add_argument("--no-autotune", action="store_true", help="built-in rows-per-lane costs instead of measured ones")
     ap.add_argument("--serving-only", action="store_true", help="only the serving workload (one JSON line)")
     ap.add_argument("--configs-only", action="store_true", help="only configurations 1, 2 and 4 (one JSON line)")
     ap.add_argument("--serve-seconds", type=float, default=SERVE["seconds"])
@@ -340,6 +341,8 @@ def main():
     def share_of(step):
         return (step * world + rank) % SHARES
 
+    # the autotuner times each rows-per-lane choice on a sample of this job (before any timing)
+    tuned = None if (a.no_autotune or a.rows_per_lane) else eng.autotune(out.data_ptr(), N)
     share_cells = {}
     eng.set_option("plan_only", 1)  # plan and capture every share before timing; launch nothing
     for s in range(SHARES):
@@ -392,7 +395,8 @@ def main():
                                      f"clipped 50-1500, 200 roots, EDNAFULL, open 16 / extend 4, PercentIdentity Int16",
                          "step": f"one rank's share of an {SHARES}-rank MPI run of the job (whole job = {SHARES} steps)",
                          "l2": "flushed (256 MB write) before every timed step",
-                         "cells_per_job": int(sum(share_cells.values())), "pairs_per_job": N * (N - 1) // 2},
+                         "cells_per_job": int(sum(share_cells.values())), "pairs_per_job": N * (N - 1) // 2,
+                         "rows_per_lane_costs": tuned or "built-in"},
               "gpu_launches": int(launches), "clocks": clk.summary()}
 
     if rank == 0:

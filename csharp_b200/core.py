@@ -237,6 +237,13 @@ class Engine:
         self._ck(L.load().sw_compute_rank_blocks(self._h, rank, world, C.c_void_p(d_out_ptr), ld, C.byref(p)))
         return p.value
 
+    def autotune(self, d_out_ptr, ld):
+        """Measures the rows-per-lane costs on this device and job (writing sample distances
+        into the N x N device matrix at d_out_ptr); returns {rows per lane: weight}."""
+        w = np.zeros(7, dtype=np.int32)
+        self._ck(L.load().sw_autotune(self._h, C.c_void_p(d_out_ptr), ld, L.ptr(w)))
+        return {k: int(v) for k, v in zip((4, 6, 8, 10, 12, 14, 16), w)}
+
     def rerun_count(self):
         n = C.c_int64()
         self._ck(L.load().sw_last_rerun_count(self._h, C.byref(n)))

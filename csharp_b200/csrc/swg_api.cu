@@ -428,6 +428,8 @@ int sw_last_rerun_count(const sw_ctx* ctx_, int64_t* count) {
   return rc ? fail(ctx, rc, msg) : SW_OK;
 }
 
+static swg::EngineParams db_params(sw_ctx* ctx);
+
 static int run_engine(sw_ctx* ctx, int32_t ranks, int row_lo, int row_hi, int16_t* d_out,
                       int64_t ld, int64_t* pairs, int64_t* cells) {
   if (!ctx->d_seq) return fail(ctx, SW_E_STATE, "no sequences uploaded");
@@ -485,6 +487,26 @@ int sw_compute_rank_blocks(sw_ctx* ctx, int32_t rank, int32_t world, int16_t* d_
   }
   int64_t cells = 0;
   return run_engine(ctx, world, st[rank], en[rank], d_out, ld, pairs, &cells);
+}
+
+int sw_autotune(sw_ctx* ctx, int16_t* d_out, int64_t ld, int32_t weights[7]) {
+  if (!ctx) return SW_E_ARG;
+  if (!ctx->d_seq) return fail(ctx, SW_E_STATE, "no sequences uploaded");
+  if (!d_out || ld < ctx->nseq) return fail(ctx, SW_E_ARG, "bad output buffer");
+  cudaSetDevice(ctx->cfg.device);
+  if (!ctx->engine) {
+    ctx->engine = swg::Engine::create();
+    if (!ctx->engine) return fail(ctx, SW_E_OOM, "engine");
+  }
+  swg::EngineParams P = db_params(ctx);
+  P.out = d_out;
+  P.ld = ld;
+  std::string msg;
+  int w[7];
+  const int rc = ctx->engine->autotune(P, w, &msg);
+  if (rc) return fail(ctx, rc, msg);
+  if (weights) for (int x = 0; x < 7; x++) weights[x] = w[x];
+  return check_throws(ctx);
 }
 
 int sw_query(sw_ctx* ctx, const char* key, int64_t* value) {

@@ -23,6 +23,7 @@
 // best score still reaches the trip threshold is rerun with 32-bit lanes.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <cmath>
 #include <map>
 #include <memory>
 #include <cstdio>
@@ -727,7 +728,7 @@ long k_weight(int k) {
 }
 
 // Rows per lane and passes for a query of m rows: fewest padded rows, then fewest passes.
-void choose_k(int m, int kov, int* K, int* passes, bool nw = false) {
+void choose_k(int m, int kov, int* K, int* passes, bool nw = false, const int* tuned = nullptr) {
   if (nw && kov > 14) kov = 14;  // NW kernels stop at 14 rows per lane
   if (kov) { *K = kov; *passes = std::max(1, (m + 32 * kov - 1) / (32 * kov)); return; }
   long best = -1;
@@ -737,7 +738,8 @@ void choose_k(int m, int kov, int* K, int* passes, bool nw = false) {
     // rows computed (padding included) times the per-row cost of that K (few rows per lane do
     // not amortise the per-step shuffles, loads and column bookkeeping); ties go to fewer passes
     // (each pass adds a wavefront fill and a scratch round trip)
-    const long weight = nw ? k_weight_nw(k) : k_weight(k);
+    const int ki = (int)(std::find(std::begin(kKs), std::end(kKs), k) - std::begin(kKs));
+    const long weight = (tuned && tuned[ki] > 0) ? tuned[ki] : nw ? k_weight_nw(k) : k_weight(k);
     const long cost = (long)p * 32 * k * weight * 16 + p;
     if (best < 0 || cost < best) { best = cost; *K = k; *passes = p; }
   }
@@ -754,6 +756,7 @@ struct Bin {
   size_t smem = 0;
   int grid = 0;
   size_t scratch_off = 0;  // words into the pass scratch (bins run concurrently)
+  double padded = 0;       // cells computed, padding rows included
 };
 
 template <class T>
@@ -950,6 +953,72 @@ class EngineImpl : public Engine {
     return -1;
   }
 
+  int autotune(const EngineParams& P0, int weights[7], std::string* msg) override {
+    int rc;
+    for (int x = 0; x < kNumK; x++) weights[x] = 0;
+    if (!base_) {
+      base_.reset(new Base());
+      if ((rc = build_base(*base_, P0, msg))) { base_.reset(); return rc; }
+    }
+    Base& B = *base_;
+    const bool nw = P0.mode == kModeNw;
+    const bool kim = P0.dist_fn != 0 && !P0.protein;
+    if (B.alpha > kMaxAlpha16 || (nw && !B.nw16) || kim || P0.lanes == SW_LANES_32 || P0.nseq < 2)
+      return SW_OK;  // 32-bit lanes only: nothing to choose
+    if ((rc = ensure_streams(msg))) return rc;
+    // sample: the last R queries of the set (each aligned against every earlier sequence), with
+    // at least 12 work items per CTA slot of the 2-CTA kernels so that tails do not decide the
+    // timing, and at most ~4e11 cells
+    const int N = P0.nseq;
+    double mean = 0;
+    for (int l : B.len) mean += l;
+    mean = std::max(1.0, mean / N);
+    const int chunk = std::min(std::max(opt_.chunk, 32), kMaxChunk);
+    const double nchunks = std::ceil((double)N / chunk);
+    const double r_items = std::ceil(12.0 * 2 * P0.sms / nchunks);
+    const double r_cells = 4e11 / ((double)N * mean * mean);
+    const int R = (int)std::max(8.0, std::min((double)N, std::max(r_items, std::min(r_cells, 4 * r_items))));
+    EngineParams P = P0;
+    P.ranks = 1;
+    P.row_lo = N - R;
+    P.row_hi = N - 1;
+    const PlanKey key{P.mode, 1, P.row_lo, P.row_hi};
+    const int saved = opt_.k_override;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    double rate[kNumK] = {0};
+    for (int x = 0; x < kNumK; x++) {
+      if (nw && kKs[x] > 14) continue;
+      opt_.k_override = kKs[x];
+      Plan pl;
+      if ((rc = build_plan(P, key, pl, msg))) break;
+      double padded = 0;
+      for (auto& bn : pl.bins) padded += bn.padded;
+      float ms = 0;
+      cudaError_t e = cudaEventRecord(t0, P.stream);
+      if (e == cudaSuccess) e = enqueue(P, key, pl);
+      if (e == cudaSuccess) e = cudaEventRecord(t1, P.stream);
+      if (e == cudaSuccess) e = cudaEventSynchronize(t1);
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, t0, t1);
+      if (e != cudaSuccess) { *msg = std::string("autotune: ") + cudaGetErrorString(e); rc = SW_E_CUDA; break; }
+      if (ms > 0 && padded > 0) rate[x] = padded / ms;
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    opt_.k_override = saved;
+    if (rc) return rc;
+    double best = 0;
+    for (double r : rate) best = std::max(best, r);
+    if (best <= 0) return SW_OK;
+    for (int x = 0; x < kNumK; x++)
+      weights[x] = rate[x] > 0 ? (int)std::lround(100.0 * best / rate[x]) : 0;
+    for (int x = 0; x < kNumK; x++) opt_.k_weights[x] = weights[x];
+    plans_.clear();  // later plans use the measured costs
+    last_ = nullptr;
+    return SW_OK;
+  }
+
   int rerun_count(cudaStream_t st, int64_t* count, std::string* msg) override {
     *count = 0;
     if (!last_ || last_->plain_only || !last_->d_rerun_count) return SW_OK;
@@ -1059,7 +1128,7 @@ class EngineImpl : public Engine {
     for (int q = key.row_lo; q <= key.row_hi; q++) {
       const int m = B.len[q];
       int K, passes;
-      choose_k(m, opt_.k_override, &K, &passes, nw);
+      choose_k(m, opt_.k_override, &K, &passes, nw, opt_.k_weights);
       // a profile beyond shared memory (long queries, large alphabets): 32-bit lanes
       const bool fits = engine_smem(A, passes * 32 * K, B.maxcol, K, nw) <= 227 * 1024;
       const int bi = (int)(std::find(std::begin(kKs), std::end(kKs), K) - std::begin(kKs));
@@ -1103,6 +1172,7 @@ class EngineImpl : public Engine {
         bn.max_passes = std::max(bn.max_passes, passes);
         bn.items.push_back(make_int4(q, c * chunk, std::min(N, (c + 1) * chunk), passes));
         bn.cost.push_back((double)passes * 32 * K * (lsum + 31.0 * cnt) * k_weight(K));
+        bn.padded += (double)passes * 32 * K * lsum;
         bn.total_cost += bn.cost.back();
       }
     }

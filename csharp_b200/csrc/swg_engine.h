@@ -36,6 +36,8 @@ struct EngineOptions {
   int chunk = 512;                 // database entries per work item
   int k_override = 0;              // 0: per-query choice; else rows per lane
   int plan_only = 0;               // build plans and graphs, launch nothing
+  int k_weights[7] = {0, 0, 0, 0, 0, 0, 0};  // cost per row at 4, 6, ..., 16 rows per lane
+                                             // (0: built-in table; set by autotune)
 };
 
 class Engine {
@@ -52,6 +54,10 @@ class Engine {
   virtual int64_t stat(const char* key) const = 0;
   // Pairs the last run gave to 32-bit lanes (static guard plus tripped lanes); waits on st.
   virtual int rerun_count(cudaStream_t st, int64_t* count, std::string* msg) = 0;
+  // Times every rows-per-lane choice forced on a sample of the job's queries (writing their
+  // distances to p.out) and installs the measured per-row costs for later plans; weights gets
+  // them (100 = the cheapest, 0 = not measured).  Waits on p.stream.
+  virtual int autotune(const EngineParams& p, int weights[7], std::string* msg) = 0;
 };
 
 // ---- query mode (serving) ---------------------------------------------------------------------

@@ -30,6 +30,7 @@ EXPORTS = [
     "sw_write_full_matrix", "sw_write_ms_block", "sw_read_ms_block_dims", "sw_read_ms_block_values",
     "sw_measure_int_peak", "sw_set_option", "sw_compute_rank_blocks", "sw_query",
     "sw_compute_block_static", "sw_submit_job", "sw_poll", "sw_serve_stats", "sw_serve_drain",
+    "sw_autotune",
 ]
 
 
@@ -116,6 +117,7 @@ def load():
         "sw_poll": ([P, I64, I32, C.POINTER(I32), C.POINTER(sw_job_info)], I32),
         "sw_serve_stats": ([P, C.POINTER(sw_serve_counters)], I32),
         "sw_serve_drain": ([P], I32),
+        "sw_autotune": ([P, P, I64, P], I32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

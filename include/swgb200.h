@@ -163,6 +163,14 @@ int sw_compute_rank_blocks(sw_ctx* ctx, int32_t rank, int32_t world_size, int16_
  * Unknown keys are SW_E_ARG. */
 int sw_set_option(sw_ctx* ctx, const char* key, int64_t value);
 
+/* Autotuner (no reference counterpart; the reference has one aligner loop): times every
+ * rows-per-lane choice of the 16-bit engine (4, 6, ..., 16) forced on a sample of this context's
+ * queries (the last ones, each against every earlier sequence; their distances are written to
+ * d_out, an N x N device matrix) and installs the measured cost per row, so later jobs choose the
+ * tile shape per query from this device and this length mix.  weights (optional) receives them
+ * (100 = the cheapest, 0 = not measured). */
+int sw_autotune(sw_ctx* ctx, int16_t* d_out, int64_t ld_out, int32_t weights[7]);
+
 /* Counters of the last engine call: "launches" (kernels it enqueued), "pairs", "cells",
  * "bins" (rows-per-lane classes used), "alphabet" (distinct residue bytes), "planned_items",
  * and, after waiting for the device, "items" (work items taken), "lane16_pairs" (pairs finished

@@ -363,3 +363,15 @@ def test_jukes_cantor_log_zero_is_reported(cs, oracle_mod):
     want, _ = oracle_mod.block(concat, off, 0, 1, 0, 1, False, 1, m.Scores[:127, :127].astype(np.float32), 16.0, 4.0, 1, 2)
     np.testing.assert_array_equal(full, want)
     assert full[1, 0] == -10  # (short)(int)(10 * 32767): 327670 keeps its low 16 bits
+
+
+def test_autotune_installs_weights_and_changes_no_result(cs):
+    import torch
+    z = load_npz("mpi_p3.npz")
+    eng = _golden_engine(cs, z)
+    N = len(z["offsets"]) - 1
+    d = torch.zeros((N, N), dtype=torch.int16, device="cuda")
+    w = eng.autotune(d.data_ptr(), N)
+    assert min(w.values()) >= 100 and sorted(w.values())[0] == 100
+    full, _, _ = eng.all_pairs(3)
+    np.testing.assert_array_equal(full, z["distances"])
