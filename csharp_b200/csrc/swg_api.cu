@@ -517,7 +517,7 @@ int sw_query(sw_ctx* ctx, const char* key, int64_t* value) {
     return SW_OK;
   }
   if (k != "launches" && k != "bins" && k != "alphabet" && k != "items" && k != "lane16_pairs" &&
-      k != "tripped" && k != "planned_items")
+      k != "tripped" && k != "planned_items" && k != "box_fallbacks")
     return fail(ctx, SW_E_ARG, "unknown counter " + k);
   *value = ctx->engine ? ctx->engine->stat(key) : 0;
   return SW_OK;
@@ -554,6 +554,7 @@ int sw_set_option(sw_ctx* ctx, const char* key, int64_t value) {
   swg::EngineOptions& o = ctx->engine->options();
   if (k == "int16_threshold") o.int16_threshold = value;
   else if (k == "use_graph") o.use_graph = value ? 1 : 0;
+  else if (k == "two_pass") o.two_pass = value ? 1 : 0;
   else if (k == "chunk") {
     if (value < 32 || value > 1024) return fail(ctx, SW_E_ARG, "chunk must be in [32, 1024]");
     o.chunk = (int)value;

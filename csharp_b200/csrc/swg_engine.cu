@@ -73,6 +73,9 @@ struct EngineJob {
   int mpad;                 // profile rows staged (passes * 32 * K of the bin)
   int protein;              // NW distance rule: similarity over the full length
   unsigned long long* stats; // [0] items taken, [1] pairs finished in 16-bit lanes, [2] tripped
+  int4* box;                // two-pass: pairs whose counters the box kernel finds
+  int* box_count;
+  int box_cap;
   // Query mode (serving): s1 is query slot q of a separate set, s2 every database entry of the
   // chunk, the distance goes to qout[q][d].  Raw residue bytes index qtab/qflag (row 127 = pad).
   int qmode;
@@ -276,6 +279,108 @@ __device__ __forceinline__ void align_two(const uint32_t* __restrict__ prof, int
       const int sB = (int)(int16_t)(BEST[r] >> 16) - J.bias;
       if (sA > bestA) { bestA = sA; rowA = row; cntA = bcA[r]; }
       if (sB > bestB) { bestB = sB; rowB = row; cntB = bcB[r]; }
+    }
+  }
+}
+
+// Score-only counterpart of align_two (first pass of the two-pass SW path): the same DP without
+// counters, keeping per query row the best V and the column where it was first reached.  Returns
+// per lane half the best score and its cell (row and column, 0-based) in the reference's order
+// (first strictly greater in row-major order).
+template <int K, int NP>
+__device__ __forceinline__ void score_two(const uint32_t* __restrict__ prof, int mpad, int passes,
+                                          const uint8_t* __restrict__ ca,
+                                          const uint8_t* __restrict__ cb, int ncols,
+                                          const EngineJob& J, uint32_t* __restrict__ scr,
+                                          int lane, int& bestA, int& rowA, uint32_t& colA,
+                                          int& bestB, int& rowB, uint32_t& colB) {
+  const uint32_t bias2 = (uint32_t)J.bias * 0x10001u;
+  const uint32_t O2 = (uint32_t)J.o * 0x10001u, E2 = (uint32_t)J.e * 0x10001u;
+  const uint32_t sent2 = (uint32_t)(J.bias - J.o - J.e) * 0x10001u;  // -infinity + bias
+  const uint32_t best0 = (uint32_t)(J.bias - 1) * 0x10001u;          // below any V
+  const uint32_t vo_top = (uint32_t)(J.bias - J.o) * 0x10001u;        // V(0,j) - o + bias
+  const int plane = NP * mpad;
+  bestA = bestB = -1;
+  rowA = rowB = 0;
+  colA = colB = 0u;
+  for (int p = 0; p < passes; p++) {
+    uint32_t VOL[K], H[K], BEST[K], bcA[K], bcB[K];
+#pragma unroll
+    for (int r = 0; r < K; r++) {
+      VOL[r] = vo_top; H[r] = sent2; BEST[r] = best0;
+      bcA[r] = bcB[r] = 0u;
+    }
+    uint32_t uVO = vo_top, uG = sent2, dVO = vo_top;
+    const int pbase = p * 32 * K;
+    const uint32_t* pl = prof + pbase + lane * 4;
+    const int nsteps = ncols + 31;
+    for (int s = 0; s < nsteps; s++) {
+      const uint32_t bVO = __shfl_up_sync(0xffffffffu, uVO, 1);
+      const uint32_t bG = __shfl_up_sync(0xffffffffu, uG, 1);
+      uint32_t VOU, GU;
+      if (lane == 0) {
+        if (p == 0 || s >= ncols) {
+          VOU = vo_top; GU = sent2;
+        } else {
+          const uint2 x = *reinterpret_cast<const uint2*>(scr + (long)s * 2);
+          VOU = x.x; GU = x.y;
+        }
+      } else {
+        VOU = bVO; GU = bG;
+      }
+      uint32_t VOD = dVO;
+      dVO = VOU;
+      const int col = 32 + s - lane;
+      const uint32_t colv = (uint32_t)(s - lane);  // this lane's column at this step
+      const int xa = ca[col], xb = cb[col];
+      const uint32_t* pla = pl + xa * plane;
+      const uint32_t* phb = pl + xb * plane + (NP == 3 ? mpad : 0);
+      auto cell = [&](const int r, const uint32_t pl_r, const uint32_t ph_r) {
+        const uint32_t F = (NP == 3) ? VOD + pl_r + ph_r : mad_hi16(ph_r, VOD + pl_r);
+        const uint32_t G = __vmaxs2(VOU, GU - E2);
+        H[r] = __vmaxs2(VOL[r], H[r] - E2);
+        const uint32_t V = __vmaxs2(__vimax3_s16x2(F, G, H[r]), bias2);
+        bool hiB, loA;
+        BEST[r] = vmax2(BEST[r], V, hiB, loA);  // kept unless V is strictly greater
+        bcA[r] = loA ? bcA[r] : colv;
+        bcB[r] = hiB ? bcB[r] : colv;
+        const uint32_t VO = V - O2;
+        VOD = VOL[r];
+        VOL[r] = VO;
+        VOU = VO;
+        GU = G;
+      };
+#pragma unroll
+      for (int g = 0; g < K / 4; g++) {
+        const uint4 PL = *reinterpret_cast<const uint4*>(pla + g * 128);
+        const uint4 PH = *reinterpret_cast<const uint4*>(phb + g * 128);
+        cell(g * 4 + 0, PL.x, PH.x);
+        cell(g * 4 + 1, PL.y, PH.y);
+        cell(g * 4 + 2, PL.z, PH.z);
+        cell(g * 4 + 3, PL.w, PH.w);
+      }
+      if (K % 4 == 2) {
+        const int t2 = (K / 4) * 128 - lane * 2;
+        const uint2 PL = *reinterpret_cast<const uint2*>(pla + t2);
+        const uint2 PH = *reinterpret_cast<const uint2*>(phb + t2);
+        cell(K - 2, PL.x, PH.x);
+        cell(K - 1, PL.y, PH.y);
+      }
+      uVO = VOU;
+      uG = GU;
+      if (lane == 31 && p + 1 < passes) {
+        const int j = s - 31;
+        if (j >= 0 && j < ncols) *reinterpret_cast<uint2*>(scr + (long)j * 2) = make_uint2(uVO, uG);
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < K; r++) {
+      const int row = pbase + lane * K + r;
+      const int sA = (int)(int16_t)(BEST[r] & 0xFFFFu) - J.bias;
+      const int sB = (int)(int16_t)(BEST[r] >> 16) - J.bias;
+      if (sA > bestA) { bestA = sA; rowA = row; colA = bcA[r]; }
+      if (sB > bestB) { bestB = sB; rowB = row; colB = bcB[r]; }
     }
   }
 }
@@ -487,9 +592,13 @@ __device__ __forceinline__ void emit(const EngineJob& J, int q, int d, int16_t d
   if (J.mode != kModeSwgMs) J.out[(long long)d * J.ld + q] = dist;
 }
 
-template <int K, int NP, bool NW>
-__global__ void __launch_bounds__(warps_of(K, NW) * 32, ctas_of(K, NW)) engine_kernel(EngineJob J) {
-  constexpr int kEngWarps = warps_of(K, NW);
+// What a kernel instantiation computes per pair.
+enum { kKindSw = 0, kKindNw = 1, kKindScore = 2 };
+
+template <int K, int NP, int KIND>
+__global__ void __launch_bounds__(warps_of(K) * 32, ctas_of(K)) engine_kernel(EngineJob J) {
+  constexpr bool NW = KIND == kKindNw;
+  constexpr int kEngWarps = warps_of(K);
   constexpr int kScr = NW ? kScrWordsNw : kScrWords;
   extern __shared__ __align__(16) uint8_t smem[];
   uint32_t* prof = reinterpret_cast<uint32_t*>(smem);
@@ -577,6 +686,37 @@ __global__ void __launch_bounds__(warps_of(K, NW) * 32, ctas_of(K, NW)) engine_k
       }
       for (int k = 32 + ncols + lane; k < 64 + ncols; k += 32) { ca[k] = (uint8_t)J.A; cb[k] = (uint8_t)J.A; }
       __syncwarp();
+      if constexpr (KIND == kKindScore) {
+        // first pass of the two-pass path: best score and cell; the box kernel finds the counters
+        int bA = 0, rA = 0, bB = 0, rB = 0;
+        uint32_t cA = 0, cB = 0;
+        if (m > 0 && ncols > 0)
+          score_two<K, NP>(prof, J.mpad, passes, ca, cb, ncols, J, scr, lane, bA, rA, cA, bB, rB, cB);
+        warp_best(bA, rA, cA);
+        warp_best(bB, rB, cB);
+        if (lane == 0) {
+          unsigned long long done16 = 0;
+          auto finish = [&](int d, int n, int best, int row, uint32_t col) {
+            if (m == 0 || n == 0 || best <= 0) {  // empty alignment: 0/0
+              emit(J, q, d, fraction_distance(0, 0));
+              done16++;
+            } else if (best > J.thresh) {  // the 16-bit lanes may have saturated: 32-bit DP
+              const int w = atomicAdd(J.rerun_count, 1);
+              if (w < J.rerun_cap) J.rerun[w] = make_int2(q, d);
+              atomicAdd(J.stats + 2, 1ull);
+            } else {
+              const int w = atomicAdd(J.box_count, 1);
+              if (w < J.box_cap) J.box[w] = make_int4(q, d, best, (int)(((uint32_t)(row + 1) << 16) | (col + 1)));
+              done16++;
+            }
+          };
+          finish(dA, nA, bA, rA, cA);
+          if (dB >= 0) finish(dB, nB, bB, rB, cB);
+          atomicAdd(J.stats + 1, done16);
+        }
+        __syncwarp();
+        continue;
+      }
       if constexpr (NW) {
         uint32_t a0 = 0, a1 = 0, b0 = 0, b1 = 0;
         if (m > 0 && ncols > 0)
@@ -668,33 +808,32 @@ auto with_k(int K, Fn fn) {
 
 // The kernel instantiation for K rows per lane, the planes of alphabet A and the DP kind.
 template <class Fn>
-auto with_kp(int K, int A, bool nw, Fn fn) {
+auto with_kp(int K, int A, int kind, Fn fn) {
   return with_k(K, [&](auto k) {
     constexpr int kk = decltype(k)::value;
-    if (nw) {
-      if (planes_of(A) == 3) return fn(engine_kernel<kk, 3, true>, warps_of(kk, true) * 32);
-      return fn(engine_kernel<kk, 2, true>, warps_of(kk, true) * 32);
-    }
-    if (planes_of(A) == 3) return fn(engine_kernel<kk, 3, false>, warps_of(kk) * 32);
-    return fn(engine_kernel<kk, 2, false>, warps_of(kk) * 32);
+    const int threads = warps_of(kk) * 32;
+    const bool p3 = planes_of(A) == 3;
+    if (kind == kKindNw) return p3 ? fn(engine_kernel<kk, 3, kKindNw>, threads) : fn(engine_kernel<kk, 2, kKindNw>, threads);
+    if (kind == kKindScore) return p3 ? fn(engine_kernel<kk, 3, kKindScore>, threads) : fn(engine_kernel<kk, 2, kKindScore>, threads);
+    return p3 ? fn(engine_kernel<kk, 3, kKindSw>, threads) : fn(engine_kernel<kk, 2, kKindSw>, threads);
   });
 }
 
-cudaError_t allow_smem_k(int K, int A, bool nw, size_t smem) {
-  return with_kp(K, A, nw, [&](auto kern, int) {
+cudaError_t allow_smem_k(int K, int A, int kind, size_t smem) {
+  return with_kp(K, A, kind, [&](auto kern, int) {
     return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   });
 }
 
-cudaError_t launch_engine_k(int K, const EngineJob& J, int grid, size_t smem, cudaStream_t st) {
-  return with_kp(K, J.A, J.mode == kModeNw, [&](auto kern, int threads) {
+cudaError_t launch_engine_k(int K, int kind, const EngineJob& J, int grid, size_t smem, cudaStream_t st) {
+  return with_kp(K, J.A, kind, [&](auto kern, int threads) {
     kern<<<grid, threads, smem, st>>>(J);
     return cudaGetLastError();
   });
 }
 
-int occupancy_k(int K, int A, bool nw, size_t smem) {
-  return with_kp(K, A, nw, [&](auto kern, int threads) {
+int occupancy_k(int K, int A, int kind, size_t smem) {
+  return with_kp(K, A, kind, [&](auto kern, int threads) {
     int n = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem);
     return n;
@@ -788,9 +927,14 @@ struct Base {
   size_t scratch_bytes = 0;
   void* d_carry = nullptr;
   long carry_threads = 0;
+  // two-pass SW: the first pass's (pair, best score, best cell) list and the box kernel's scratch
+  int4* d_box = nullptr;
+  int* d_box_count = nullptr;
+  long long box_cap = 0;
   ~Base() {
     cudaFree(d_code); cudaFree(d_sorted); cudaFree(d_lettab); cudaFree(d_flagtab);
     cudaFree(d_scratch); cudaFree(d_carry);
+    cudaFree(d_box); cudaFree(d_box_count);
   }
 };
 
@@ -870,6 +1014,7 @@ int build_base(Base& B, const EngineParams& P, std::string* msg) {
 // One job (mode, world size, query range): its work items, 32-bit pair list and CUDA graph.
 struct Plan {
   bool plain_only = false;
+  int kind = kKindSw;       // the bins' kernel: SW with counters, NW, or the two-pass first pass
   bool zeroes_diagonal = false;
   int thresh = 0;
   std::vector<Bin> bins;
@@ -930,6 +1075,7 @@ class EngineImpl : public Engine {
     if (k == "launches") {
       int64_t n = 2;  // the 32-bit lane kernel and the rerun-count reset
       for (auto& bn : last_->bins) n += bn.items.empty() ? 0 : 1;
+      if (!last_->plain_only && last_->kind == kKindScore) n += 1;  // the box kernel
       return n + (last_->zeroes_diagonal ? 1 : 0);
     }
     if (k == "bins") {
@@ -938,12 +1084,12 @@ class EngineImpl : public Engine {
       return n;
     }
     if (k == "alphabet") return base_ ? base_->alpha : 0;
-    if (k == "items" || k == "lane16_pairs" || k == "tripped") {
+    if (k == "items" || k == "lane16_pairs" || k == "tripped" || k == "box_fallbacks") {
       if (!last_->d_stats) return 0;
       unsigned long long h[4] = {0, 0, 0, 0};
       cudaDeviceSynchronize();
       cudaMemcpy(h, last_->d_stats, sizeof(h), cudaMemcpyDeviceToHost);
-      return (int64_t)(k == "items" ? h[0] : (k == "lane16_pairs" ? h[1] : h[2]));
+      return (int64_t)(k == "items" ? h[0] : k == "lane16_pairs" ? h[1] : k == "tripped" ? h[2] : h[3]);
     }
     if (k == "planned_items") {
       int64_t n = 0;
@@ -1092,6 +1238,7 @@ class EngineImpl : public Engine {
     const bool nw = P.mode == kModeNw;
     const bool kim = P.dist_fn != 0 && !P.protein;  // Kimura2 / JukesCantor: 32-bit lanes
     pl.plain_only = B.alpha > kMaxAlpha16 || (nw && !B.nw16) || kim || P.lanes == SW_LANES_32;
+    pl.kind = nw ? kKindNw : opt_.two_pass ? kKindScore : kKindSw;
     std::vector<int2> big;
     if (pl.plain_only) {
       for (int q = key.row_lo; q <= key.row_hi; q++)
@@ -1195,8 +1342,8 @@ class EngineImpl : public Engine {
       if (bn.items.empty()) continue;
       bn.smem = engine_smem(A, bn.mpad, B.maxcol, bn.K, nw);
       if (bn.smem > 227 * 1024) { *msg = "query profile exceeds shared memory"; return SW_E_UNSUPPORTED; }
-      if (allow_smem_k(bn.K, A, nw, bn.smem) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
-      const int occ = std::max(1, occupancy_k(bn.K, A, nw, bn.smem));
+      if (allow_smem_k(bn.K, A, pl.kind, bn.smem) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
+      const int occ = std::max(1, occupancy_k(bn.K, A, pl.kind, bn.smem));
       bn.grid = (int)std::min<long>((long)P.sms * occ, (long)bn.items.size());
       bn.scratch_off = scr_words;
       if (bn.max_passes > 1) scr_words += (size_t)bn.grid * warps_of(bn.K, nw) * B.maxcol * (nw ? kScrWordsNw : kScrWords);
@@ -1218,7 +1365,24 @@ class EngineImpl : public Engine {
       B.scratch_bytes = scr;
     }
     pl.big_count = (int)big.size();
-    pl.rerun_cap = (int)std::min<int64_t>(pl.npairs + 1, (int64_t)big.size() + std::max<int64_t>(1 << 16, pl.npairs / 16));
+    // the two-pass box kernel gives its long pairs (family members) to the 32-bit lanes too
+    const int64_t spare = std::max<int64_t>(1 << 16, pl.npairs / (pl.kind == kKindScore ? 4 : 16));
+    pl.rerun_cap = (int)std::min<int64_t>(pl.npairs + 1, (int64_t)big.size() + spare);
+    if (pl.kind == kKindScore) {
+      if (pl.npairs > B.box_cap) {  // one list for every plan (plans run one after another)
+        for (auto& kv : plans_) if (kv.second->graph) { cudaGraphExecDestroy(kv.second->graph); kv.second->graph = nullptr; }
+        cudaFree(B.d_box);
+        B.d_box = nullptr;
+        B.box_cap = 0;
+        if (cudaMalloc(&B.d_box, sizeof(int4) * (size_t)std::max<int64_t>(pl.npairs, 1)) != cudaSuccess) {
+          cudaGetLastError(); *msg = "cudaMalloc two-pass pair list"; return SW_E_OOM;
+        }
+        B.box_cap = std::max<int64_t>(pl.npairs, 1);
+      }
+      if (!B.d_box_count && cudaMalloc(&B.d_box_count, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError(); B.d_box_count = nullptr; *msg = "cudaMalloc two-pass count"; return SW_E_OOM;
+      }
+    }
     std::vector<int2> rl(big);
     rl.resize((size_t)pl.rerun_cap);
     if ((rc = upload_vec(&pl.d_rerun, rl, msg, "rerun list"))) return rc;
@@ -1233,6 +1397,8 @@ class EngineImpl : public Engine {
     if (pl.zeroes_diagonal)
       zero_diagonal_kernel<<<(P.nseq + 255) / 256, 256, 0, P.stream>>>(P.out, P.ld, P.nseq);
     set_int_kernel<<<1, 1, 0, P.stream>>>(pl.d_rerun_count, pl.big_count);
+    const bool two = !pl.plain_only && pl.kind == kKindScore;
+    if (two && (e = cudaMemsetAsync(B.d_box_count, 0, sizeof(int), P.stream)) != cudaSuccess) return e;
     if (!pl.plain_only) {
       if ((e = cudaMemsetAsync(pl.d_counters, 0, sizeof(int) * (pl.bins.size() + 1), P.stream)) != cudaSuccess) return e;
       if ((e = cudaMemsetAsync(pl.d_stats, 0, sizeof(unsigned long long) * 4, P.stream)) != cudaSuccess) return e;
@@ -1247,6 +1413,7 @@ class EngineImpl : public Engine {
       J.scratch = B.d_scratch; J.maxcol = B.maxcol;
       J.rerun = pl.d_rerun; J.rerun_count = pl.d_rerun_count; J.rerun_cap = pl.rerun_cap;
       J.stats = pl.d_stats;
+      J.box = B.d_box; J.box_count = B.d_box_count; J.box_cap = (int)std::min<long long>(B.box_cap, 0x7fffffff);
       // fork: each bin on its own stream, all after the resets above; join before the rerun
       const bool fork = pl.order.size() > 1;
       if (fork && (e = cudaEventRecord(fork_, P.stream)) != cudaSuccess) return e;
@@ -1260,12 +1427,26 @@ class EngineImpl : public Engine {
         J.counter = pl.d_counters + b;
         J.mpad = bn.mpad;
         J.scratch = B.d_scratch + bn.scratch_off;
-        if ((e = launch_engine_k(bn.K, J, bn.grid, bn.smem, st)) != cudaSuccess) return e;
+        if ((e = launch_engine_k(bn.K, pl.kind, J, bn.grid, bn.smem, st)) != cudaSuccess) return e;
         if (fork) {
           if ((e = cudaEventRecord(join_[x], st)) != cudaSuccess) return e;
           if ((e = cudaStreamWaitEvent(P.stream, join_[x], 0)) != cudaSuccess) return e;
         }
       }
+    }
+    if (two) {
+      // counters of the first pass's best cells from boxes around their traceback paths
+      BoxJob X;
+      std::memset(&X, 0, sizeof(X));
+      X.seq = P.seq; X.off = P.off;
+      X.list = B.d_box; X.count = B.d_box_count;
+      X.out = P.out; X.ld = P.ld; X.mirror = P.mode != kModeSwgMs;
+      X.scores = P.scores; X.flags = P.flags; X.o = P.o; X.e = P.e;
+      X.carry = B.d_carry; X.maxlen = B.maxcol;
+      X.budget = 1 << 16;
+      X.rerun = pl.d_rerun; X.rerun_count = pl.d_rerun_count; X.rerun_cap = pl.rerun_cap;
+      X.stats = pl.d_stats;
+      if ((e = launch_box(X, (int)(B.carry_threads / 128), 128, P.stream)) != cudaSuccess) return e;
     }
     // 32-bit lanes: pairs the static guard routed here, those whose 16-bit lanes tripped, or all
     PlainJob R;
@@ -1279,7 +1460,7 @@ class EngineImpl : public Engine {
     R.o = P.o; R.e = P.e; R.mode = P.mode; R.protein = P.protein;
     R.dist_fn = P.dist_fn; R.throws = P.throws;
     R.carry = B.d_carry;
-    const int grid = pl.big_count > 0 ? (int)(B.carry_threads / 128) : P.sms;
+    const int grid = (pl.big_count > 0 || two) ? (int)(B.carry_threads / 128) : P.sms;
     return launch_plain_block(R, grid, 128, P.stream);
   }
 
@@ -1474,8 +1655,8 @@ class QueryRunnerImpl : public QueryRunner {
     for (size_t x = 0; x < ls.size(); x++) {
       smem[x] = engine_smem(A, ls[x].mpad, B_.maxcol, ls[x].K);
       if (smem[x] > 227 * 1024) { *msg = "query profile exceeds shared memory"; return SW_E_UNSUPPORTED; }
-      if (allow_smem_k(ls[x].K, A, false, smem[x]) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
-      const int occ = std::max(1, occupancy_k(ls[x].K, A, false, smem[x]));
+      if (allow_smem_k(ls[x].K, A, kKindSw, smem[x]) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
+      const int occ = std::max(1, occupancy_k(ls[x].K, A, kKindSw, smem[x]));
       grid[x] = std::min(P_.sms * occ, ls[x].count);
       scr_off[x] = scr_words;
       if (ls[x].max_passes > 1) scr_words += (size_t)grid[x] * warps_of(ls[x].K) * B_.maxcol * kScrWords;
@@ -1515,7 +1696,7 @@ class QueryRunnerImpl : public QueryRunner {
         J.counter = W.d_counters + ls[x].b;
         J.mpad = ls[x].mpad;
         J.scratch = W.d_scratch + scr_off[x];
-        if ((e = launch_engine_k(ls[x].K, J, grid[x], smem[x], s2)) != cudaSuccess) return cuda_err(e, msg);
+        if ((e = launch_engine_k(ls[x].K, kKindSw, J, grid[x], smem[x], s2)) != cudaSuccess) return cuda_err(e, msg);
         if (fork) {
           if ((e = cudaEventRecord(W.join[x], s2)) != cudaSuccess) return cuda_err(e, msg);
           if ((e = cudaStreamWaitEvent(st, W.join[x], 0)) != cudaSuccess) return cuda_err(e, msg);

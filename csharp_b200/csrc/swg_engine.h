@@ -36,6 +36,7 @@ struct EngineOptions {
   int chunk = 512;                 // database entries per work item
   int k_override = 0;              // 0: per-query choice; else rows per lane
   int plan_only = 0;               // build plans and graphs, launch nothing
+  int two_pass = 1;                // SW: score-only pass, then counters from boxes (box kernel)
   int k_weights[7] = {0, 0, 0, 0, 0, 0, 0};  // cost per row at 4, 6, ..., 16 rows per lane
                                              // (0: built-in table; set by autotune)
 };

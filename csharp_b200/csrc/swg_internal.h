@@ -53,6 +53,31 @@ struct PairJob {
   sw_pair_result_dev* out;
 };
 
+// Second step of the two-pass SW path: for each pair the first pass found the best cell
+// (ie, je) and score S of, the counters of the reference's traceback path from a DP confined to
+// a box around that path (see box_kernel).
+struct BoxJob {
+  const uint8_t* seq;
+  const int64_t* off;
+  const int4* list;        // (s1 index, s2 index, S, ie << 16 | je), ie and je 1-based
+  const int* count;
+  int16_t* out;
+  long long ld;
+  int mirror;
+  const int16_t* scores;   // device [128*128]
+  const uint8_t* flags;
+  int o, e;
+  void* carry;             // per thread (maxlen + 1) Carry<SwCnt>, interleaved by thread
+  int maxlen;
+  long long budget;        // cells of the reverse scan and of the box before giving up
+  int2* rerun;             // pairs given up on: the 32-bit full DP
+  int* rerun_count;
+  int rerun_cap;
+  unsigned long long* stats;  // [1] pairs finished in 16-bit lanes, [3] pairs given up on
+};
+
+cudaError_t launch_box(const BoxJob& J, int grid, int block, cudaStream_t st);
+
 size_t plain_carry_bytes(int mode, long threads, int maxlen, int dist_fn = 0);
 cudaError_t launch_plain_block(const PlainJob& J, int grid, int block, cudaStream_t st);
 size_t pair_carry_bytes(int n);

@@ -212,6 +212,216 @@ __global__ void __launch_bounds__(128) plain_block_kernel(PlainJob J) {
   }
 }
 
+// ---- box kernel: the counters of the best cell from a confined DP --------------------------------
+// The first pass gives, per pair, the best score S and the reference's traceback start cell
+// (ie, je) (first maximum in row-major order).  Every optimal local alignment ending there has,
+// at each of its cells, a suffix score (from that cell to (ie, je)) >= 0: its prefix up to the
+// cell scores at most the best V there, which is at most S.  A reverse DP anchored at (ie, je),
+// with every state below 0 pruned, therefore keeps all such alignments and finds all their first
+// pairs (the cells whose reverse score plus their own pair score equals S).  The box from the
+// smallest such row and column to (ie, je) contains the reference's traceback path, and a local
+// DP confined to the box (zero boundary) reproduces its values and pointer choices along that
+// path (each value on the path is reached inside the box, and off-path competitors can only be
+// lower than in the full matrix), so the counters of the box's first maximum, which is (ie, je)
+// with score S, are the traceback's.  Pairs whose scan or box exceed the budget, or whose box
+// does not end at S, go to the 32-bit full DP.
+// One warp per pair.  The reverse scan goes row by row (rows ie-1 .. 0) with the lanes on a
+// window of 64 positions (two chunks of 32) ending at the row's rightmost live position; within
+// a row the gap chain RHs(j) = max(X(j), RHs(j+1) - min(e, o)) is a max-plus prefix scan over
+// the lanes.  The box DP is a warp wavefront (lane = box row, 32 rows per pass).
+constexpr int kBoxWarps = 4;
+constexpr int kBoxMaxW = 256;   // box columns (else 32-bit full DP)
+constexpr int kBoxMaxH = 256;   // box rows
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ int scan_max_up(int y, int lane) {
+#pragma unroll
+  for (int k = 1; k < 32; k <<= 1) {
+    const int t = __shfl_up_sync(kFull, y, k);
+    if (lane >= k) y = max(y, t);
+  }
+  return y;
+}
+
+__global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
+  extern __shared__ __align__(16) uint8_t box_smem[];
+  int16_t* sc = reinterpret_cast<int16_t*>(box_smem);
+  uint8_t* fl = box_smem + sizeof(int16_t) * kTable * kTable;
+  for (int k = threadIdx.x; k < kTable * kTable; k += blockDim.x) {
+    sc[k] = J.scores[k];
+    fl[k] = J.flags[k];
+  }
+  __syncthreads();
+  constexpr int NEG = kNegInf;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // bottom row of a box pass: V, G, and the two counter words per column
+  int4* buf = reinterpret_cast<int4*>(box_smem + (sizeof(int16_t) + 1) * kTable * kTable) + warp * kBoxMaxW;
+  const long nwarps = (long)gridDim.x * kBoxWarps;
+  const int np = *J.count;
+  const int o = J.o, e = J.e, dchain = min(J.e, J.o);
+  for (long p = (long)blockIdx.x * kBoxWarps + warp; p < np; p += nwarps) {
+    const int4 rec = J.list[p];
+    const int q = rec.x, d = rec.y, S = rec.z;
+    const int ie = (int)((uint32_t)rec.w >> 16), je = rec.w & 0xFFFF;
+    const uint8_t* a = J.seq + J.off[q];
+    const uint8_t* b = J.seq + J.off[d];
+    // ---- reverse scan: positions (i, j) = residues consumed ----
+    int hi = je, lo = je;
+    int rwb0 = lane == 0 ? 0 : NEG, rwb1 = NEG, rgb0 = NEG, rgb1 = NEG;  // row below, pos lane / 32+lane
+    int cand_i = 1 << 30, cand_j = 1 << 30;
+    bool ok = true;
+    long long cells = 0;
+    for (int i = ie - 1; i >= 0; i--) {
+      const int arow = (int)a[i] * kTable;
+      // chunk 0: pos = lane, j = hi - lane
+      const int j0 = hi - lane;
+      int rwn0 = __shfl_up_sync(kFull, rwb0, 1);  // RW(i+1, j0+1)
+      if (lane == 0) rwn0 = NEG;
+      int pair0 = NEG;
+      if (rwn0 > NEG && j0 >= 0 && j0 < je) {
+        pair0 = (int)sc[arow + b[j0]] + rwn0;
+        if (pair0 == S) { cand_i = min(cand_i, i + 1); cand_j = min(cand_j, j0 + 1); }
+      }
+      const int x0 = max(pair0, rgb0 > NEG ? rgb0 - o : NEG);
+      int y0 = scan_max_up(x0 > NEG ? x0 + dchain * lane : NEG, lane);
+      int rh0 = (y0 > NEG && j0 >= 0) ? y0 - dchain * lane : NEG;  // RHs(i, j0)
+      int rhp0 = __shfl_up_sync(kFull, rh0, 1);                     // RHs(i, j0+1)
+      if (lane == 0) rhp0 = NEG;
+      int rw0 = max(x0, rhp0 > NEG ? rhp0 - o : NEG);
+      int rg0 = max(rgb0 > NEG ? rgb0 - e : NEG, rw0);
+      if (j0 < 0) rw0 = rg0 = NEG;
+      if (rw0 < 0) rw0 = NEG;
+      if (rg0 < 0) rg0 = NEG;
+      if (rh0 < 0) rh0 = NEG;
+      // chunk 1 (pos 32 + lane): when the row below reaches it or the gap chain runs into it
+      const int rh31 = __shfl_sync(kFull, rh0, 31);
+      int rw1 = NEG, rg1 = NEG;
+      if (hi - lo >= 31 || rh31 >= dchain) {
+        const int j1 = hi - 32 - lane;
+        int rwn1 = __shfl_up_sync(kFull, rwb1, 1);
+        const int last0 = __shfl_sync(kFull, rwb0, 31);
+        if (lane == 0) rwn1 = last0;
+        int pair1 = NEG;
+        if (rwn1 > NEG && j1 >= 0 && j1 < je) {
+          pair1 = (int)sc[arow + b[j1]] + rwn1;
+          if (pair1 == S) { cand_i = min(cand_i, i + 1); cand_j = min(cand_j, j1 + 1); }
+        }
+        const int x1 = max(pair1, rgb1 > NEG ? rgb1 - o : NEG);
+        int y1 = scan_max_up(x1 > NEG ? x1 + dchain * (32 + lane) : NEG, lane);
+        y1 = max(y1, __shfl_sync(kFull, y0, 31));  // the chain from chunk 0
+        int rh1 = (y1 > NEG && j1 >= 0) ? y1 - dchain * (32 + lane) : NEG;
+        int rhp1 = __shfl_up_sync(kFull, rh1, 1);
+        if (lane == 0) rhp1 = rh31;
+        rw1 = max(x1, rhp1 > NEG ? rhp1 - o : NEG);
+        rg1 = max(rgb1 > NEG ? rgb1 - e : NEG, rw1);
+        if (j1 < 0) rw1 = rg1 = NEG;
+        if (rw1 < 0) rw1 = NEG;
+        if (rg1 < 0) rg1 = NEG;
+        if (rh1 < 0) rh1 = NEG;
+        if (__shfl_sync(kFull, rh1, 31) >= dchain) ok = false;  // the chain leaves the window
+      }
+      cells += 64;
+      const unsigned b0 = __ballot_sync(kFull, rw0 > NEG || rg0 > NEG);
+      const unsigned b1 = __ballot_sync(kFull, rw1 > NEG || rg1 > NEG);
+      if (!ok || cells > J.budget) { ok = false; break; }
+      if (!b0 && !b1) break;  // nothing above can still reach (ie, je)
+      const int minpos = b0 ? __ffs(b0) - 1 : 32 + __ffs(b1) - 1;
+      const int maxpos = b1 ? 63 - __clz(b1) : 31 - __clz(b0);
+      // next row: positions relative to the new rightmost live column
+      const int sft = minpos, src = (lane + sft) & 31;
+      const int a0 = __shfl_sync(kFull, rw0, src), a1 = __shfl_sync(kFull, rw1, src);
+      const int g0 = __shfl_sync(kFull, rg0, src), g1 = __shfl_sync(kFull, rg1, src);
+      rwb0 = lane + sft < 32 ? a0 : (lane + sft < 64 ? a1 : NEG);
+      rgb0 = lane + sft < 32 ? g0 : (lane + sft < 64 ? g1 : NEG);
+      rwb1 = lane + sft < 32 ? a1 : NEG;
+      rgb1 = lane + sft < 32 ? g1 : NEG;
+      lo = hi - maxpos;
+      hi = hi - minpos;
+    }
+#pragma unroll
+    for (int k = 16; k >= 1; k >>= 1) {
+      cand_i = min(cand_i, __shfl_xor_sync(kFull, cand_i, k));
+      cand_j = min(cand_j, __shfl_xor_sync(kFull, cand_j, k));
+    }
+    const int ilo = cand_i, jlo = cand_j;
+    const int h = ie - ilo + 1, w = je - jlo + 1;
+    if (ilo > ie || jlo > je || h > kBoxMaxH || w > kBoxMaxW) ok = false;
+    // ---- box DP: rows ilo..ie (lanes), columns jlo..je (steps); local, zero boundary ----
+    int vcap = NEG;
+    uint32_t ccap = 0u;
+    if (ok) {
+      const int passes = (h + 31) / 32;
+      for (int ps = 0; ps < passes; ps++) {
+        const int t = ps * 32 + lane;  // box row of this lane
+        const bool row_ok = t < h;
+        const int arow = row_ok ? (int)a[ilo - 1 + t] * kTable : 0;
+        int vl = 0, hh = NEG;
+        uint32_t cl = 0u, ch = 0u;
+        int uv = 0, ug = NEG, dv = 0;
+        uint32_t ucv = 0u, ucg = 0u, dcv = 0u;
+        for (int s2 = 0; s2 < w + 31; s2++) {
+          const int bv = __shfl_up_sync(kFull, uv, 1), bg = __shfl_up_sync(kFull, ug, 1);
+          const uint32_t bcv = __shfl_up_sync(kFull, ucv, 1), bcg = __shfl_up_sync(kFull, ucg, 1);
+          const int c = s2 - lane;
+          int vu, gu;
+          uint32_t cvu, cgu;
+          if (lane == 0) {
+            if (ps == 0 || c < 0 || c >= w) { vu = 0; gu = NEG; cvu = cgu = 0u; }
+            else { const int4 x = buf[c]; vu = x.x; gu = x.y; cvu = (uint32_t)x.z; cgu = (uint32_t)x.w; }
+          } else {
+            vu = bv; gu = bg; cvu = bcv; cgu = bcg;
+          }
+          const int vd = dv;
+          const uint32_t cd = dcv;
+          dv = vu;
+          dcv = cvu;
+          if (row_ok && c >= 0 && c < w) {
+            const int col = (int)b[jlo - 1 + c];
+            int v, g;
+            uint32_t cv, cg;
+            gotoh_cell<true, SwCnt>((int)sc[arow + col], (uint32_t)fl[arow + col], vd, cd, vu, gu, cvu, cgu,
+                                    vl, cl, hh, ch, o, e, 0, 0, v, g, cv, cg);
+            vl = v;
+            cl = cv;
+            uv = v; ug = g; ucv = cv; ucg = cg;
+            if (t == h - 1 && c == w - 1) { vcap = v; ccap = cv; }
+          } else {
+            uv = 0; ug = NEG; ucv = ucg = 0u;  // outside the box: the zero boundary
+          }
+          if (lane == 31 && ps + 1 < passes && c >= 0 && c < w) buf[c] = make_int4(uv, ug, (int)ucv, (int)ucg);
+        }
+        __syncwarp();
+      }
+      const int holder = (h - 1) & 31;
+      vcap = __shfl_sync(kFull, vcap, holder);
+      ccap = __shfl_sync(kFull, ccap, holder);
+      if (vcap != S) ok = false;
+    }
+    if (lane == 0) {
+      if (!ok) {
+        const int wr = atomicAdd(J.rerun_count, 1);
+        if (wr < J.rerun_cap) J.rerun[wr] = make_int2(q, d);
+        atomicAdd(J.stats + 3, 1ull);
+        atomicAdd(J.stats + 1, ~0ull);  // no longer finished in 16-bit lanes
+      } else {
+        const int16_t dist = fraction_distance((int)(ccap & 0xFFFFu), (int)(ccap >> 16));
+        J.out[(long long)q * J.ld + d] = dist;
+        if (J.mirror) J.out[(long long)d * J.ld + q] = dist;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+cudaError_t launch_box(const BoxJob& J, int grid, int block, cudaStream_t st) {
+  const size_t smem = (sizeof(int16_t) + 1) * kTable * kTable + sizeof(int4) * kBoxMaxW * kBoxWarps;
+  const cudaError_t e = cudaFuncSetAttribute(box_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  (void)block;
+  box_kernel<<<grid, kBoxWarps * 32, smem, st>>>(J);
+  return cudaGetLastError();
+}
+
 // Single pair with every PairwiseAlignment field (SmithWatermanGotoh.Align).
 __global__ void __launch_bounds__(32) align_pair_kernel(PairJob J) {
   __shared__ int16_t sc[kTable * kTable];

@@ -375,3 +375,32 @@ def test_autotune_installs_weights_and_changes_no_result(cs):
     assert min(w.values()) >= 100 and sorted(w.values())[0] == 100
     full, _, _ = eng.all_pairs(3)
     np.testing.assert_array_equal(full, z["distances"])
+
+
+def test_two_pass_equals_one_pass_and_oracle(cs, oracle_mod):
+    """Score-only first pass + box kernel against the counter engine and the oracle, with
+    close family members (long alignments: boxes beyond the budget go to 32-bit lanes),
+    multi-pass queries, empty and 1-residue sequences."""
+    from csharp_b200 import synth
+    rng = np.random.default_rng(77)
+    lens = np.concatenate([rng.integers(20, 1400, 140), [0, 1, 2]])
+    seqs = [s.tobytes() for s in synth.dna_family(len(lens), 3, lens, seed=78, sub_range=(0.0, 0.05),
+                                                  indel_range=(0.0, 0.05))]
+    seqs += [s.tobytes() for s in synth.dna_family(60, 30, rng.integers(50, 600, 60), seed=79)]
+    one = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4).upload(seqs)
+    one.set_option("two_pass", 0)
+    want, pairs, _ = one.all_pairs(1)
+    two = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4).upload(seqs)
+    got, pairs2, _ = two.all_pairs(1)
+    assert pairs2 == pairs
+    assert two.query("box_fallbacks") > 0  # the near-identical family members
+    assert two.query("lane16_pairs") + two.rerun_count() == pairs
+    np.testing.assert_array_equal(got, want)
+    N = len(seqs)
+    sel = rng.choice(N * (N - 1) // 2, 3000, replace=False)
+    pr = np.array([(i, j) for i in range(N) for j in range(i)], dtype=np.int32)[sel]
+    ref = _oracle_distances(oracle_mod, seqs, pr, "EDNAFULL", 16.0, 4.0)
+    np.testing.assert_array_equal(got[pr[:, 0], pr[:, 1]], ref)
+    got3, _, _ = two.all_pairs(3)
+    want3, _, _ = one.all_pairs(3)
+    np.testing.assert_array_equal(got3, want3)
