@@ -396,7 +396,8 @@ def main():
                          "step": f"one rank's share of an {SHARES}-rank MPI run of the job (whole job = {SHARES} steps)",
                          "l2": "flushed (256 MB write) before every timed step",
                          "cells_per_job": int(sum(share_cells.values())), "pairs_per_job": N * (N - 1) // 2,
-                         "rows_per_lane_costs": tuned or "built-in"},
+                         "rows_per_lane_costs": (tuned if tuned and any(tuned.values()) else
+                                                 "built-in" + (" (kept by the autotuner)" if tuned else ""))},
               "gpu_launches": int(launches), "clocks": clk.summary()}
 
     if rank == 0:

@@ -45,9 +45,16 @@ namespace swg {
 // 10- and 12-row kernels 16% faster than 8.
 // NW carries twice the counter words and spills a little at these register caps; measured on
 // B200, the occupancy still pays more than the spills cost (8 warps with no spill: -9 %).
+// The score-only first pass keeps 5 registers per row: up to 10 rows fit 128 registers (2 CTAs
+// of 8 warps), 12-16 rows fit 168 (1 CTA of 12 warps).
 constexpr int kMaxWarps = 12;
-__host__ __device__ constexpr int warps_of(int K, bool nw = false) { return K <= 8 ? 8 : K <= 12 ? 12 : 8; }
-__host__ __device__ constexpr int ctas_of(int K, bool nw = false) { return K <= 8 ? 2 : 1; }
+constexpr int kKindScoreShape = 2;  // the kind value of the score-only kernels (see kKindScore)
+__host__ __device__ constexpr int warps_of(int K, int kind = 0) {
+  return kind == kKindScoreShape ? (K <= 10 ? 8 : 12) : (K <= 8 ? 8 : K <= 12 ? 12 : 8);
+}
+__host__ __device__ constexpr int ctas_of(int K, int kind = 0) {
+  return kind == kKindScoreShape ? (K <= 10 ? 2 : 1) : (K <= 8 ? 2 : 1);
+}
 constexpr int kMaxChunk = 1024;
 constexpr int kScrWords = 8;    // words of carried state per column in the pass scratch (SW)
 constexpr int kScrWordsNw = 12; // NW: V, G and two counter words per state and lane
@@ -596,9 +603,10 @@ __device__ __forceinline__ void emit(const EngineJob& J, int q, int d, int16_t d
 enum { kKindSw = 0, kKindNw = 1, kKindScore = 2 };
 
 template <int K, int NP, int KIND>
-__global__ void __launch_bounds__(warps_of(K) * 32, ctas_of(K)) engine_kernel(EngineJob J) {
+__global__ void __launch_bounds__(warps_of(K, KIND) * 32, ctas_of(K, KIND)) engine_kernel(EngineJob J) {
+  static_assert(kKindScore == kKindScoreShape, "score kind");
   constexpr bool NW = KIND == kKindNw;
-  constexpr int kEngWarps = warps_of(K);
+  constexpr int kEngWarps = warps_of(K, KIND);
   constexpr int kScr = NW ? kScrWordsNw : kScrWords;
   extern __shared__ __align__(16) uint8_t smem[];
   uint32_t* prof = reinterpret_cast<uint32_t*>(smem);
@@ -785,9 +793,9 @@ constexpr int kKs[kNumK] = {4, 6, 8, 10, 12, 14, 16};
 constexpr int kMaxAlpha16 = 32;
 int planes_of(int A) { return A > 8 ? 2 : 3; }
 
-size_t engine_smem(int A, int mpad, int maxcol, int K, bool nw = false) {
+size_t engine_smem(int A, int mpad, int maxcol, int K, int kind = 0) {
   const int cbuf = 64 + ((maxcol + 31) / 32) * 32;
-  return (size_t)(A + 1) * planes_of(A) * mpad * 4 + kMaxChunk * 4 + (size_t)warps_of(K, nw) * 2 * cbuf;
+  return (size_t)(A + 1) * planes_of(A) * mpad * 4 + kMaxChunk * 4 + (size_t)warps_of(K, kind) * 2 * cbuf;
 }
 
 __global__ void set_int_kernel(int* p, int v) { *p = v; }
@@ -811,7 +819,7 @@ template <class Fn>
 auto with_kp(int K, int A, int kind, Fn fn) {
   return with_k(K, [&](auto k) {
     constexpr int kk = decltype(k)::value;
-    const int threads = warps_of(kk) * 32;
+    const int threads = warps_of(kk, kind) * 32;
     const bool p3 = planes_of(A) == 3;
     if (kind == kKindNw) return p3 ? fn(engine_kernel<kk, 3, kKindNw>, threads) : fn(engine_kernel<kk, 2, kKindNw>, threads);
     if (kind == kKindScore) return p3 ? fn(engine_kernel<kk, 3, kKindScore>, threads) : fn(engine_kernel<kk, 2, kKindScore>, threads);
@@ -1112,18 +1120,14 @@ class EngineImpl : public Engine {
     if (B.alpha > kMaxAlpha16 || (nw && !B.nw16) || kim || P0.lanes == SW_LANES_32 || P0.nseq < 2)
       return SW_OK;  // 32-bit lanes only: nothing to choose
     if ((rc = ensure_streams(msg))) return rc;
-    // sample: the last R queries of the set (each aligned against every earlier sequence), with
-    // at least 12 work items per CTA slot of the 2-CTA kernels so that tails do not decide the
-    // timing, and at most ~4e11 cells
+    // sample: the last R queries of the set (each aligned against every earlier sequence); each
+    // K is timed on the sampled queries it serves in one pass with under 64 rows of padding
+    // (lengths in (32(K-2), 32K]), the regime where it competes with its neighbours
     const int N = P0.nseq;
     double mean = 0;
     for (int l : B.len) mean += l;
     mean = std::max(1.0, mean / N);
-    const int chunk = std::min(std::max(opt_.chunk, 32), kMaxChunk);
-    const double nchunks = std::ceil((double)N / chunk);
-    const double r_items = std::ceil(12.0 * 2 * P0.sms / nchunks);
-    const double r_cells = 4e11 / ((double)N * mean * mean);
-    const int R = (int)std::max(8.0, std::min((double)N, std::max(r_items, std::min(r_cells, 4 * r_items))));
+    const int R = (int)std::max(64.0, std::min((double)N, 2e12 / ((double)N * mean * mean)));
     EngineParams P = P0;
     P.ranks = 1;
     P.row_lo = N - R;
@@ -1137,15 +1141,18 @@ class EngineImpl : public Engine {
     for (int x = 0; x < kNumK; x++) {
       if (nw && kKs[x] > 14) continue;
       opt_.k_override = kKs[x];
+      opt_.m_lo = 32 * (kKs[x] - 2);
+      opt_.m_hi = 32 * kKs[x];
       Plan pl;
-      if ((rc = build_plan(P, key, pl, msg))) break;
+      rc = build_plan(P, key, pl, msg);
+      opt_.m_lo = opt_.m_hi = 0;
+      if (rc) break;
       double padded = 0;
       for (auto& bn : pl.bins) padded += bn.padded;
+      if (padded < 1e9) continue;  // too few sampled queries of these lengths: built-in cost
       float ms = 0;
-      cudaError_t e = cudaEventRecord(t0, P.stream);
-      if (e == cudaSuccess) e = enqueue(P, key, pl);
-      if (e == cudaSuccess) e = cudaEventRecord(t1, P.stream);
-      if (e == cudaSuccess) e = cudaEventSynchronize(t1);
+      cudaError_t e = enqueue(P, key, pl, t0, t1);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(P.stream);
       if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, t0, t1);
       if (e != cudaSuccess) { *msg = std::string("autotune: ") + cudaGetErrorString(e); rc = SW_E_CUDA; break; }
       if (ms > 0 && padded > 0) rate[x] = padded / ms;
@@ -1157,12 +1164,35 @@ class EngineImpl : public Engine {
     double best = 0;
     for (double r : rate) best = std::max(best, r);
     if (best <= 0) return SW_OK;
-    for (int x = 0; x < kNumK; x++)
-      weights[x] = rate[x] > 0 ? (int)std::lround(100.0 * best / rate[x]) : 0;
-    for (int x = 0; x < kNumK; x++) opt_.k_weights[x] = weights[x];
-    plans_.clear();  // later plans use the measured costs
+    int tuned[kNumK];
+    for (int x = 0; x < kNumK; x++) tuned[x] = rate[x] > 0 ? (int)std::lround(100.0 * best / rate[x]) : 0;
+    // keep the measured costs only if they plan the whole sample faster than the current ones
+    double t_cur = 0, t_new = 0;
+    const int saved_w[kNumK] = {opt_.k_weights[0], opt_.k_weights[1], opt_.k_weights[2], opt_.k_weights[3],
+                                opt_.k_weights[4], opt_.k_weights[5], opt_.k_weights[6]};
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    for (int variant = 0; variant < 2 && rc == SW_OK; variant++) {
+      for (int x = 0; x < kNumK; x++) opt_.k_weights[x] = variant ? tuned[x] : saved_w[x];
+      Plan pl;
+      if ((rc = build_plan(P, key, pl, msg))) break;
+      float ms = 0;
+      cudaError_t e = enqueue(P, key, pl, t0, t1);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(P.stream);
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, t0, t1);
+      if (e != cudaSuccess) { *msg = std::string("autotune: ") + cudaGetErrorString(e); rc = SW_E_CUDA; break; }
+      (variant ? t_new : t_cur) = ms;
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    const bool take = rc == SW_OK && t_new > 0 && t_new < t_cur;
+    for (int x = 0; x < kNumK; x++) {
+      opt_.k_weights[x] = take ? tuned[x] : saved_w[x];
+      weights[x] = take ? tuned[x] : 0;  // 0: the built-in table stays
+    }
+    plans_.clear();  // later plans use the chosen costs
     last_ = nullptr;
-    return SW_OK;
+    return rc;
   }
 
   int rerun_count(cudaStream_t st, int64_t* count, std::string* msg) override {
@@ -1274,10 +1304,11 @@ class EngineImpl : public Engine {
     for (int k : kKs) { Bin b; b.K = k; b.mpad = 0; pl.bins.push_back(b); }
     for (int q = key.row_lo; q <= key.row_hi; q++) {
       const int m = B.len[q];
+      if (opt_.m_hi > 0 && (m <= opt_.m_lo || m > opt_.m_hi)) continue;  // autotuner sample
       int K, passes;
       choose_k(m, opt_.k_override, &K, &passes, nw, opt_.k_weights);
       // a profile beyond shared memory (long queries, large alphabets): 32-bit lanes
-      const bool fits = engine_smem(A, passes * 32 * K, B.maxcol, K, nw) <= 227 * 1024;
+      const bool fits = engine_smem(A, passes * 32 * K, B.maxcol, K, pl.kind) <= 227 * 1024;
       const int bi = (int)(std::find(std::begin(kKs), std::end(kKs), K) - std::begin(kKs));
       const int bq = blk[q];
       for (int c = 0; c < nchunks; c++) {
@@ -1340,13 +1371,13 @@ class EngineImpl : public Engine {
     size_t scr_words = 0;
     for (auto& bn : pl.bins) {
       if (bn.items.empty()) continue;
-      bn.smem = engine_smem(A, bn.mpad, B.maxcol, bn.K, nw);
+      bn.smem = engine_smem(A, bn.mpad, B.maxcol, bn.K, pl.kind);
       if (bn.smem > 227 * 1024) { *msg = "query profile exceeds shared memory"; return SW_E_UNSUPPORTED; }
       if (allow_smem_k(bn.K, A, pl.kind, bn.smem) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
       const int occ = std::max(1, occupancy_k(bn.K, A, pl.kind, bn.smem));
       bn.grid = (int)std::min<long>((long)P.sms * occ, (long)bn.items.size());
       bn.scratch_off = scr_words;
-      if (bn.max_passes > 1) scr_words += (size_t)bn.grid * warps_of(bn.K, nw) * B.maxcol * (nw ? kScrWordsNw : kScrWords);
+      if (bn.max_passes > 1) scr_words += (size_t)bn.grid * warps_of(bn.K, pl.kind) * B.maxcol * (nw ? kScrWordsNw : kScrWords);
     }
     pl.order.clear();
     for (size_t b = 0; b < pl.bins.size(); b++)
@@ -1390,7 +1421,10 @@ class EngineImpl : public Engine {
     return upload_vec(&pl.d_rerun_count, cnt, msg, "rerun count");
   }
 
-  cudaError_t enqueue(const EngineParams& P, const PlanKey& key, Plan& pl) {
+  // bins_t0 / bins_t1 (optional): events recorded around the bins' kernels (the autotuner's
+  // timing: rows per lane changes them and nothing else).
+  cudaError_t enqueue(const EngineParams& P, const PlanKey& key, Plan& pl, cudaEvent_t bins_t0 = nullptr,
+                      cudaEvent_t bins_t1 = nullptr) {
     Base& B = *base_;
     cudaError_t e;
     pl.zeroes_diagonal = P.mode != kModeSwgMs && P.nseq > 0 && key.row_lo == 0 && key.row_hi == P.nseq - 1;
@@ -1415,6 +1449,7 @@ class EngineImpl : public Engine {
       J.stats = pl.d_stats;
       J.box = B.d_box; J.box_count = B.d_box_count; J.box_cap = (int)std::min<long long>(B.box_cap, 0x7fffffff);
       // fork: each bin on its own stream, all after the resets above; join before the rerun
+      if (bins_t0 && (e = cudaEventRecord(bins_t0, P.stream)) != cudaSuccess) return e;
       const bool fork = pl.order.size() > 1;
       if (fork && (e = cudaEventRecord(fork_, P.stream)) != cudaSuccess) return e;
       for (size_t x = 0; x < pl.order.size(); x++) {
@@ -1433,6 +1468,7 @@ class EngineImpl : public Engine {
           if ((e = cudaStreamWaitEvent(P.stream, join_[x], 0)) != cudaSuccess) return e;
         }
       }
+      if (bins_t1 && (e = cudaEventRecord(bins_t1, P.stream)) != cudaSuccess) return e;
     }
     if (two) {
       // counters of the first pass's best cells from boxes around their traceback paths

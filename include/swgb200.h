@@ -166,9 +166,11 @@ int sw_set_option(sw_ctx* ctx, const char* key, int64_t value);
 /* Autotuner (no reference counterpart; the reference has one aligner loop): times every
  * rows-per-lane choice of the 16-bit engine (4, 6, ..., 16) forced on a sample of this context's
  * queries (the last ones, each against every earlier sequence; their distances are written to
- * d_out, an N x N device matrix) and installs the measured cost per row, so later jobs choose the
- * tile shape per query from this device and this length mix.  weights (optional) receives them
- * (100 = the cheapest, 0 = not measured). */
+ * d_out, an N x N device matrix), each choice on the sampled queries it would serve in one pass,
+ * and installs the measured cost per row if the whole sample then runs faster than with the
+ * current costs, so later jobs choose the tile shape per query from this device and this length
+ * mix.  weights (optional) receives the installed costs (100 = the cheapest), all 0 when the
+ * current costs were kept. */
 int sw_autotune(sw_ctx* ctx, int16_t* d_out, int64_t ld_out, int32_t weights[7]);
 
 /* Counters of the last engine call: "launches" (kernels it enqueued), "pairs", "cells",
