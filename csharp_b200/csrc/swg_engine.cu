@@ -1474,11 +1474,11 @@ class EngineImpl : public Engine {
       // counters of the first pass's best cells from boxes around their traceback paths
       BoxJob X;
       std::memset(&X, 0, sizeof(X));
-      X.seq = P.seq; X.off = P.off;
+      X.seq = B.d_code; X.off = P.off;
       X.list = B.d_box; X.count = B.d_box_count;
       X.out = P.out; X.ld = P.ld; X.mirror = P.mode != kModeSwgMs;
-      X.scores = P.scores; X.flags = P.flags; X.o = P.o; X.e = P.e;
-      X.carry = B.d_carry; X.maxlen = B.maxcol;
+      X.lettab = B.d_lettab; X.flagtab = B.d_flagtab; X.A = B.alpha; X.o = P.o; X.e = P.e;
+      X.maxlen = B.maxcol;
       X.budget = 1 << 16;
       X.rerun = pl.d_rerun; X.rerun_count = pl.d_rerun_count; X.rerun_cap = pl.rerun_cap;
       X.stats = pl.d_stats;

@@ -57,17 +57,17 @@ struct PairJob {
 // (ie, je) and score S of, the counters of the reference's traceback path from a DP confined to
 // a box around that path (see box_kernel).
 struct BoxJob {
-  const uint8_t* seq;
+  const uint8_t* seq;      // dense residue codes 0..A-1 (the engine's), same offsets as the residues
   const int64_t* off;
   const int4* list;        // (s1 index, s2 index, S, ie << 16 | je), ie and je 1-based
   const int* count;
   int16_t* out;
   long long ld;
   int mirror;
-  const int16_t* scores;   // device [128*128]
-  const uint8_t* flags;
+  const int32_t* lettab;   // device [(A+1)^2] S(a, b) + o of the dense codes
+  const uint32_t* flagtab; // device [(A+1)^2] counted-column flags
+  int A;
   int o, e;
-  void* carry;             // per thread (maxlen + 1) Carry<SwCnt>, interleaved by thread
   int maxlen;
   long long budget;        // cells of the reverse scan and of the box before giving up
   int2* rerun;             // pairs given up on: the 32-bit full DP

@@ -243,19 +243,22 @@ __device__ __forceinline__ int scan_max_up(int y, int lane) {
   return y;
 }
 
+constexpr int kBoxMaxA1 = 33;  // letters + padding of the dense codes
+
 __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
-  extern __shared__ __align__(16) uint8_t box_smem[];
-  int16_t* sc = reinterpret_cast<int16_t*>(box_smem);
-  uint8_t* fl = box_smem + sizeof(int16_t) * kTable * kTable;
-  for (int k = threadIdx.x; k < kTable * kTable; k += blockDim.x) {
-    sc[k] = J.scores[k];
-    fl[k] = J.flags[k];
+  __shared__ int sc[kBoxMaxA1 * kBoxMaxA1];        // S(a, b) of the dense codes
+  __shared__ uint32_t fl[kBoxMaxA1 * kBoxMaxA1];
+  __shared__ int4 rowbuf[kBoxWarps * kBoxMaxW];
+  const int A1 = J.A + 1;
+  for (int k = threadIdx.x; k < A1 * A1; k += blockDim.x) {
+    sc[k] = J.lettab[k] - J.o;
+    fl[k] = J.flagtab[k];
   }
   __syncthreads();
   constexpr int NEG = kNegInf;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // bottom row of a box pass: V, G, and the two counter words per column
-  int4* buf = reinterpret_cast<int4*>(box_smem + (sizeof(int16_t) + 1) * kTable * kTable) + warp * kBoxMaxW;
+  int4* buf = rowbuf + warp * kBoxMaxW;
   const long nwarps = (long)gridDim.x * kBoxWarps;
   const int np = *J.count;
   const int o = J.o, e = J.e, dchain = min(J.e, J.o);
@@ -272,7 +275,7 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
     bool ok = true;
     long long cells = 0;
     for (int i = ie - 1; i >= 0; i--) {
-      const int arow = (int)a[i] * kTable;
+      const int arow = (int)a[i] * A1;
       // chunk 0: pos = lane, j = hi - lane
       const int j0 = hi - lane;
       int rwn0 = __shfl_up_sync(kFull, rwb0, 1);  // RW(i+1, j0+1)
@@ -354,7 +357,7 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
       for (int ps = 0; ps < passes; ps++) {
         const int t = ps * 32 + lane;  // box row of this lane
         const bool row_ok = t < h;
-        const int arow = row_ok ? (int)a[ilo - 1 + t] * kTable : 0;
+        const int arow = row_ok ? (int)a[ilo - 1 + t] * A1 : 0;
         int vl = 0, hh = NEG;
         uint32_t cl = 0u, ch = 0u;
         int uv = 0, ug = NEG, dv = 0;
@@ -379,7 +382,7 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
             const int col = (int)b[jlo - 1 + c];
             int v, g;
             uint32_t cv, cg;
-            gotoh_cell<true, SwCnt>((int)sc[arow + col], (uint32_t)fl[arow + col], vd, cd, vu, gu, cvu, cgu,
+            gotoh_cell<true, SwCnt>(sc[arow + col], fl[arow + col], vd, cd, vu, gu, cvu, cgu,
                                     vl, cl, hh, ch, o, e, 0, 0, v, g, cv, cg);
             vl = v;
             cl = cv;
@@ -414,11 +417,9 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
 }
 
 cudaError_t launch_box(const BoxJob& J, int grid, int block, cudaStream_t st) {
-  const size_t smem = (sizeof(int16_t) + 1) * kTable * kTable + sizeof(int4) * kBoxMaxW * kBoxWarps;
-  const cudaError_t e = cudaFuncSetAttribute(box_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
+  if (J.A + 1 > kBoxMaxA1) return cudaErrorInvalidValue;
   (void)block;
-  box_kernel<<<grid, kBoxWarps * 32, smem, st>>>(J);
+  box_kernel<<<grid, kBoxWarps * 32, 0, st>>>(J);
   return cudaGetLastError();
 }
 
