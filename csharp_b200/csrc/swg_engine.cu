@@ -1268,7 +1268,10 @@ class EngineImpl : public Engine {
     const bool nw = P.mode == kModeNw;
     const bool kim = P.dist_fn != 0 && !P.protein;  // Kimura2 / JukesCantor: 32-bit lanes
     pl.plain_only = B.alpha > kMaxAlpha16 || (nw && !B.nw16) || kim || P.lanes == SW_LANES_32;
-    pl.kind = nw ? kKindNw : opt_.two_pass ? kKindScore : kKindSw;
+    // Two passes pay off where the reverse scan's gap chain is short: it decays by min(o, e) per
+    // column, and with e = 1 (BLOSUM62 10/1) it runs past the box kernel's 64-column window for
+    // most pairs, which then go to 32-bit lanes: such jobs keep the one-pass counter kernel.
+    pl.kind = nw ? kKindNw : (opt_.two_pass && std::min(P.o, P.e) >= 2) ? kKindScore : kKindSw;
     std::vector<int2> big;
     if (pl.plain_only) {
       for (int q = key.row_lo; q <= key.row_hi; q++)
@@ -1396,8 +1399,8 @@ class EngineImpl : public Engine {
       B.scratch_bytes = scr;
     }
     pl.big_count = (int)big.size();
-    // the two-pass box kernel gives its long pairs (family members) to the 32-bit lanes too
-    const int64_t spare = std::max<int64_t>(1 << 16, pl.npairs / (pl.kind == kKindScore ? 4 : 16));
+    // the two-pass box kernel may give any pair to the 32-bit lanes: room for all of them
+    const int64_t spare = pl.kind == kKindScore ? pl.npairs : std::max<int64_t>(1 << 16, pl.npairs / 16);
     pl.rerun_cap = (int)std::min<int64_t>(pl.npairs + 1, (int64_t)big.size() + spare);
     if (pl.kind == kKindScore) {
       if (pl.npairs > B.box_cap) {  // one list for every plan (plans run one after another)

@@ -405,3 +405,20 @@ def test_two_pass_equals_one_pass_and_oracle(cs, oracle_mod):
     got3, _, _ = two.all_pairs(3)
     want3, _, _ = one.all_pairs(3)
     np.testing.assert_array_equal(got3, want3)
+
+
+def test_two_pass_with_most_pairs_falling_back(cs):
+    """Cheap gaps and close relatives: the box kernel gives most pairs to the 32-bit lanes, whose
+    list must hold them all (an overflow would raise in rerun_count)."""
+    from csharp_b200 import synth
+    rng = np.random.default_rng(5)
+    seqs = [s.tobytes() for s in synth.dna_family(90, 2, rng.integers(200, 700, 90), seed=6, sub_range=(0.0, 0.03),
+                                                  indel_range=(0.0, 0.03))]
+    one = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 3, 2).upload(seqs)
+    one.set_option("two_pass", 0)
+    want, pairs, _ = one.all_pairs(1)
+    two = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 3, 2).upload(seqs)
+    got, _, _ = two.all_pairs(1)
+    assert two.query("box_fallbacks") > pairs // 2
+    assert two.query("lane16_pairs") + two.rerun_count() == pairs
+    np.testing.assert_array_equal(got, want)
