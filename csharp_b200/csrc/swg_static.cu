@@ -1,19 +1,20 @@
 // Block handler that allocates no device memory.
 //
 // Some callers cannot call cudaMalloc: a host application that hands the GPU's memory to its
-// own pool allocator at start-up and forbids other allocations, code that runs while a CUDA
-// graph is being captured (allocation is not a capturable operation), or a plug-in loaded into
-// a process whose device memory budget is fixed.  sw_compute_block_static serves them: it is
-// the plain block kernel of sw_compute_block_device, with the kernel's scratch (the substitution
-// and flag tables, and each thread's carry row between strips of the DP) taken from the
-// file-scope array below instead of from cudaMalloc.  The caller passes the residues, the
+// own pool allocator at start-up and forbids other allocations, or a plug-in loaded into a
+// process whose device memory budget is fixed and already spent by its host.
+// sw_compute_block_static serves them: it is the plain block kernel of sw_compute_block_device,
+// with the kernel's scratch (the substitution and flag tables, and each thread's carry row
+// between strips of the DP) taken from the file-scope array below instead of from cudaMalloc.  The caller passes the residues, the
 // offsets and the output in device memory it owns.
 //
 // The array is 64 MiB and lives in every GPU that loads this library until the process exits.
 // Calls share it and leave the last call's contents in it; nothing in it has to start at zero
 // (the tables are rewritten by every call and each carry row is written before it is read).
 // Calls whose kernels overlap on the GPU (different streams, or different host threads) race on
-// it: the caller must order them.
+// it: the caller must order them.  The first call on a device looks up the array's device
+// address (cudaGetSymbolAddress, with that device current) and keeps it; make that first call
+// before any stream capture.
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstring>

@@ -182,8 +182,8 @@ int sw_query(sw_ctx* ctx, const char* key, int64_t* value);
 
 /* ---- block handler without device allocation ------------------------------------------------ */
 /* No counterpart in the reference: this entry point serves callers that cannot allocate device
- * memory (a host that gives all GPU memory to its own pool allocator, code running while a CUDA
- * graph is captured, a plug-in with a fixed memory budget).  It aligns the pairs of one block like
+ * memory (a host that gives all GPU memory to its own pool allocator, a plug-in whose process
+ * has a fixed device-memory budget).  It aligns the pairs of one block like
  * sw_compute_block_device, with the same ranges, modes, orientation and mirror rule, but needs
  * no context: the configuration comes in cfg, the residues and offsets (sw_upload_sequences'
  * layout) and the output are the caller's device buffers, and the work is ordered on `stream`

@@ -1,11 +1,12 @@
 """sw_compute_block_static: the block handler for callers that cannot allocate device memory.
 
 Some callers cannot call cudaMalloc (a host whose GPU memory all belongs to its own pool
-allocator, code running inside a CUDA graph capture, a plug-in with a fixed memory budget).
+allocator, a plug-in whose process has a fixed device-memory budget).
 The static entry point runs the same plain block kernel as sw_compute_block_device with its
 scratch in the library's own device array.  It must give the same Int16 distances as the
 allocating entry point (exact equality), on two calls in a row (the second reuses the array
-the first left behind), and those calls must not change the device's free memory.
+the first left behind), and the second call must not change the device's free memory (the first
+may: loading the library's device image on first use places the array).
 """
 import ctypes as C
 
@@ -41,7 +42,6 @@ def test_static_block_handler_matches_allocating_one_twice():
     cfg = _cfg(lib, matrix, 16, 4)
     blocks = [(0, N - 1, 0, N - 1, 1), (40, 72, 3, 30, 0)]
     L = lib.load()
-    free_after_first = None
     for call, (rs, re_, cs_, ce, diag) in enumerate(blocks):
         R, Cc = re_ - rs + 1, ce - cs_ + 1
         want = torch.zeros((R, Cc), dtype=torch.int16, device="cuda")
@@ -59,8 +59,7 @@ def test_static_block_handler_matches_allocating_one_twice():
         assert n.value == expected_pairs
         np.testing.assert_array_equal(got.cpu().numpy(), want.cpu().numpy())
         if call == 1:
-            assert torch.cuda.mem_get_info()[0] == free_before == free_after_first
-        free_after_first = torch.cuda.mem_get_info()[0]
+            assert torch.cuda.mem_get_info()[0] == free_before
 
 
 def test_static_block_handler_rejects_out_of_table_residues():
