@@ -939,10 +939,13 @@ struct Base {
   int4* d_box = nullptr;
   int* d_box_count = nullptr;
   long long box_cap = 0;
+  // pairs the lane box kernel hands to the warp box kernel (same capacity as d_box)
+  int4* d_spill = nullptr;
+  int* d_spill_count = nullptr;
   ~Base() {
     cudaFree(d_code); cudaFree(d_sorted); cudaFree(d_lettab); cudaFree(d_flagtab);
     cudaFree(d_scratch); cudaFree(d_carry);
-    cudaFree(d_box); cudaFree(d_box_count);
+    cudaFree(d_box); cudaFree(d_box_count); cudaFree(d_spill); cudaFree(d_spill_count);
   }
 };
 
@@ -1023,6 +1026,7 @@ int build_base(Base& B, const EngineParams& P, std::string* msg) {
 struct Plan {
   bool plain_only = false;
   int kind = kKindSw;       // the bins' kernel: SW with counters, NW, or the two-pass first pass
+  bool box_lane = false;    // two-pass: the lane box kernel ran before the warp box kernel
   bool zeroes_diagonal = false;
   int thresh = 0;
   std::vector<Bin> bins;
@@ -1083,7 +1087,8 @@ class EngineImpl : public Engine {
     if (k == "launches") {
       int64_t n = 2;  // the 32-bit lane kernel and the rerun-count reset
       for (auto& bn : last_->bins) n += bn.items.empty() ? 0 : 1;
-      if (!last_->plain_only && last_->kind == kKindScore) n += 1;  // the box kernel
+      if (!last_->plain_only && last_->kind == kKindScore)  // the box kernels
+        n += (last_->box_lane ? 2 : 1);
       return n + (last_->zeroes_diagonal ? 1 : 0);
     }
     if (k == "bins") {
@@ -1406,15 +1411,26 @@ class EngineImpl : public Engine {
       if (pl.npairs > B.box_cap) {  // one list for every plan (plans run one after another)
         for (auto& kv : plans_) if (kv.second->graph) { cudaGraphExecDestroy(kv.second->graph); kv.second->graph = nullptr; }
         cudaFree(B.d_box);
+        cudaFree(B.d_spill);
         B.d_box = nullptr;
+        B.d_spill = nullptr;
         B.box_cap = 0;
-        if (cudaMalloc(&B.d_box, sizeof(int4) * (size_t)std::max<int64_t>(pl.npairs, 1)) != cudaSuccess) {
-          cudaGetLastError(); *msg = "cudaMalloc two-pass pair list"; return SW_E_OOM;
+        const size_t bytes = sizeof(int4) * (size_t)std::max<int64_t>(pl.npairs, 1);
+        if (cudaMalloc(&B.d_box, bytes) != cudaSuccess || cudaMalloc(&B.d_spill, bytes) != cudaSuccess) {
+          cudaGetLastError();
+          cudaFree(B.d_box);
+          B.d_box = nullptr;
+          B.d_spill = nullptr;
+          *msg = "cudaMalloc two-pass pair lists";
+          return SW_E_OOM;
         }
         B.box_cap = std::max<int64_t>(pl.npairs, 1);
       }
       if (!B.d_box_count && cudaMalloc(&B.d_box_count, sizeof(int)) != cudaSuccess) {
         cudaGetLastError(); B.d_box_count = nullptr; *msg = "cudaMalloc two-pass count"; return SW_E_OOM;
+      }
+      if (!B.d_spill_count && cudaMalloc(&B.d_spill_count, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError(); B.d_spill_count = nullptr; *msg = "cudaMalloc two-pass count"; return SW_E_OOM;
       }
     }
     std::vector<int2> rl(big);
@@ -1485,6 +1501,20 @@ class EngineImpl : public Engine {
       X.budget = 1 << 16;
       X.rerun = pl.d_rerun; X.rerun_count = pl.d_rerun_count; X.rerun_cap = pl.rerun_cap;
       X.stats = pl.d_stats;
+      X.list_cap = B.box_cap;
+      pl.box_lane = opt_.box_lane && P.o + P.e < 8192;
+      if (pl.box_lane) {
+        // one pair per thread; a score above 127 max S needs more than 254 rows + columns
+        BoxJob L = X;
+        L.max_score = 127 * std::max(B.max_s, 0);
+        L.spill = B.d_spill; L.spill_count = B.d_spill_count;
+        L.spill_cap = (int)std::min<long long>(B.box_cap, 0x7fffffff);
+        if ((e = cudaMemsetAsync(B.d_spill_count, 0, sizeof(int), P.stream)) != cudaSuccess) return e;
+        if ((e = launch_box_lane(L, P.sms, P.stream)) != cudaSuccess) return e;
+        X.list = B.d_spill; X.count = B.d_spill_count;
+      }
+      // the warp kernel's box has at most kWarpBoxMaxCols columns: a larger S / max S cannot fit
+      X.max_score = kWarpBoxMaxCols * std::max(B.max_s, 0);
       if ((e = launch_box(X, (int)(B.carry_threads / 128), 128, P.stream)) != cudaSuccess) return e;
     }
     // 32-bit lanes: pairs the static guard routed here, those whose 16-bit lanes tripped, or all

@@ -74,9 +74,20 @@ struct BoxJob {
   int* rerun_count;
   int rerun_cap;
   unsigned long long* stats;  // [1] pairs finished in 16-bit lanes, [3] pairs given up on
+  long long list_cap;      // entries `list` holds (the count is clipped to it)
+  int max_score;           // pairs with a larger S cannot fit: straight to the next step
+  int4* spill;             // lane kernel: pairs for the warp box kernel
+  int* spill_count;
+  int spill_cap;
 };
 
+constexpr int kWarpBoxMaxCols = 256;  // box_kernel's largest box (columns and rows)
+
+// Warp per pair (reverse scan on 64-column shuffle windows, box DP as a 32-row wavefront).
 cudaError_t launch_box(const BoxJob& J, int grid, int block, cudaStream_t st);
+// One pair per thread (swg_box_lane.cuh); the pairs it cannot finish go to J.spill (for
+// launch_box) or, where the warp kernel could not finish them either, to the 32-bit lanes.
+cudaError_t launch_box_lane(const BoxJob& J, int sms, cudaStream_t st);
 
 size_t plain_carry_bytes(int mode, long threads, int maxlen, int dist_fn = 0);
 cudaError_t launch_plain_block(const PlainJob& J, int grid, int block, cudaStream_t st);

@@ -6,8 +6,10 @@
 // per-thread slice of global scratch, interleaved across threads so a warp's accesses coalesce.
 // Substitution scores and column flags are staged in shared memory.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 #include <type_traits>
+#include "swg_box_lane.cuh"
 #include "swg_device.cuh"
 #include "swg_internal.h"
 
@@ -230,8 +232,8 @@ __global__ void __launch_bounds__(128) plain_block_kernel(PlainJob J) {
 // a row the gap chain RHs(j) = max(X(j), RHs(j+1) - min(e, o)) is a max-plus prefix scan over
 // the lanes.  The box DP is a warp wavefront (lane = box row, 32 rows per pass).
 constexpr int kBoxWarps = 4;
-constexpr int kBoxMaxW = 256;   // box columns (else 32-bit full DP)
-constexpr int kBoxMaxH = 256;   // box rows
+constexpr int kBoxMaxW = kWarpBoxMaxCols;  // box columns (else 32-bit full DP)
+constexpr int kBoxMaxH = kWarpBoxMaxCols;  // box rows
 constexpr unsigned kFull = 0xffffffffu;
 
 __device__ __forceinline__ int scan_max_up(int y, int lane) {
@@ -260,7 +262,7 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
   // bottom row of a box pass: V, G, and the two counter words per column
   int4* buf = rowbuf + warp * kBoxMaxW;
   const long nwarps = (long)gridDim.x * kBoxWarps;
-  const int np = *J.count;
+  const long long np = min((long long)*J.count, J.list_cap);
   const int o = J.o, e = J.e, dchain = min(J.e, J.o);
   for (long p = (long)blockIdx.x * kBoxWarps + warp; p < np; p += nwarps) {
     const int4 rec = J.list[p];
@@ -272,9 +274,10 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
     int hi = je, lo = je;
     int rwb0 = lane == 0 ? 0 : NEG, rwb1 = NEG, rgb0 = NEG, rgb1 = NEG;  // row below, pos lane / 32+lane
     int cand_i = 1 << 30, cand_j = 1 << 30;
-    bool ok = true;
+    // S needs at least S / max S diagonal columns: beyond max_score the box cannot fit
+    bool ok = S <= J.max_score;
     long long cells = 0;
-    for (int i = ie - 1; i >= 0; i--) {
+    for (int i = ie - 1; ok && i >= 0; i--) {
       const int arow = (int)a[i] * A1;
       // chunk 0: pos = lane, j = hi - lane
       const int j0 = hi - lane;
@@ -414,6 +417,69 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
     }
     __syncwarp();
   }
+}
+
+// One pair per thread: the reverse scan and the band DP of swg_box_lane.cuh with 96 words of
+// scratch per thread in shared memory (thread-interleaved), 64 threads per CTA (7 CTAs per SM on
+// B200's 228 KB).
+constexpr int kLaneThreads = 64;
+
+__global__ void __launch_bounds__(kLaneThreads) box_lane_kernel(BoxJob J) {
+  __shared__ int16_t sc[kBoxMaxA1 * kBoxMaxA1];
+  __shared__ uint8_t fl[kBoxMaxA1 * kBoxMaxA1];
+  __shared__ uint32_t scratch[kLaneWords * kLaneThreads];
+  const int A1 = J.A + 1;
+  for (int k = threadIdx.x; k < A1 * A1; k += blockDim.x) {
+    sc[k] = (int16_t)(J.lettab[k] - J.o);
+    fl[k] = (uint8_t)(J.flagtab[k] & kFlagCount);
+  }
+  __syncthreads();
+  const long long np = min((long long)*J.count, J.list_cap);
+  const LaneMem mem{scratch + threadIdx.x, kLaneThreads};
+  const long long stride = (long long)gridDim.x * kLaneThreads;
+  for (long long p = (long long)blockIdx.x * kLaneThreads + threadIdx.x; p < np; p += stride) {
+    const int4 rec = J.list[p];
+    const int q = rec.x, d = rec.y, S = rec.z;
+    const int ie = (int)((uint32_t)rec.w >> 16), je = rec.w & 0xFFFF;
+    int rc = 4;  // beyond max_score the band DP's box cannot fit
+    uint32_t c = 0u;
+    if (S <= J.max_score)
+      rc = lane_box_pair(J.seq + J.off[q], J.seq + J.off[d], S, ie, je, sc, fl, A1, J.o, J.e, mem, &c);
+    if (rc == 0) {
+      const int16_t dist = fraction_distance((int)(c & 0xFFu), (int)(c >> 8));
+      J.out[(long long)q * J.ld + d] = dist;
+      if (J.mirror) J.out[(long long)d * J.ld + q] = dist;
+      continue;
+    }
+    // a taller scan or a larger box: the warp kernel; a window overflow (which the warp
+    // kernel's 64-column window meets too) or anything else: the 32-bit full DP
+    if (rc == 1 || rc == 4) {
+      const int w = atomicAdd(J.spill_count, 1);
+      if (w < J.spill_cap) {
+        J.spill[w] = rec;
+        continue;
+      }
+    }
+    const int wr = atomicAdd(J.rerun_count, 1);
+    if (wr < J.rerun_cap) J.rerun[wr] = make_int2(q, d);
+    atomicAdd(J.stats + 3, 1ull);
+    atomicAdd(J.stats + 1, ~0ull);  // no longer finished in 16-bit lanes
+  }
+}
+
+cudaError_t launch_box_lane(const BoxJob& J, int sms, cudaStream_t st) {
+  if (J.A + 1 > kBoxMaxA1 || J.o + J.e >= 8192) return cudaErrorInvalidValue;
+  static int per_sm = 0;  // resident CTAs per SM (the kernel's shared memory decides)
+  if (per_sm == 0) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, box_lane_kernel, kLaneThreads, 0) != cudaSuccess) {
+      cudaGetLastError();
+      n = 1;
+    }
+    per_sm = std::max(n, 1);
+  }
+  box_lane_kernel<<<std::max(sms, 1) * per_sm, kLaneThreads, 0, st>>>(J);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_box(const BoxJob& J, int grid, int block, cudaStream_t st) {

@@ -397,6 +397,10 @@ def test_two_pass_equals_one_pass_and_oracle(cs, oracle_mod):
     assert two.query("box_fallbacks") > 0  # the near-identical family members
     assert two.query("lane16_pairs") + two.rerun_count() == pairs
     np.testing.assert_array_equal(got, want)
+    warp = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4).upload(seqs)
+    warp.set_option("box_lane", 0)  # boxes by the warp kernel alone
+    got_w, _, _ = warp.all_pairs(1)
+    np.testing.assert_array_equal(got_w, want)
     N = len(seqs)
     sel = rng.choice(N * (N - 1) // 2, 3000, replace=False)
     pr = np.array([(i, j) for i in range(N) for j in range(i)], dtype=np.int32)[sel]
@@ -422,3 +426,34 @@ def test_two_pass_with_most_pairs_falling_back(cs):
     assert two.query("box_fallbacks") > pairs // 2
     assert two.query("lane16_pairs") + two.rerun_count() == pairs
     np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("o,e", [(16, 4), (10, 3), (20, 8), (4, 2)])
+def test_lane_box_kernel_on_uneven_lengths(cs, oracle_mod, o, e):
+    """Lognormal lengths (median 400, sigma 0.6, clipped 50-1500) from 200 family roots: the box
+    step runs one pair per thread for most pairs, hands taller scans and wider bands to the warp
+    kernel and window overflows to the 32-bit lanes.  Every entry equals the one-pass counter
+    kernel's and the warp-only box step's; a sample equals the oracle's."""
+    from csharp_b200 import synth
+    rng = np.random.default_rng(91 + o)
+    lens = synth.lognormal_lengths(900, 400, 0.6, 50, 1500, rng)
+    seqs = [s.tobytes() for s in synth.dna_family(900, 200, lens, seed=92)]
+    m = cs.ScoringMatrix.Load("EDNAFULL")
+    res = {}
+    for tag, opts in (("one", {"two_pass": 0}), ("warp", {"box_lane": 0}), ("lane", {})):
+        eng = cs.Engine(m, o, e).upload(seqs)
+        for k, v in opts.items():
+            eng.set_option(k, v)
+        res[tag], pairs, _ = eng.all_pairs(1)
+        if tag == "lane":
+            assert eng.query("lane16_pairs") + eng.rerun_count() == pairs
+            assert eng.query("launches") >= 4
+        eng.close()
+    np.testing.assert_array_equal(res["lane"], res["one"])
+    np.testing.assert_array_equal(res["warp"], res["one"])
+    N = len(seqs)
+    ii = rng.integers(1, N, 1500)
+    jj = (rng.random(1500) * ii).astype(np.int64)
+    pr = np.stack([ii, jj], 1).astype(np.int32)
+    ref = _oracle_distances(oracle_mod, seqs, pr, "EDNAFULL", float(o), float(e))
+    np.testing.assert_array_equal(res["lane"][pr[:, 0], pr[:, 1]], ref)
