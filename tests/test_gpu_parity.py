@@ -397,10 +397,12 @@ def test_two_pass_equals_one_pass_and_oracle(cs, oracle_mod):
     assert two.query("box_fallbacks") > 0  # the near-identical family members
     assert two.query("lane16_pairs") + two.rerun_count() == pairs
     np.testing.assert_array_equal(got, want)
-    warp = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4).upload(seqs)
-    warp.set_option("box_lane", 0)  # boxes by the warp kernel alone
-    got_w, _, _ = warp.all_pairs(1)
-    np.testing.assert_array_equal(got_w, want)
+    for lane in (0, 1):  # boxes by the warp kernel alone, or one pair per thread first
+        other = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4).upload(seqs)
+        other.set_option("box_lane", lane)
+        got_o, _, _ = other.all_pairs(1)
+        np.testing.assert_array_equal(got_o, want)
+        other.close()
     N = len(seqs)
     sel = rng.choice(N * (N - 1) // 2, 3000, replace=False)
     pr = np.array([(i, j) for i in range(N) for j in range(i)], dtype=np.int32)[sel]
@@ -440,7 +442,7 @@ def test_lane_box_kernel_on_uneven_lengths(cs, oracle_mod, o, e):
     seqs = [s.tobytes() for s in synth.dna_family(900, 200, lens, seed=92)]
     m = cs.ScoringMatrix.Load("EDNAFULL")
     res = {}
-    for tag, opts in (("one", {"two_pass": 0}), ("warp", {"box_lane": 0}), ("lane", {})):
+    for tag, opts in (("one", {"two_pass": 0}), ("warp", {"box_lane": 0}), ("lane", {"box_lane": 1})):
         eng = cs.Engine(m, o, e).upload(seqs)
         for k, v in opts.items():
             eng.set_option(k, v)
