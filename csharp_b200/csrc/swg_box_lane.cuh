@@ -29,11 +29,12 @@
 // threads so a warp's accesses hit 32 distinct banks).  The reverse scan keeps row i+1's RW | RG
 // (two int16) in word j % kLaneWin; the band DP keeps the row above's V | G and its two 16-bit
 // counter words (aligned << 8 | counted) of column j in words j % kLaneBand and kLaneBand +
-// j % kLaneBand.  The pair is given up (nonzero return) when the scan exceeds kLaneMaxRows rows or
-// a row's live span exceeds kLaneWin columns, or the band exceeds kLaneBand diagonals or the box
-// 254 rows + columns (the counters' range).
+// j % kLaneBand.  A pair is given up when the scan exceeds kLaneMaxRows rows or a row's live span
+// exceeds kLaneWin columns, or the band exceeds kLaneBand diagonals or the box 254 rows + columns
+// (the counters' range).
 #pragma once
 #include <cstdint>
+#include <vector_types.h>
 
 #ifdef __CUDACC__
 #define SWG_LANE_FN __host__ __device__ __forceinline__
@@ -71,90 +72,172 @@ SWG_LANE_FN int lane_hi(uint32_t w) { return (int)(int16_t)(uint16_t)(w >> 16); 
 SWG_LANE_FN int lane_max(int a, int b) { return a > b ? a : b; }
 SWG_LANE_FN int lane_min(int a, int b) { return a < b ? a : b; }
 
-// a, b: residue codes of s1 and s2 (indices into the tables' rows and columns, row stride A1);
-// sc: substitution scores S(x, y); fl: flags (bit 0 = counted column).  Requires 1 <= S <= 32767,
-// 1 <= ie <= m, 1 <= je <= n, o + e < 8192.  Returns 0 with *cnt = aligned << 8 | counted, or the
-// reason it gave up: 1 scan rows, 2 scan window, 3 no first pair found, 4 band or box size,
-// 5 score.
-template <class ScT, class FlT>
-SWG_LANE_FN int lane_box_pair(const uint8_t* a, const uint8_t* b, int S, int ie, int je, const ScT* sc,
-                              const FlT* fl, int A1, int o, int e, LaneMem mem, uint32_t* cnt) {
+// Runs the two DPs for the pairs list[first], list[first + stride], ... below np, flattened into
+// one loop whose every iteration does one cell (of the reverse scan or of the band DP) of the
+// current pair: lanes of a warp that hold pairs of different shapes still issue the same loop body
+// together, and a lane that finishes a pair takes its next one in the following iteration.  Each
+// record is (s1 index, s2 index, S, ie << 16 | je) with 1 <= S <= 32767, 1 <= ie <= m and
+// 1 <= je <= n; seq + off[k] are the residue codes of sequence k (indices into the tables' rows
+// and columns, row stride A1); sc holds the substitution scores S(x, y) and fl the flags (bit 0 =
+// counted column); o + e < 8192.  emit(record, reason, counters) receives every pair's outcome:
+// reason 0 with counters = aligned << 8 | counted, or the reason the pair was given up: 1 scan
+// rows, 2 scan window, 3 no first pair found, 4 band or box size (or S above max_score), 5 score.
+template <class ScT, class FlT, class Emit>
+SWG_LANE_FN void lane_box_run(const int4* list, long long first, long long np, long long stride,
+                              const uint8_t* seq, const int64_t* off, const ScT* sc, const FlT* fl,
+                              int A1, int o, int e, int max_score, LaneMem mem, Emit& emit) {
   constexpr int D = kLaneDead;
-  // ---- reverse scan, rows ie-1 .. 0; [lo, hi] = live columns of the row below ----
-  int lo = je, hi = je;
-  mem[je % kLaneWin] = lane_pack(0, D);
-  int ci = 1 << 30, cj = 1 << 30;
-  // diagonals (j - i) spanned by the live states of the rows below the current one, and their
-  // value when the topmost first pair so far was found (the band of the rows ci..ie)
-  int dlo = je - ie, dhi = je - ie, blo = 0, bhi = -1;
-  for (int i = ie - 1; i >= 0; i--) {
-    if (ie - i > kLaneMaxRows) return 1;
-    const ScT* srow = sc + (int)a[i] * A1;
-    int rh = D;   // RH(i, j+1)
-    int drw = D;  // RW(i+1, j+1)
-    int nlo = 0, nhi = -1;
-    bool first_pair = false;
-    for (int j = hi; j >= 0; j--) {
-      if (nhi >= 0 && nhi - j >= kLaneWin) return 2;  // the row's span would exceed the window
-      int rwb = D, rgb = D;
-      if (j >= lo) {
-        const uint32_t w = mem[j % kLaneWin];
-        rwb = lane_lo(w);
-        rgb = lane_hi(w);
+  constexpr int kFetch = 0, kScan = 1, kBand = 2;
+  int phase = kFetch;
+  long long p = first;
+  int4 nrec;  // the next pair's record, loaded one pair ahead
+  nrec.x = nrec.y = nrec.z = nrec.w = 0;
+  if (p < np) nrec = list[p];
+  int4 rec = nrec;
+  const uint8_t* a = seq;
+  const uint8_t* b = seq;
+  int S = 0, ie = 0, je = 0;
+  // reverse scan
+  int i = 0, j = 0, lo = 0, hi = 0, nlo = 0, nhi = -1, rh = D, drw = D;
+  int ci = 0, cj = 0, dlo = 0, dhi = 0, blo = 0, bhi = -1;
+  bool first_pair = false;
+  const ScT* srow = sc;
+  // band DP
+  int jl = 0, jr = -1, plo = 1, phi = 0, vl = 0, hh = D, vd = 0, vlast = 0;
+  uint32_t cl = 0u, ch = 0u, cd = 0u, clast = 0u;
+  const FlT* frow = fl;
+  for (;;) {
+    int rc = -1;  // >= 0: the current pair is finished with this outcome
+    if (phase == kFetch) {
+      if (p >= np) break;
+      rec = nrec;
+      if (p + stride < np) nrec = list[p + stride];
+      S = rec.z;
+      ie = (int)((uint32_t)rec.w >> 16);
+      je = rec.w & 0xFFFF;
+      if (S > max_score) {
+        rc = 4;
+      } else {
+        a = seq + off[rec.x];
+        b = seq + off[rec.y];
+        lo = hi = je;
+        mem[je % kLaneWin] = lane_pack(0, D);
+        ci = cj = 1 << 30;
+        dlo = dhi = je - ie;
+        blo = 0;
+        bhi = -1;
+        i = ie - 1;
+        j = hi;
+        rh = drw = D;
+        nlo = 0;
+        nhi = -1;
+        first_pair = false;
+        srow = sc + (int)a[i] * A1;
+        phase = kScan;
       }
-      int x = rgb - o;
-      if (drw >= 0) {
-        const int pr = (int)srow[b[j]] + drw;
-        if (pr == S) {
-          ci = lane_min(ci, i + 1);
-          cj = lane_min(cj, j + 1);
-          first_pair = true;
+    } else if (phase == kScan) {
+      // cell (i, j) of the reverse scan
+      if (nhi >= 0 && nhi - j >= kLaneWin) {
+        rc = 2;  // the row's span would exceed the window
+      } else {
+        int rwb = D, rgb = D;
+        if (j >= lo) {
+          const uint32_t w = mem[j % kLaneWin];
+          rwb = lane_lo(w);
+          rgb = lane_hi(w);
         }
-        x = lane_max(x, pr);
+        int x = rgb - o;
+        if (drw >= 0) {
+          const int pr = (int)srow[b[j]] + drw;
+          if (pr == S) {
+            ci = lane_min(ci, i + 1);
+            cj = lane_min(cj, j + 1);
+            first_pair = true;
+          }
+          x = lane_max(x, pr);
+        }
+        int rw = lane_max(x, rh - o);
+        rh = lane_max(rw, rh - e);
+        int rg = lane_max(rw, rgb - e);
+        if (rw < 0) rw = D;
+        if (rg < 0) rg = D;
+        if (rh < 0) rh = D;
+        mem[j % kLaneWin] = lane_pack(rw, rg);
+        if (rw >= 0 || rg >= 0) {
+          nlo = j;
+          if (nhi < 0) nhi = j;
+        }
+        drw = rwb;
+        const bool row_end = (j < lo && rh < 0) || j == 0;
+        j--;
+        if (row_end) {
+          if (first_pair) { blo = dlo; bhi = dhi; }  // the rows i+1 .. ie
+          if (nhi >= 0 && i > 0) {
+            lo = nlo;
+            hi = nhi;
+            dlo = lane_min(dlo, lo - i);
+            dhi = lane_max(dhi, hi - i);
+            i--;
+            if (ie - i > kLaneMaxRows) {
+              rc = 1;
+            } else {
+              j = hi;
+              rh = drw = D;
+              nlo = 0;
+              nhi = -1;
+              first_pair = false;
+              srow = sc + (int)a[i] * A1;
+            }
+          } else if (ci > ie || cj > je || bhi < blo) {
+            rc = 3;  // the scan is over: the box of the first pairs
+          } else {
+            const int h = ie - ci + 1, w = je - cj + 1;
+            blo = lane_max(blo, cj - ie);
+            bhi = lane_min(bhi, je - ci);
+            if (bhi - blo + 1 > kLaneBand || h + w > 254) {
+              rc = 4;
+            } else {
+              i = ci;
+              plo = 1;
+              phi = 0;
+              jl = 1;
+              jr = 0;
+              j = 1;  // past the empty row: the row set-up below runs first
+              phase = kBand;
+            }
+          }
+        }
       }
-      int rw = lane_max(x, rh - o);
-      rh = lane_max(rw, rh - e);
-      int rg = lane_max(rw, rgb - e);
-      if (rw < 0) rw = D;
-      if (rg < 0) rg = D;
-      if (rh < 0) rh = D;
-      mem[j % kLaneWin] = lane_pack(rw, rg);
-      if (rw >= 0 || rg >= 0) {
-        nlo = j;
-        if (nhi < 0) nhi = j;
+    } else {
+      // cell (i, j) of the band DP, after the set-up of row i when j has left the row
+      if (j > jr) {
+        if (jl <= jr) {  // the row just finished becomes the row above
+          plo = jl;
+          phi = jr;
+          i++;
+        }
+        for (;;) {  // rows whose band lies outside the box are empty (never row ie)
+          jl = lane_max(cj, i + blo);
+          jr = lane_min(je, i + bhi);
+          if (jl <= jr) break;
+          plo = jl;
+          phi = jr;
+          i++;
+        }
+        const int arow = (int)a[i - 1] * A1;
+        srow = sc + arow;
+        frow = fl + arow;
+        vl = 0;
+        hh = D;
+        vd = 0;
+        cl = ch = cd = 0u;
+        if (jl - 1 >= plo && jl - 1 <= phi) {
+          const int k = (jl - 1) % kLaneBand;
+          vd = lane_lo(mem[k]);
+          cd = mem[kLaneBand + k] & 0xFFFFu;
+        }
+        j = jl;
       }
-      drw = rwb;
-      if (j < lo && rh < 0) break;  // nothing further left in this row can be live
-    }
-    if (first_pair) { blo = dlo; bhi = dhi; }  // the rows i+1 .. ie
-    if (nhi < 0) break;  // no live state: nothing above can reach (ie, je)
-    lo = nlo;
-    hi = nhi;
-    dlo = lane_min(dlo, lo - i);
-    dhi = lane_max(dhi, hi - i);
-  }
-  if (ci > ie || cj > je || bhi < blo) return 3;
-  const int h = ie - ci + 1, w = je - cj + 1;
-  blo = lane_max(blo, cj - ie);  // clipped to the box's own diagonals
-  bhi = lane_min(bhi, je - ci);
-  if (bhi - blo + 1 > kLaneBand || h + w > 254) return 4;
-  // ---- band DP: rows ci..ie, columns cj..je with blo <= j - i <= bhi, zero boundary ----
-  int vlast = 0;
-  uint32_t clast = 0u;
-  int plo = 1, phi = 0;  // columns of the row above (none: the top boundary)
-  for (int i = ci; i <= ie; i++) {
-    const int jl = lane_max(cj, i + blo), jr = lane_min(je, i + bhi);
-    const int arow = (int)a[i - 1] * A1;
-    const ScT* srow = sc + arow;
-    const FlT* frow = fl + arow;
-    int vl = 0, hh = D, vd = 0;
-    uint32_t cl = 0u, ch = 0u, cd = 0u;
-    if (jl - 1 >= plo && jl - 1 <= phi) {
-      const int k = (jl - 1) % kLaneBand;
-      vd = lane_lo(mem[k]);
-      cd = mem[kLaneBand + k] & 0xFFFFu;
-    }
-    for (int j = jl; j <= jr; j++) {
       const int k = j % kLaneBand;
       int vu = 0, gu = D;
       uint32_t cvu = 0u, cgu = 0u;
@@ -184,13 +267,15 @@ SWG_LANE_FN int lane_box_pair(const uint8_t* a, const uint8_t* b, int S, int ie,
       cl = cv;
       vlast = v;
       clast = cv;
+      j++;
+      if (i == ie && j > jr) rc = (vlast == S) ? 0 : 5;  // (ie, je) was the last cell
     }
-    plo = jl;
-    phi = jr;
+    if (rc >= 0) {
+      emit(rec, rc, clast);
+      phase = kFetch;
+      p += stride;
+    }
   }
-  if (vlast != S) return 5;
-  *cnt = clast;
-  return 0;
 }
 
 }  // namespace swg

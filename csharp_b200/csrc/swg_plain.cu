@@ -419,10 +419,37 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
   }
 }
 
-// One pair per thread: the reverse scan and the band DP of swg_box_lane.cuh with 96 words of
-// scratch per thread in shared memory (thread-interleaved), 64 threads per CTA (7 CTAs per SM on
-// B200's 228 KB).
+// One pair per thread: the reverse scan and the band DP of swg_box_lane.cuh as one flattened loop
+// (a cell per iteration, the next pair at once when one finishes), 96 words of scratch per thread
+// in shared memory (thread-interleaved), 64 threads per CTA (7 CTAs per SM on B200's 228 KB).
 constexpr int kLaneThreads = 64;
+
+// Where each pair's outcome goes: its distance, the warp box kernel's list (a taller scan or a
+// larger box than the lane kernel keeps), or the 32-bit lanes (a window overflow, which the warp
+// kernel's 64-column window meets too, or anything else).
+struct LaneEmit {
+  const BoxJob* J;
+  __device__ __forceinline__ void operator()(const int4& rec, int rc, uint32_t c) const {
+    const int q = rec.x, d = rec.y;
+    if (rc == 0) {
+      const int16_t dist = fraction_distance((int)(c & 0xFFu), (int)(c >> 8));
+      J->out[(long long)q * J->ld + d] = dist;
+      if (J->mirror) J->out[(long long)d * J->ld + q] = dist;
+      return;
+    }
+    if (rc == 1 || rc == 4) {
+      const int w = atomicAdd(J->spill_count, 1);
+      if (w < J->spill_cap) {
+        J->spill[w] = rec;
+        return;
+      }
+    }
+    const int wr = atomicAdd(J->rerun_count, 1);
+    if (wr < J->rerun_cap) J->rerun[wr] = make_int2(q, d);
+    atomicAdd(J->stats + 3, 1ull);
+    atomicAdd(J->stats + 1, ~0ull);  // no longer finished in 16-bit lanes
+  }
+};
 
 __global__ void __launch_bounds__(kLaneThreads) box_lane_kernel(BoxJob J) {
   __shared__ int16_t sc[kBoxMaxA1 * kBoxMaxA1];
@@ -436,35 +463,9 @@ __global__ void __launch_bounds__(kLaneThreads) box_lane_kernel(BoxJob J) {
   __syncthreads();
   const long long np = min((long long)*J.count, J.list_cap);
   const LaneMem mem{scratch + threadIdx.x, kLaneThreads};
-  const long long stride = (long long)gridDim.x * kLaneThreads;
-  for (long long p = (long long)blockIdx.x * kLaneThreads + threadIdx.x; p < np; p += stride) {
-    const int4 rec = J.list[p];
-    const int q = rec.x, d = rec.y, S = rec.z;
-    const int ie = (int)((uint32_t)rec.w >> 16), je = rec.w & 0xFFFF;
-    int rc = 4;  // beyond max_score the band DP's box cannot fit
-    uint32_t c = 0u;
-    if (S <= J.max_score)
-      rc = lane_box_pair(J.seq + J.off[q], J.seq + J.off[d], S, ie, je, sc, fl, A1, J.o, J.e, mem, &c);
-    if (rc == 0) {
-      const int16_t dist = fraction_distance((int)(c & 0xFFu), (int)(c >> 8));
-      J.out[(long long)q * J.ld + d] = dist;
-      if (J.mirror) J.out[(long long)d * J.ld + q] = dist;
-      continue;
-    }
-    // a taller scan or a larger box: the warp kernel; a window overflow (which the warp
-    // kernel's 64-column window meets too) or anything else: the 32-bit full DP
-    if (rc == 1 || rc == 4) {
-      const int w = atomicAdd(J.spill_count, 1);
-      if (w < J.spill_cap) {
-        J.spill[w] = rec;
-        continue;
-      }
-    }
-    const int wr = atomicAdd(J.rerun_count, 1);
-    if (wr < J.rerun_cap) J.rerun[wr] = make_int2(q, d);
-    atomicAdd(J.stats + 3, 1ull);
-    atomicAdd(J.stats + 1, ~0ull);  // no longer finished in 16-bit lanes
-  }
+  LaneEmit emit{&J};
+  lane_box_run(J.list, (long long)blockIdx.x * kLaneThreads + threadIdx.x, np,
+               (long long)gridDim.x * kLaneThreads, J.seq, J.off, sc, fl, A1, J.o, J.e, J.max_score, mem, emit);
 }
 
 cudaError_t launch_box_lane(const BoxJob& J, int sms, cudaStream_t st) {
