@@ -36,6 +36,13 @@ OPS_PER_CELL = 11      # algorithmic integer ops of one SW-Gotoh cell (E, F, H, 
 LANES_PER_OP = 2       # the engine's score registers hold two 16-bit lanes
 SHARES = 8             # steps per whole job: the shares of an 8-rank run
 SERVE = dict(db=100000, qmin=1, qmax=512, load=0.7, seconds=40.0, seed=6)
+ENGINE_OPTIONS = {}    # engine knobs from the command line (sw_set_option), applied to every engine
+
+
+def with_options(eng):
+    for k, v in ENGINE_OPTIONS.items():
+        eng.set_option(k, v)
+    return eng
 
 
 def workload_sequences(n):
@@ -258,14 +265,15 @@ def other_configs(cs, device, stream, flush):
         seqs = gen()
         concat, off = pack_sequences(seqs)
         n = len(seqs)
-        eng = cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=mode, alignment_type=atype, device=device)
+        eng = with_options(cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=mode, alignment_type=atype, device=device))
         eng.upload(concat=concat, offsets=off)
         eng.use_stream(stream.cuda_stream)
         full = torch.zeros((n, n), dtype=torch.int16, device="cuda")
         ms, cells = timed(eng, n, full)
         m = min(sub, n)
-        a16 = cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=mode, alignment_type=atype, device=device)
-        a32 = cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=mode, alignment_type=atype, device=device, lanes=32)
+        a16 = with_options(cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=mode, alignment_type=atype, device=device))
+        a32 = with_options(cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=mode, alignment_type=atype, device=device,
+                                     lanes=32))
         r = {}
         for tag, x in (("lanes16", a16), ("lanes32", a32)):
             x.upload(concat=concat[: off[m]], offsets=off[: m + 1])
@@ -299,7 +307,11 @@ def main():
     ap.add_argument("--serving-only", action="store_true", help="only the serving workload (one JSON line)")
     ap.add_argument("--configs-only", action="store_true", help="only configurations 1, 2 and 4 (one JSON line)")
     ap.add_argument("--serve-seconds", type=float, default=SERVE["seconds"])
+    ap.add_argument("--box-lane", type=int, default=-1, choices=[-1, 0, 1],
+                    help="two-pass box step: 1 one pair per thread first, 0 warp kernel only (-1: engine default)")
     a = ap.parse_args()
+    if a.box_lane >= 0:
+        ENGINE_OPTIONS["box_lane"] = a.box_lane
     if a.serving_only:
         import csharp_b200 as cs
         print(json.dumps({"serving": serving(cs, 0, a.serve_seconds, SERVE["load"])}))
@@ -328,7 +340,7 @@ def main():
     concat, off = workload_sequences(a.n)
     lens = np.diff(off)
     N = a.n
-    eng = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4, device=local)
+    eng = with_options(cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4, device=local))
     eng.upload(concat=concat, offsets=off)
     if a.rows_per_lane:
         eng.set_option("rows_per_lane", a.rows_per_lane)
@@ -396,6 +408,7 @@ def main():
                          "step": f"one rank's share of an {SHARES}-rank MPI run of the job (whole job = {SHARES} steps)",
                          "l2": "flushed (256 MB write) before every timed step",
                          "cells_per_job": int(sum(share_cells.values())), "pairs_per_job": N * (N - 1) // 2,
+                         "engine_options": dict(ENGINE_OPTIONS) or "defaults",
                          "rows_per_lane_costs": (tuned if tuned and any(tuned.values()) else
                                                  "built-in" + (" (kept by the autotuner)" if tuned else ""))},
               "gpu_launches": int(launches), "clocks": clk.summary()}
@@ -466,7 +479,7 @@ def main():
                             "tolerance": "exact Int16"}
         # plain one-launch-per-block kernel vs the batched engine on the same 2,000-sequence block
         M = min(2000, N)
-        sub = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4, device=local)
+        sub = with_options(cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4, device=local))
         sub.upload(concat=concat[: off[M]], offsets=off[: M + 1])
         sub.use_stream(stream.cuda_stream)
         o2 = torch.zeros((M, M), dtype=torch.int16, device="cuda")

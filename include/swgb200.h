@@ -161,8 +161,8 @@ int sw_compute_rank_blocks(sw_ctx* ctx, int32_t rank, int32_t world_size, int16_
  * (database entries per work item), "rows_per_lane" (0 = chosen per query, else an even number 4..16),
  * "plan_only" (1: engine calls build their work plans and graphs but launch nothing; 0: run),
  * "two_pass" (1, the default: SW-Gotoh with open and extend >= 2 runs a score-only pass and finds
- * each pair's counters near its best cell; 0: the one-pass counter kernels), "box_lane" (1, the
- * default: the two-pass box step runs one pair per thread first; 0: the warp-per-pair kernel only).
+ * each pair's counters near its best cell; 0: the one-pass counter kernels), "box_lane" (1: the
+ * two-pass box step runs one pair per thread first; 0, the default: the warp-per-pair kernel only).
  * Every knob gives the same distances.  Unknown keys are SW_E_ARG. */
 int sw_set_option(sw_ctx* ctx, const char* key, int64_t value);
 
