@@ -470,15 +470,14 @@ __global__ void __launch_bounds__(kLaneThreads) box_lane_kernel(BoxJob J) {
 
 cudaError_t launch_box_lane(const BoxJob& J, int sms, cudaStream_t st) {
   if (J.A + 1 > kBoxMaxA1 || J.o + J.e >= 8192) return cudaErrorInvalidValue;
-  static int per_sm = 0;  // resident CTAs per SM (the kernel's shared memory decides)
-  if (per_sm == 0) {
+  static const int per_sm = [] {  // resident CTAs per SM (the kernel's shared memory decides)
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, box_lane_kernel, kLaneThreads, 0) != cudaSuccess) {
       cudaGetLastError();
       n = 1;
     }
-    per_sm = std::max(n, 1);
-  }
+    return std::max(n, 1);
+  }();
   box_lane_kernel<<<std::max(sms, 1) * per_sm, kLaneThreads, 0, st>>>(J);
   return cudaGetLastError();
 }
