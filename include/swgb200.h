@@ -192,7 +192,8 @@ int sw_query(sw_ctx* ctx, const char* key, int64_t* value);
  * layout) and the output are the caller's device buffers, and the work is ordered on `stream`
  * (a cudaStream_t, NULL = the legacy default stream).  It calls no cudaMalloc or cudaFree: the
  * kernel's scratch is a 64 MiB array in the library's device image, present on every GPU that
- * loads the library until the process exits.  Sequences up to 16,383 residues.  The first call
+ * loads the library until the process exits.  Sequences up to 16,383 residues: a longer one in the
+ * block returns SW_E_UNSUPPORTED before anything is launched.  The first call
  * on a device looks up that array's address with the device current; make that first call before
  * any stream capture.  Calls share the array: calls whose kernels overlap on the GPU race and
  * must be ordered by the caller.  The call waits for its input checks (small copies of the
