@@ -554,7 +554,10 @@ int sw_set_option(sw_ctx* ctx, const char* key, int64_t value) {
   swg::EngineOptions& o = ctx->engine->options();
   if (k == "int16_threshold") o.int16_threshold = value;
   else if (k == "use_graph") o.use_graph = value ? 1 : 0;
-  else if (k == "two_pass") o.two_pass = value ? 1 : 0;
+  else if (k == "two_pass") {
+    if (value < 0 || value > 2) return fail(ctx, SW_E_ARG, "two_pass must be 0, 1 or 2");
+    o.two_pass = (int)value;
+  }
   else if (k == "box_lane") o.box_lane = value ? 1 : 0;
   else if (k == "chunk") {
     if (value < 32 || value > 1024) return fail(ctx, SW_E_ARG, "chunk must be in [32, 1024]");

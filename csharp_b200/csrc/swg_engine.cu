@@ -1273,10 +1273,18 @@ class EngineImpl : public Engine {
     const bool nw = P.mode == kModeNw;
     const bool kim = P.dist_fn != 0 && !P.protein;  // Kimura2 / JukesCantor: 32-bit lanes
     pl.plain_only = B.alpha > kMaxAlpha16 || (nw && !B.nw16) || kim || P.lanes == SW_LANES_32;
-    // Two passes pay off where the reverse scan's gap chain is short: it decays by min(o, e) per
-    // column, and with e = 1 (BLOSUM62 10/1) it runs past the box kernel's 64-column window for
-    // most pairs, which then go to 32-bit lanes: such jobs keep the one-pass counter kernel.
-    pl.kind = nw ? kKindNw : (opt_.two_pass && std::min(P.o, P.e) >= 2) ? kKindScore : kKindSw;
+    // Two passes pay off only where the box step finishes nearly every pair: a pair it gives up
+    // on costs the int32 full DP, about nine times a score-pass cell, so a few per cent of them
+    // eat the gain.  The box step needs short local alignments and short gap chains (they decay by
+    // min(o, e) per column).  Measured on the CPU with the box step's own source over uneven DNA
+    // families (EDNAFULL) and BLOSUM62 protein families: with o >= 3 max S and e >= 3 it finished
+    // 93-100 % of the pairs; with cheaper opening (EDNAFULL o <= 12, any BLOSUM62 setting) unrelated
+    // sequences align over most of their length and it finished 0-70 % (EDNAFULL 10/3: 3 %); with
+    // e <= 2 the gap chains outrun its window (BLOSUM62 10/1: 2 %).  two_pass = 1 applies that
+    // rule, 2 uses two passes whenever min(o, e) >= 2, 0 never.
+    const bool two_pass_ok = std::min(P.o, P.e) >= 2 &&
+                             (opt_.two_pass == 2 || (opt_.two_pass == 1 && P.o >= 3 * B.max_s && P.e >= 3));
+    pl.kind = nw ? kKindNw : two_pass_ok ? kKindScore : kKindSw;
     std::vector<int2> big;
     if (pl.plain_only) {
       for (int q = key.row_lo; q <= key.row_hi; q++)

@@ -160,8 +160,10 @@ int sw_compute_rank_blocks(sw_ctx* ctx, int32_t rank, int32_t world_size, int16_
  * lanes; -1 restores the value derived from the lane range), "use_graph" (0/1), "chunk"
  * (database entries per work item), "rows_per_lane" (0 = chosen per query, else an even number 4..16),
  * "plan_only" (1: engine calls build their work plans and graphs but launch nothing; 0: run),
- * "two_pass" (1, the default: SW-Gotoh with open and extend >= 2 runs a score-only pass and finds
- * each pair's counters near its best cell; 0: the one-pass counter kernels), "box_lane" (1: the
+ * "two_pass" (SW-Gotoh: a score-only pass, then each pair's counters from the neighbourhood of
+ * its best cell; 1, the default: where open >= 3 x the largest substitution score and extend >= 3,
+ * the gap costs with which that neighbourhood stays small; 2: whenever open and extend >= 2; 0:
+ * never, the one-pass counter kernels), "box_lane" (1: the
  * two-pass box step runs one pair per thread first; 0, the default: the warp-per-pair kernel only).
  * Every knob gives the same distances.  Unknown keys are SW_E_ARG. */
 int sw_set_option(sw_ctx* ctx, const char* key, int64_t value);

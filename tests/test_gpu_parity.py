@@ -424,6 +424,7 @@ def test_two_pass_with_most_pairs_falling_back(cs):
     one.set_option("two_pass", 0)
     want, pairs, _ = one.all_pairs(1)
     two = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 3, 2).upload(seqs)
+    two.set_option("two_pass", 2)  # two passes although the default rule keeps 3/2 on one
     got, _, _ = two.all_pairs(1)
     assert two.query("box_fallbacks") > pairs // 2
     assert two.query("lane16_pairs") + two.rerun_count() == pairs
@@ -432,17 +433,19 @@ def test_two_pass_with_most_pairs_falling_back(cs):
 
 @pytest.mark.parametrize("o,e", [(16, 4), (10, 3), (20, 8), (4, 2)])
 def test_lane_box_kernel_on_uneven_lengths(cs, oracle_mod, o, e):
-    """Lognormal lengths (median 400, sigma 0.6, clipped 50-1500) from 200 family roots: the box
-    step runs one pair per thread for most pairs, hands taller scans and wider bands to the warp
-    kernel and window overflows to the 32-bit lanes.  Every entry equals the one-pass counter
-    kernel's and the warp-only box step's; a sample equals the oracle's."""
+    """Lognormal lengths (median 400, sigma 0.6, clipped 50-1500) from 200 family roots, two
+    passes forced at every gap setting: the box step runs one pair per thread for most pairs at
+    16/4, hands taller scans and wider bands to the warp kernel and window overflows to the 32-bit
+    lanes (most pairs at 10/3 and 4/2).  Every entry equals the one-pass counter kernel's, the
+    warp-only box step's and the default choice's; a sample equals the oracle's."""
     from csharp_b200 import synth
     rng = np.random.default_rng(91 + o)
     lens = synth.lognormal_lengths(900, 400, 0.6, 50, 1500, rng)
     seqs = [s.tobytes() for s in synth.dna_family(900, 200, lens, seed=92)]
     m = cs.ScoringMatrix.Load("EDNAFULL")
     res = {}
-    for tag, opts in (("one", {"two_pass": 0}), ("warp", {"box_lane": 0}), ("lane", {"box_lane": 1})):
+    for tag, opts in (("one", {"two_pass": 0}), ("warp", {"two_pass": 2, "box_lane": 0}),
+                      ("lane", {"two_pass": 2, "box_lane": 1}), ("auto", {})):
         eng = cs.Engine(m, o, e).upload(seqs)
         for k, v in opts.items():
             eng.set_option(k, v)
@@ -453,6 +456,7 @@ def test_lane_box_kernel_on_uneven_lengths(cs, oracle_mod, o, e):
         eng.close()
     np.testing.assert_array_equal(res["lane"], res["one"])
     np.testing.assert_array_equal(res["warp"], res["one"])
+    np.testing.assert_array_equal(res["auto"], res["one"])
     N = len(seqs)
     ii = rng.integers(1, N, 1500)
     jj = (rng.random(1500) * ii).astype(np.int64)
