@@ -307,11 +307,11 @@ def main():
     ap.add_argument("--serving-only", action="store_true", help="only the serving workload (one JSON line)")
     ap.add_argument("--configs-only", action="store_true", help="only configurations 1, 2 and 4 (one JSON line)")
     ap.add_argument("--serve-seconds", type=float, default=SERVE["seconds"])
-    ap.add_argument("--box-lane", type=int, default=-1, choices=[-1, 0, 1],
-                    help="two-pass box step: 1 one pair per thread first, 0 warp kernel only (-1: engine default)")
+    ap.add_argument("--box-reg", type=int, default=-1, choices=[-1, 0, 1],
+                    help="two-pass box step: 1 register box step first, 0 warp box kernel only (-1: engine default)")
     a = ap.parse_args()
-    if a.box_lane >= 0:
-        ENGINE_OPTIONS["box_lane"] = a.box_lane
+    if a.box_reg >= 0:
+        ENGINE_OPTIONS["box_reg"] = a.box_reg
     if a.serving_only:
         import csharp_b200 as cs
         print(json.dumps({"serving": serving(cs, 0, a.serve_seconds, SERVE["load"])}))

@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "../../include/swgb200.h"
+#include "swg_box_reg.cuh"
 #include "swg_device.cuh"
 #include "swg_engine.h"
 #include "swg_internal.h"
@@ -80,9 +81,11 @@ struct EngineJob {
   int mpad;                 // profile rows staged (passes * 32 * K of the bin)
   int protein;              // NW distance rule: similarity over the full length
   unsigned long long* stats; // [0] items taken, [1] pairs finished in 16-bit lanes, [2] tripped
-  int4* box;                // two-pass: pairs whose counters the box kernel finds
+  int4* box;                // two-pass: pairs whose counters the box step finds
+  uint32_t* boxwin;         // two-pass: per box record, the threshold codes of the 128 rows above ie
   int* box_count;
   int box_cap;
+  uint32_t* rowbuf;         // two-pass: per (CTA, warp) slot, mpad words: each row's best V (lanes A | B)
   // Query mode (serving): s1 is query slot q of a separate set, s2 every database entry of the
   // chunk, the distance goes to qout[q][d].  Raw residue bytes index qtab/qflag (row 127 = pad).
   int qmode;
@@ -293,12 +296,14 @@ __device__ __forceinline__ void align_two(const uint32_t* __restrict__ prof, int
 // Score-only counterpart of align_two (first pass of the two-pass SW path): the same DP without
 // counters, keeping per query row the best V and the column where it was first reached.  Returns
 // per lane half the best score and its cell (row and column, 0-based) in the reference's order
-// (first strictly greater in row-major order).
+// (first strictly greater in row-major order), and stores each row's best V (value + bias, lanes
+// A | B) at rowbuf[row]: the box step's bound of that row (padding columns can only raise it).
 template <int K, int NP>
 __device__ __forceinline__ void score_two(const uint32_t* __restrict__ prof, int mpad, int passes,
                                           const uint8_t* __restrict__ ca,
                                           const uint8_t* __restrict__ cb, int ncols,
                                           const EngineJob& J, uint32_t* __restrict__ scr,
+                                          uint32_t* __restrict__ rowbuf,
                                           int lane, int& bestA, int& rowA, uint32_t& colA,
                                           int& bestB, int& rowB, uint32_t& colB) {
   const uint32_t bias2 = (uint32_t)J.bias * 0x10001u;
@@ -381,6 +386,9 @@ __device__ __forceinline__ void score_two(const uint32_t* __restrict__ prof, int
       }
     }
     __syncwarp();
+#pragma unroll
+    for (int r = 0; r < K; r += 2)
+      *reinterpret_cast<uint2*>(rowbuf + pbase + lane * K + r) = make_uint2(BEST[r], BEST[r + 1]);
 #pragma unroll
     for (int r = 0; r < K; r++) {
       const int row = pbase + lane * K + r;
@@ -620,6 +628,7 @@ __global__ void __launch_bounds__(warps_of(K, KIND) * 32, ctas_of(K, KIND)) engi
   uint8_t* ca = codes + (size_t)warp * 2 * cbuf;
   uint8_t* cb = ca + cbuf;
   uint32_t* scr = J.scratch + ((long)blockIdx.x * kEngWarps + warp) * (long)J.maxcol * kScr;
+  uint32_t* rowb = J.rowbuf ? J.rowbuf + ((long)blockIdx.x * kEngWarps + warp) * (long)J.mpad : nullptr;
   if (threadIdx.x == 0) s_q = -1;
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(J.counter, 1);
@@ -695,32 +704,75 @@ __global__ void __launch_bounds__(warps_of(K, KIND) * 32, ctas_of(K, KIND)) engi
       for (int k = 32 + ncols + lane; k < 64 + ncols; k += 32) { ca[k] = (uint8_t)J.A; cb[k] = (uint8_t)J.A; }
       __syncwarp();
       if constexpr (KIND == kKindScore) {
-        // first pass of the two-pass path: best score and cell; the box kernel finds the counters
+        // first pass of the two-pass path: best score, its cell and the rows' bounds; the box step
+        // finds the counters
         int bA = 0, rA = 0, bB = 0, rB = 0;
         uint32_t cA = 0, cB = 0;
         if (m > 0 && ncols > 0)
-          score_two<K, NP>(prof, J.mpad, passes, ca, cb, ncols, J, scr, lane, bA, rA, cA, bB, rB, cB);
+          score_two<K, NP>(prof, J.mpad, passes, ca, cb, ncols, J, scr, rowb, lane, bA, rA, cA, bB, rB, cB);
         warp_best(bA, rA, cA);
         warp_best(bB, rB, cB);
+        bA = __shfl_sync(0xffffffffu, bA, 0);
+        rA = __shfl_sync(0xffffffffu, rA, 0);
+        cA = __shfl_sync(0xffffffffu, cA, 0);
+        bB = __shfl_sync(0xffffffffu, bB, 0);
+        rB = __shfl_sync(0xffffffffu, rB, 0);
+        cB = __shfl_sync(0xffffffffu, cB, 0);
+        const bool goA = m > 0 && nA > 0 && bA > 0 && bA <= J.thresh;
+        const bool goB = dB >= 0 && m > 0 && nB > 0 && bB > 0 && bB <= J.thresh;
+        int wA = 0, wB = 0;
         if (lane == 0) {
           unsigned long long done16 = 0;
-          auto finish = [&](int d, int n, int best, int row, uint32_t col) {
+          auto other = [&](int d, int n, int best) {  // pairs that skip the box step
             if (m == 0 || n == 0 || best <= 0) {  // empty alignment: 0/0
               emit(J, q, d, fraction_distance(0, 0));
               done16++;
-            } else if (best > J.thresh) {  // the 16-bit lanes may have saturated: 32-bit DP
+            } else {  // the 16-bit lanes may have saturated: 32-bit DP
               const int w = atomicAdd(J.rerun_count, 1);
               if (w < J.rerun_cap) J.rerun[w] = make_int2(q, d);
               atomicAdd(J.stats + 2, 1ull);
-            } else {
-              const int w = atomicAdd(J.box_count, 1);
-              if (w < J.box_cap) J.box[w] = make_int4(q, d, best, (int)(((uint32_t)(row + 1) << 16) | (col + 1)));
-              done16++;
             }
           };
-          finish(dA, nA, bA, rA, cA);
-          if (dB >= 0) finish(dB, nB, bB, rB, cB);
-          atomicAdd(J.stats + 1, done16);
+          if (!goA) other(dA, nA, bA);
+          if (dB >= 0 && !goB) other(dB, nB, bB);
+          const int ng = (int)goA + (int)goB;
+          if (ng) {
+            wA = atomicAdd(J.box_count, ng);
+            wB = wA + (int)goA;
+          }
+          atomicAdd(J.stats + 1, done16 + (unsigned long long)ng);
+        }
+        wA = __shfl_sync(0xffffffffu, wA, 0);
+        wB = __shfl_sync(0xffffffffu, wB, 0);
+        __syncwarp();  // the rows' bounds in rowb are visible to every lane
+        // each half-warp writes one pair's box record and the threshold codes of its 128 rows
+        // above ie (rows further up share one threshold, in the record)
+        const int hl = lane & 15;
+        const bool hB = lane >= 16;
+        const bool go = hB ? goB : goA;
+        const int S = hB ? bB : bA, ie = (hB ? rB : rA) + 1, w = hB ? wB : wA;
+        uint32_t word = 0u;
+        int umax = 0;
+        if (go) {
+          auto bound = [&](int i) {  // position row i >= 1: the best V of query row i - 1
+            const uint32_t v = rowb[i - 1];
+            return (int)(int16_t)(hB ? (v >> 16) : (v & 0xFFFFu)) - J.bias;
+          };
+#pragma unroll
+          for (int u = 0; u < 8; u++) {
+            const int i = ie - 1 - (hl * 8 + u);
+            const int ub = i >= 1 ? bound(i) : 0;
+            word |= (uint32_t)reg_code_of(S - min(ub, S)) << (4 * u);
+          }
+          for (int i = 1 + hl; i <= ie - 1 - kRegWinRows; i += 16) umax = max(umax, bound(i));
+        }
+#pragma unroll
+        for (int x = 8; x >= 1; x >>= 1) umax = max(umax, __shfl_xor_sync(0xffffffffu, umax, x));
+        if (go && w < J.box_cap) {
+          J.boxwin[(long long)w * kRegWinWords + hl] = word;
+          if (hl == 0)
+            J.box[w] = make_int4(q, hB ? dB : dA, S | ((S - min(umax, S)) << 16),
+                                 (int)(((uint32_t)ie << 16) | ((hB ? cB : cA) + 1)));
         }
         __syncwarp();
         continue;
@@ -788,6 +840,9 @@ namespace {
 
 constexpr int kNumK = 7;
 constexpr int kKs[kNumK] = {4, 6, 8, 10, 12, 14, 16};
+// Engine work counters: items taken, pairs finished in 16-bit lanes, tripped 16-bit lanes, pairs
+// the box step gave up on, pairs handed to the warp box kernel.
+constexpr int kNumStats = 8;
 
 // Largest alphabet of the 16-bit lanes (two-plane profiles beyond 8 letters).
 constexpr int kMaxAlpha16 = 32;
@@ -903,6 +958,7 @@ struct Bin {
   size_t smem = 0;
   int grid = 0;
   size_t scratch_off = 0;  // words into the pass scratch (bins run concurrently)
+  size_t rowbuf_off = 0;   // two-pass: words into the rows' bounds buffer
   double padded = 0;       // cells computed, padding rows included
 };
 
@@ -935,17 +991,28 @@ struct Base {
   size_t scratch_bytes = 0;
   void* d_carry = nullptr;
   long carry_threads = 0;
-  // two-pass SW: the first pass's (pair, best score, best cell) list and the box kernel's scratch
+  // two-pass SW: the first pass's box records (pair, best score, best cell) with the threshold
+  // codes of the rows above each best cell, the box step's band classes and the pairs it hands to
+  // the warp box kernel, and the score kernels' per-warp row bounds
   int4* d_box = nullptr;
-  int* d_box_count = nullptr;
+  uint32_t* d_boxwin = nullptr;
+  int* d_cls[2] = {nullptr, nullptr};
+  int* d_counts = nullptr;     // [0] box records, [1] spilled pairs, [2..5] band classes
   long long box_cap = 0;
-  // pairs the lane box kernel hands to the warp box kernel (same capacity as d_box)
   int4* d_spill = nullptr;
-  int* d_spill_count = nullptr;
+  long long spill_cap = 0;
+  uint32_t* d_rowbuf = nullptr;
+  size_t rowbuf_bytes = 0;
+  void free_box() {
+    cudaFree(d_box); cudaFree(d_boxwin); cudaFree(d_cls[0]); cudaFree(d_cls[1]); cudaFree(d_spill);
+    d_box = nullptr; d_boxwin = nullptr; d_cls[0] = d_cls[1] = nullptr; d_spill = nullptr;
+    box_cap = spill_cap = 0;
+  }
   ~Base() {
     cudaFree(d_code); cudaFree(d_sorted); cudaFree(d_lettab); cudaFree(d_flagtab);
     cudaFree(d_scratch); cudaFree(d_carry);
-    cudaFree(d_box); cudaFree(d_box_count); cudaFree(d_spill); cudaFree(d_spill_count);
+    free_box();
+    cudaFree(d_counts); cudaFree(d_rowbuf);
   }
 };
 
@@ -1026,7 +1093,6 @@ int build_base(Base& B, const EngineParams& P, std::string* msg) {
 struct Plan {
   bool plain_only = false;
   int kind = kKindSw;       // the bins' kernel: SW with counters, NW, or the two-pass first pass
-  bool box_lane = false;    // two-pass: the lane box kernel ran before the warp box kernel
   bool zeroes_diagonal = false;
   int thresh = 0;
   std::vector<Bin> bins;
@@ -1087,8 +1153,8 @@ class EngineImpl : public Engine {
     if (k == "launches") {
       int64_t n = 2;  // the 32-bit lane kernel and the rerun-count reset
       for (auto& bn : last_->bins) n += bn.items.empty() ? 0 : 1;
-      if (!last_->plain_only && last_->kind == kKindScore)  // the box kernels
-        n += (last_->box_lane ? 2 : 1);
+      if (!last_->plain_only && last_->kind == kKindScore)  // the box step: scan, 4 band classes, warp kernel
+        n += opt_.box_reg ? 6 : 1;
       return n + (last_->zeroes_diagonal ? 1 : 0);
     }
     if (k == "bins") {
@@ -1097,12 +1163,12 @@ class EngineImpl : public Engine {
       return n;
     }
     if (k == "alphabet") return base_ ? base_->alpha : 0;
-    if (k == "items" || k == "lane16_pairs" || k == "tripped" || k == "box_fallbacks") {
+    if (k == "items" || k == "lane16_pairs" || k == "tripped" || k == "box_fallbacks" || k == "box_spilled") {
       if (!last_->d_stats) return 0;
-      unsigned long long h[4] = {0, 0, 0, 0};
+      unsigned long long h[kNumStats] = {};
       cudaDeviceSynchronize();
       cudaMemcpy(h, last_->d_stats, sizeof(h), cudaMemcpyDeviceToHost);
-      return (int64_t)(k == "items" ? h[0] : k == "lane16_pairs" ? h[1] : k == "tripped" ? h[2] : h[3]);
+      return (int64_t)(k == "items" ? h[0] : k == "lane16_pairs" ? h[1] : k == "tripped" ? h[2] : k == "box_fallbacks" ? h[3] : h[4]);
     }
     if (k == "planned_items") {
       int64_t n = 0;
@@ -1379,12 +1445,13 @@ class EngineImpl : public Engine {
       for (size_t k : ord) all.push_back(bn.items[k]);
     }
     if ((rc = upload_vec(&pl.d_items, all, msg, "items"))) return rc;
-    std::vector<unsigned long long> st0(4, 0ull);
+    std::vector<unsigned long long> st0(kNumStats, 0ull);
     if ((rc = upload_vec(&pl.d_stats, st0, msg, "stats"))) return rc;
     std::vector<int> zeros(pl.bins.size() + 1, 0);
     if ((rc = upload_vec(&pl.d_counters, zeros, msg, "counters"))) return rc;
-    // the bins run concurrently: each multi-pass bin gets its own scratch slots
-    size_t scr_words = 0;
+    // the bins run concurrently: each multi-pass bin gets its own scratch slots (and each
+    // score bin its own rows' bounds)
+    size_t scr_words = 0, row_words = 0;
     for (auto& bn : pl.bins) {
       if (bn.items.empty()) continue;
       bn.smem = engine_smem(A, bn.mpad, B.maxcol, bn.K, pl.kind);
@@ -1394,6 +1461,8 @@ class EngineImpl : public Engine {
       bn.grid = (int)std::min<long>((long)P.sms * occ, (long)bn.items.size());
       bn.scratch_off = scr_words;
       if (bn.max_passes > 1) scr_words += (size_t)bn.grid * warps_of(bn.K, pl.kind) * B.maxcol * (nw ? kScrWordsNw : kScrWords);
+      bn.rowbuf_off = row_words;
+      if (pl.kind == kKindScore) row_words += (size_t)bn.grid * warps_of(bn.K, pl.kind) * bn.mpad;
     }
     pl.order.clear();
     for (size_t b = 0; b < pl.bins.size(); b++)
@@ -1416,29 +1485,40 @@ class EngineImpl : public Engine {
     const int64_t spare = pl.kind == kKindScore ? pl.npairs : std::max<int64_t>(1 << 16, pl.npairs / 16);
     pl.rerun_cap = (int)std::min<int64_t>(pl.npairs + 1, (int64_t)big.size() + spare);
     if (pl.kind == kKindScore) {
-      if (pl.npairs > B.box_cap) {  // one list for every plan (plans run one after another)
+      // one set of box-step buffers for every plan (plans run one after another); every plan's
+      // graph holds their pointers, so growing them retires the graphs
+      auto retire = [&]() {
         for (auto& kv : plans_) if (kv.second->graph) { cudaGraphExecDestroy(kv.second->graph); kv.second->graph = nullptr; }
-        cudaFree(B.d_box);
-        cudaFree(B.d_spill);
-        B.d_box = nullptr;
-        B.d_spill = nullptr;
-        B.box_cap = 0;
-        const size_t bytes = sizeof(int4) * (size_t)std::max<int64_t>(pl.npairs, 1);
-        if (cudaMalloc(&B.d_box, bytes) != cudaSuccess || cudaMalloc(&B.d_spill, bytes) != cudaSuccess) {
+      };
+      if (pl.npairs > B.box_cap) {
+        retire();
+        B.free_box();
+        const size_t n = (size_t)std::max<int64_t>(pl.npairs, 1);
+        const size_t nspill = std::max<size_t>(n / 16, 1 << 16);
+        if (cudaMalloc(&B.d_box, sizeof(int4) * n) != cudaSuccess ||
+            cudaMalloc(&B.d_boxwin, sizeof(uint32_t) * kRegWinWords * n) != cudaSuccess ||
+            cudaMalloc(&B.d_cls[0], sizeof(int) * n) != cudaSuccess ||
+            cudaMalloc(&B.d_cls[1], sizeof(int) * n) != cudaSuccess ||
+            cudaMalloc(&B.d_spill, sizeof(int4) * nspill) != cudaSuccess) {
           cudaGetLastError();
-          cudaFree(B.d_box);
-          B.d_box = nullptr;
-          B.d_spill = nullptr;
+          B.free_box();
           *msg = "cudaMalloc two-pass pair lists";
           return SW_E_OOM;
         }
-        B.box_cap = std::max<int64_t>(pl.npairs, 1);
+        B.box_cap = (long long)n;
+        B.spill_cap = (long long)nspill;
       }
-      if (!B.d_box_count && cudaMalloc(&B.d_box_count, sizeof(int)) != cudaSuccess) {
-        cudaGetLastError(); B.d_box_count = nullptr; *msg = "cudaMalloc two-pass count"; return SW_E_OOM;
+      if (!B.d_counts && cudaMalloc(&B.d_counts, sizeof(int) * 8) != cudaSuccess) {
+        cudaGetLastError(); B.d_counts = nullptr; *msg = "cudaMalloc two-pass counts"; return SW_E_OOM;
       }
-      if (!B.d_spill_count && cudaMalloc(&B.d_spill_count, sizeof(int)) != cudaSuccess) {
-        cudaGetLastError(); B.d_spill_count = nullptr; *msg = "cudaMalloc two-pass count"; return SW_E_OOM;
+      const size_t rb = std::max<size_t>(row_words * 4, 16);
+      if (rb > B.rowbuf_bytes) {
+        retire();
+        cudaFree(B.d_rowbuf);
+        B.d_rowbuf = nullptr;
+        B.rowbuf_bytes = 0;
+        if (cudaMalloc(&B.d_rowbuf, rb) != cudaSuccess) { cudaGetLastError(); *msg = "cudaMalloc row bounds"; return SW_E_OOM; }
+        B.rowbuf_bytes = rb;
       }
     }
     std::vector<int2> rl(big);
@@ -1459,10 +1539,10 @@ class EngineImpl : public Engine {
       zero_diagonal_kernel<<<(P.nseq + 255) / 256, 256, 0, P.stream>>>(P.out, P.ld, P.nseq);
     set_int_kernel<<<1, 1, 0, P.stream>>>(pl.d_rerun_count, pl.big_count);
     const bool two = !pl.plain_only && pl.kind == kKindScore;
-    if (two && (e = cudaMemsetAsync(B.d_box_count, 0, sizeof(int), P.stream)) != cudaSuccess) return e;
+    if (two && (e = cudaMemsetAsync(B.d_counts, 0, sizeof(int) * 8, P.stream)) != cudaSuccess) return e;
     if (!pl.plain_only) {
       if ((e = cudaMemsetAsync(pl.d_counters, 0, sizeof(int) * (pl.bins.size() + 1), P.stream)) != cudaSuccess) return e;
-      if ((e = cudaMemsetAsync(pl.d_stats, 0, sizeof(unsigned long long) * 4, P.stream)) != cudaSuccess) return e;
+      if ((e = cudaMemsetAsync(pl.d_stats, 0, sizeof(unsigned long long) * kNumStats, P.stream)) != cudaSuccess) return e;
       EngineJob J;
       std::memset(&J, 0, sizeof(J));
       J.code = B.d_code; J.off = P.off; J.sorted = B.d_sorted;
@@ -1474,7 +1554,8 @@ class EngineImpl : public Engine {
       J.scratch = B.d_scratch; J.maxcol = B.maxcol;
       J.rerun = pl.d_rerun; J.rerun_count = pl.d_rerun_count; J.rerun_cap = pl.rerun_cap;
       J.stats = pl.d_stats;
-      J.box = B.d_box; J.box_count = B.d_box_count; J.box_cap = (int)std::min<long long>(B.box_cap, 0x7fffffff);
+      J.box = B.d_box; J.boxwin = B.d_boxwin; J.box_count = B.d_counts;
+      J.box_cap = (int)std::min<long long>(B.box_cap, 0x7fffffff);
       // fork: each bin on its own stream, all after the resets above; join before the rerun
       if (bins_t0 && (e = cudaEventRecord(bins_t0, P.stream)) != cudaSuccess) return e;
       const bool fork = pl.order.size() > 1;
@@ -1489,6 +1570,7 @@ class EngineImpl : public Engine {
         J.counter = pl.d_counters + b;
         J.mpad = bn.mpad;
         J.scratch = B.d_scratch + bn.scratch_off;
+        J.rowbuf = two ? B.d_rowbuf + bn.rowbuf_off : nullptr;
         if ((e = launch_engine_k(bn.K, pl.kind, J, bn.grid, bn.smem, st)) != cudaSuccess) return e;
         if (fork) {
           if ((e = cudaEventRecord(join_[x], st)) != cudaSuccess) return e;
@@ -1498,32 +1580,33 @@ class EngineImpl : public Engine {
       if (bins_t1 && (e = cudaEventRecord(bins_t1, P.stream)) != cudaSuccess) return e;
     }
     if (two) {
-      // counters of the first pass's best cells from boxes around their traceback paths
+      // counters of the first pass's best cells from regions around their traceback paths: the
+      // register scan and band DPs (swg_box_reg.cuh), then the warp box kernel for the pairs whose
+      // region is wider than theirs
       BoxJob X;
       std::memset(&X, 0, sizeof(X));
       X.seq = B.d_code; X.off = P.off;
-      X.list = B.d_box; X.count = B.d_box_count;
+      X.list = B.d_box; X.count = B.d_counts; X.win = B.d_boxwin;
+      X.cls[0] = B.d_cls[0]; X.cls[1] = B.d_cls[1]; X.cls_count = B.d_counts + 2;
       X.out = P.out; X.ld = P.ld; X.mirror = P.mode != kModeSwgMs;
       X.lettab = B.d_lettab; X.flagtab = B.d_flagtab; X.A = B.alpha; X.o = P.o; X.e = P.e;
       X.maxlen = B.maxcol;
-      X.budget = 1 << 16;
       X.rerun = pl.d_rerun; X.rerun_count = pl.d_rerun_count; X.rerun_cap = pl.rerun_cap;
       X.stats = pl.d_stats;
       X.list_cap = B.box_cap;
-      pl.box_lane = opt_.box_lane && P.o + P.e < 8192;
-      if (pl.box_lane) {
-        // one pair per thread; a score above 127 max S needs more than 254 rows + columns
-        BoxJob L = X;
-        L.max_score = 127 * std::max(B.max_s, 0);
-        L.spill = B.d_spill; L.spill_count = B.d_spill_count;
-        L.spill_cap = (int)std::min<long long>(B.box_cap, 0x7fffffff);
-        if ((e = cudaMemsetAsync(B.d_spill_count, 0, sizeof(int), P.stream)) != cudaSuccess) return e;
-        if ((e = launch_box_lane(L, P.sms, P.stream)) != cudaSuccess) return e;
-        X.list = B.d_spill; X.count = B.d_spill_count;
+      X.spill = B.d_spill; X.spill_count = B.d_counts + 1;
+      X.spill_cap = (int)std::min<long long>(B.spill_cap, 0x7fffffff);
+      BoxJob Y = X;
+      if (opt_.box_reg) {
+        if ((e = launch_box_scan(X, P.sms, P.stream)) != cudaSuccess) return e;
+        for (int c = 0; c < 4; c++)
+          if ((e = launch_box_band(X, c, P.sms, P.stream)) != cudaSuccess) return e;
+        Y.list = B.d_spill; Y.count = B.d_counts + 1; Y.list_cap = B.spill_cap;
       }
       // the warp kernel's box has at most kWarpBoxMaxCols columns: a larger S / max S cannot fit
-      X.max_score = kWarpBoxMaxCols * std::max(B.max_s, 0);
-      if ((e = launch_box(X, (int)(B.carry_threads / 128), 128, P.stream)) != cudaSuccess) return e;
+      Y.max_score = kWarpBoxMaxCols * std::max(B.max_s, 0);
+      Y.budget = 1 << 16;
+      if ((e = launch_box(Y, (int)(B.carry_threads / 128), 128, P.stream)) != cudaSuccess) return e;
     }
     // 32-bit lanes: pairs the static guard routed here, those whose 16-bit lanes tripped, or all
     PlainJob R;

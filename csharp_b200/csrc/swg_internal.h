@@ -55,12 +55,17 @@ struct PairJob {
 
 // Second step of the two-pass SW path: for each pair the first pass found the best cell
 // (ie, je) and score S of, the counters of the reference's traceback path from a DP confined to
-// a box around that path (see box_kernel).
+// a region around that path (box_scan_kernel + box_band_kernel, then box_kernel for the pairs
+// whose region the first two cannot hold).
 struct BoxJob {
   const uint8_t* seq;      // dense residue codes 0..A-1 (the engine's), same offsets as the residues
   const int64_t* off;
-  const int4* list;        // (s1 index, s2 index, S, ie << 16 | je), ie and je 1-based
+  const int4* list;        // (s1 index, s2 index, S | T_rest << 16, ie << 16 | je), ie and je 1-based
   const int* count;
+  uint32_t* win;           // per list entry kRegWinWords threshold-code words (swg_box_reg.cuh)
+  int* cls[2];             // band classes 0..3 (width <= 8, 16, 24, 32): list indices, classes 0 / 2
+                           // from the front of cls[0] / cls[1], classes 1 / 3 from the back
+  int* cls_count;          // [4]
   int16_t* out;
   long long ld;
   int mirror;
@@ -73,21 +78,24 @@ struct BoxJob {
   int2* rerun;             // pairs given up on: the 32-bit full DP
   int* rerun_count;
   int rerun_cap;
-  unsigned long long* stats;  // [1] pairs finished in 16-bit lanes, [3] pairs given up on
+  unsigned long long* stats;  // [1] pairs finished in 16-bit lanes, [3] pairs given up on,
+                              // [4] pairs handed to the warp box kernel
   long long list_cap;      // entries `list` holds (the count is clipped to it)
-  int max_score;           // pairs with a larger S cannot fit: straight to the next step
-  int4* spill;             // lane kernel: pairs for the warp box kernel
+  int max_score;           // box_kernel: pairs with a larger S cannot fit: straight to the 32-bit lanes
+  int4* spill;             // box_scan_kernel: pairs for the warp box kernel
   int* spill_count;
   int spill_cap;
 };
 
 constexpr int kWarpBoxMaxCols = 256;  // box_kernel's largest box (columns and rows)
 
+// One pair per thread, DP rows in registers (swg_box_reg.cuh): the reverse scan sorts the pairs
+// into the band classes or hands them to J.spill; the band DP of class c writes distances and
+// hands the rest to the 32-bit lanes.
+cudaError_t launch_box_scan(const BoxJob& J, int sms, cudaStream_t st);
+cudaError_t launch_box_band(const BoxJob& J, int c, int sms, cudaStream_t st);
 // Warp per pair (reverse scan on 64-column shuffle windows, box DP as a 32-row wavefront).
 cudaError_t launch_box(const BoxJob& J, int grid, int block, cudaStream_t st);
-// One pair per thread (swg_box_lane.cuh); the pairs it cannot finish go to J.spill (for
-// launch_box) or, where the warp kernel could not finish them either, to the 32-bit lanes.
-cudaError_t launch_box_lane(const BoxJob& J, int sms, cudaStream_t st);
 
 size_t plain_carry_bytes(int mode, long threads, int maxlen, int dist_fn = 0);
 cudaError_t launch_plain_block(const PlainJob& J, int grid, int block, cudaStream_t st);

@@ -9,7 +9,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <type_traits>
-#include "swg_box_lane.cuh"
+#include "swg_box_reg.cuh"
 #include "swg_device.cuh"
 #include "swg_internal.h"
 
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
   const int o = J.o, e = J.e, dchain = min(J.e, J.o);
   for (long p = (long)blockIdx.x * kBoxWarps + warp; p < np; p += nwarps) {
     const int4 rec = J.list[p];
-    const int q = rec.x, d = rec.y, S = rec.z;
+    const int q = rec.x, d = rec.y, S = rec.z & 0xFFFF;
     const int ie = (int)((uint32_t)rec.w >> 16), je = rec.w & 0xFFFF;
     const uint8_t* a = J.seq + J.off[q];
     const uint8_t* b = J.seq + J.off[d];
@@ -419,66 +419,103 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
   }
 }
 
-// One pair per thread: the reverse scan and the band DP of swg_box_lane.cuh as one flattened loop
-// (a cell per iteration, the next pair at once when one finishes), 96 words of scratch per thread
-// in shared memory (thread-interleaved), 64 threads per CTA (7 CTAs per SM on B200's 228 KB).
-constexpr int kLaneThreads = 64;
+// ---- box step, one pair per thread with the DP rows in registers (swg_box_reg.cuh) -------------
+constexpr int kRegThreads = 128;
 
-// Where each pair's outcome goes: its distance, the warp box kernel's list (a taller scan or a
-// larger box than the lane kernel keeps), or the 32-bit lanes (a window overflow, which the warp
-// kernel's 64-column window meets too, or anything else).
-struct LaneEmit {
-  const BoxJob* J;
-  __device__ __forceinline__ void operator()(const int4& rec, int rc, uint32_t c) const {
-    const int q = rec.x, d = rec.y;
-    if (rc == 0) {
-      const int16_t dist = fraction_distance((int)(c & 0xFFu), (int)(c >> 8));
-      J->out[(long long)q * J->ld + d] = dist;
-      if (J->mirror) J->out[(long long)d * J->ld + q] = dist;
-      return;
-    }
-    if (rc == 1 || rc == 4) {
-      const int w = atomicAdd(J->spill_count, 1);
-      if (w < J->spill_cap) {
-        J->spill[w] = rec;
-        return;
-      }
-    }
-    const int wr = atomicAdd(J->rerun_count, 1);
-    if (wr < J->rerun_cap) J->rerun[wr] = make_int2(q, d);
-    atomicAdd(J->stats + 3, 1ull);
-    atomicAdd(J->stats + 1, ~0ull);  // no longer finished in 16-bit lanes
-  }
-};
+// The pair goes on to the 32-bit lanes (full DP).
+__device__ __forceinline__ void box_give_up(const BoxJob& J, int q, int d) {
+  const int wr = atomicAdd(J.rerun_count, 1);
+  if (wr < J.rerun_cap) J.rerun[wr] = make_int2(q, d);
+  atomicAdd(J.stats + 3, 1ull);
+  atomicAdd(J.stats + 1, ~0ull);  // no longer finished in 16-bit lanes
+}
 
-__global__ void __launch_bounds__(kLaneThreads) box_lane_kernel(BoxJob J) {
-  __shared__ int16_t sc[kBoxMaxA1 * kBoxMaxA1];
-  __shared__ uint8_t fl[kBoxMaxA1 * kBoxMaxA1];
-  __shared__ uint32_t scratch[kLaneWords * kLaneThreads];
+__global__ void __launch_bounds__(kRegThreads) box_scan_kernel(BoxJob J) {
+  __shared__ int sc[kBoxMaxA1 * kBoxMaxA1];
   const int A1 = J.A + 1;
   for (int k = threadIdx.x; k < A1 * A1; k += blockDim.x) {
-    sc[k] = (int16_t)(J.lettab[k] - J.o);
-    fl[k] = (uint8_t)(J.flagtab[k] & kFlagCount);
+    const int a = k / A1, c = k - a * A1;
+    sc[k] = (a == J.A || c == J.A) ? kRegPadScore : J.lettab[k] - J.o;
   }
   __syncthreads();
   const long long np = min((long long)*J.count, J.list_cap);
-  const LaneMem mem{scratch + threadIdx.x, kLaneThreads};
-  LaneEmit emit{&J};
-  lane_box_run(J.list, (long long)blockIdx.x * kLaneThreads + threadIdx.x, np,
-               (long long)gridDim.x * kLaneThreads, J.seq, J.off, sc, fl, A1, J.o, J.e, J.max_score, mem, emit);
+  auto emit = [&](long long p, const int4& rec, int rc, const RegBox& bx) {
+    const int bw = bx.bhi - bx.blo + 1;
+    if (rc == kRegScanOk && bw <= 32) {
+      // the thresholds are used up: the window's first words keep the box for the band DP
+      *reinterpret_cast<int4*>(J.win + p * kRegWinWords) = make_int4(bx.ci, bx.cj, bx.blo, bx.bhi);
+      const int c = bw <= 8 ? 0 : bw <= 16 ? 1 : bw <= 24 ? 2 : 3;
+      const int pos = atomicAdd(J.cls_count + c, 1);
+      J.cls[c >> 1][(c & 1) ? J.list_cap - 1 - pos : pos] = (int)p;
+      return;
+    }
+    // a wider window or band: the warp box kernel (its 64-column windows), else the 32-bit lanes
+    const int w = atomicAdd(J.spill_count, 1);
+    if (w < J.spill_cap) {
+      J.spill[w] = rec;
+      atomicAdd(J.stats + 4, 1ull);
+      return;
+    }
+    box_give_up(J, rec.x, rec.y);
+  };
+  reg_scan_run(J.list, J.win, (long long)blockIdx.x * kRegThreads + threadIdx.x, np,
+               (long long)gridDim.x * kRegThreads, J.seq, J.off, sc, A1, J.o, J.e, emit);
 }
 
-cudaError_t launch_box_lane(const BoxJob& J, int sms, cudaStream_t st) {
-  if (J.A + 1 > kBoxMaxA1 || J.o + J.e >= 8192) return cudaErrorInvalidValue;
-  static const int per_sm = [] {  // resident CTAs per SM (the kernel's shared memory decides)
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, box_lane_kernel, kLaneThreads, 0) != cudaSuccess) {
-      cudaGetLastError();
-      n = 1;
+template <int B>
+__global__ void __launch_bounds__(kRegThreads) box_band_kernel(BoxJob J, int c) {
+  __shared__ int scf[kBoxMaxA1 * kBoxMaxA1];
+  const int A1 = J.A + 1;
+  for (int k = threadIdx.x; k < A1 * A1; k += blockDim.x) {
+    const int a = k / A1, x = k - a * A1;
+    scf[k] = (a == J.A || x == J.A) ? (int)((uint32_t)kRegPadScore << 8)
+                                    : (int)(((uint32_t)(J.lettab[k] - J.o) << 8) | (J.flagtab[k] & kFlagCount));
+  }
+  __syncthreads();
+  const long long np = min((long long)J.cls_count[c], J.list_cap);
+  const int* idx = (c & 1) ? J.cls[c >> 1] + (J.list_cap - 1) : J.cls[c >> 1];
+  auto emit = [&](int, const int4& rec, bool ok, uint32_t cnt) {
+    if (!ok) {
+      box_give_up(J, rec.x, rec.y);
+      return;
     }
-    return std::max(n, 1);
-  }();
-  box_lane_kernel<<<std::max(sms, 1) * per_sm, kLaneThreads, 0, st>>>(J);
+    const int16_t dist = fraction_distance((int)(cnt & 0xFFFFu), (int)(cnt >> 16));
+    J.out[(long long)rec.x * J.ld + rec.y] = dist;
+    if (J.mirror) J.out[(long long)rec.y * J.ld + rec.x] = dist;
+  };
+  reg_band_run<B>(idx, (c & 1) ? -1 : 1, (long long)blockIdx.x * kRegThreads + threadIdx.x, np,
+                  (long long)gridDim.x * kRegThreads, J.list, J.win, J.seq, J.off, scf, A1, J.o, J.e, emit);
+}
+
+// Resident CTAs per SM of a kernel with kRegThreads threads (its registers decide), looked up once.
+template <class Kern>
+int reg_ctas_per_sm(Kern k) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kRegThreads, 0) != cudaSuccess) {
+    cudaGetLastError();
+    n = 1;
+  }
+  return std::max(n, 1);
+}
+
+cudaError_t launch_box_scan(const BoxJob& J, int sms, cudaStream_t st) {
+  if (J.A + 1 > kBoxMaxA1) return cudaErrorInvalidValue;
+  static const int per_sm = reg_ctas_per_sm(box_scan_kernel);
+  box_scan_kernel<<<std::max(sms, 1) * per_sm, kRegThreads, 0, st>>>(J);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_box_band(const BoxJob& J, int c, int sms, cudaStream_t st) {
+  if (J.A + 1 > kBoxMaxA1 || c < 0 || c > 3) return cudaErrorInvalidValue;
+  static const int per_sm[4] = {reg_ctas_per_sm(box_band_kernel<8>), reg_ctas_per_sm(box_band_kernel<16>),
+                                reg_ctas_per_sm(box_band_kernel<24>), reg_ctas_per_sm(box_band_kernel<32>)};
+  const int grid = std::max(sms, 1) * per_sm[c];
+  switch (c) {
+    case 0: box_band_kernel<8><<<grid, kRegThreads, 0, st>>>(J, c); break;
+    case 1: box_band_kernel<16><<<grid, kRegThreads, 0, st>>>(J, c); break;
+    case 2: box_band_kernel<24><<<grid, kRegThreads, 0, st>>>(J, c); break;
+    default: box_band_kernel<32><<<grid, kRegThreads, 0, st>>>(J, c); break;
+  }
   return cudaGetLastError();
 }
 

@@ -163,8 +163,9 @@ int sw_compute_rank_blocks(sw_ctx* ctx, int32_t rank, int32_t world_size, int16_
  * "two_pass" (SW-Gotoh: a score-only pass, then each pair's counters from the neighbourhood of
  * its best cell; 1, the default: where open >= 3 x the largest substitution score and extend >= 3,
  * the gap costs with which that neighbourhood stays small; 2: whenever open and extend >= 2; 0:
- * never, the one-pass counter kernels), "box_lane" (1: the
- * two-pass box step runs one pair per thread first; 0, the default: the warp-per-pair kernel only).
+ * never, the one-pass counter kernels), "box_reg" (two passes: 1, the default, finds each pair's
+ * counters with one thread per pair and the DP rows in registers, handing pairs whose alignment
+ * region is wider to the warp-per-pair box kernel; 0: the warp-per-pair kernel for every pair).
  * Every knob gives the same distances.  Unknown keys are SW_E_ARG. */
 int sw_set_option(sw_ctx* ctx, const char* key, int64_t value);
 
@@ -181,8 +182,9 @@ int sw_autotune(sw_ctx* ctx, int16_t* d_out, int64_t ld_out, int32_t weights[7])
 /* Counters of the last engine call: "launches" (kernels it enqueued), "pairs", "cells",
  * "bins" (rows-per-lane classes used), "alphabet" (distinct residue bytes), "planned_items",
  * and, after waiting for the device, "items" (work items taken), "lane16_pairs" (pairs finished
- * in 16-bit lanes) and "tripped" (16-bit lanes handed to 32-bit lanes).  Unknown keys are
- * SW_E_ARG. */
+ * in 16-bit lanes), "tripped" (16-bit lanes handed to 32-bit lanes), "box_spilled" (two-pass pairs
+ * the register box step handed to the warp box kernel) and "box_fallbacks" (two-pass pairs handed
+ * to 32-bit lanes).  Unknown keys are SW_E_ARG. */
 int sw_query(sw_ctx* ctx, const char* key, int64_t* value);
 
 /* ---- block handler without device allocation ------------------------------------------------ */

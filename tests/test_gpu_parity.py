@@ -397,12 +397,11 @@ def test_two_pass_equals_one_pass_and_oracle(cs, oracle_mod):
     assert two.query("box_fallbacks") > 0  # the near-identical family members
     assert two.query("lane16_pairs") + two.rerun_count() == pairs
     np.testing.assert_array_equal(got, want)
-    for lane in (0, 1):  # boxes by the warp kernel alone, or one pair per thread first
-        other = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4).upload(seqs)
-        other.set_option("box_lane", lane)
-        got_o, _, _ = other.all_pairs(1)
-        np.testing.assert_array_equal(got_o, want)
-        other.close()
+    other = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4).upload(seqs)
+    other.set_option("box_reg", 0)  # every box by the warp kernel
+    got_o, _, _ = other.all_pairs(1)
+    np.testing.assert_array_equal(got_o, want)
+    other.close()
     N = len(seqs)
     sel = rng.choice(N * (N - 1) // 2, 3000, replace=False)
     pr = np.array([(i, j) for i in range(N) for j in range(i)], dtype=np.int32)[sel]
@@ -432,29 +431,31 @@ def test_two_pass_with_most_pairs_falling_back(cs):
 
 
 @pytest.mark.parametrize("o,e", [(16, 4), (10, 3), (20, 8), (4, 2)])
-def test_lane_box_kernel_on_uneven_lengths(cs, oracle_mod, o, e):
+def test_register_box_step_on_uneven_lengths(cs, oracle_mod, o, e):
     """Lognormal lengths (median 400, sigma 0.6, clipped 50-1500) from 200 family roots, two
-    passes forced at every gap setting: the box step runs one pair per thread for most pairs at
-    16/4, hands taller scans and wider bands to the warp kernel and window overflows to the 32-bit
-    lanes (most pairs at 10/3 and 4/2).  Every entry equals the one-pass counter kernel's, the
-    warp-only box step's and the default choice's; a sample equals the oracle's."""
+    passes forced at every gap setting: the register box step (one pair per thread) finishes
+    nearly every pair at 16/4 and 20/8, hands wider regions to the warp box kernel and the rest to
+    the 32-bit lanes (most pairs at 10/3 and 4/2).  Every entry equals the one-pass counter
+    kernel's, the warp-only box step's and the default choice's; a sample equals the oracle's."""
     from csharp_b200 import synth
     rng = np.random.default_rng(91 + o)
     lens = synth.lognormal_lengths(900, 400, 0.6, 50, 1500, rng)
     seqs = [s.tobytes() for s in synth.dna_family(900, 200, lens, seed=92)]
     m = cs.ScoringMatrix.Load("EDNAFULL")
     res = {}
-    for tag, opts in (("one", {"two_pass": 0}), ("warp", {"two_pass": 2, "box_lane": 0}),
-                      ("lane", {"two_pass": 2, "box_lane": 1}), ("auto", {})):
+    for tag, opts in (("one", {"two_pass": 0}), ("warp", {"two_pass": 2, "box_reg": 0}),
+                      ("reg", {"two_pass": 2}), ("auto", {})):
         eng = cs.Engine(m, o, e).upload(seqs)
         for k, v in opts.items():
             eng.set_option(k, v)
         res[tag], pairs, _ = eng.all_pairs(1)
-        if tag == "lane":
+        if tag == "reg":
             assert eng.query("lane16_pairs") + eng.rerun_count() == pairs
-            assert eng.query("launches") >= 4
+            assert eng.query("launches") >= 8
+            if (o, e) in ((16, 4), (20, 8)):
+                assert eng.query("box_spilled") + eng.query("box_fallbacks") < 0.03 * pairs
         eng.close()
-    np.testing.assert_array_equal(res["lane"], res["one"])
+    np.testing.assert_array_equal(res["reg"], res["one"])
     np.testing.assert_array_equal(res["warp"], res["one"])
     np.testing.assert_array_equal(res["auto"], res["one"])
     N = len(seqs)
@@ -462,4 +463,4 @@ def test_lane_box_kernel_on_uneven_lengths(cs, oracle_mod, o, e):
     jj = (rng.random(1500) * ii).astype(np.int64)
     pr = np.stack([ii, jj], 1).astype(np.int32)
     ref = _oracle_distances(oracle_mod, seqs, pr, "EDNAFULL", float(o), float(e))
-    np.testing.assert_array_equal(res["lane"][pr[:, 0], pr[:, 1]], ref)
+    np.testing.assert_array_equal(res["reg"][pr[:, 0], pr[:, 1]], ref)
