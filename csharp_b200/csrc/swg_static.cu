@@ -9,14 +9,17 @@
 // offsets and the output in device memory it owns.
 //
 // The array is 64 MiB and lives in every GPU that loads this library until the process exits.
-// Calls share it and leave the last call's contents in it; nothing in it has to start at zero
-// (the tables are rewritten by every call and each carry row is written before it is read).
-// Calls whose kernels overlap on the GPU (different streams, or different host threads) race on
-// it: the caller must order them.  The first call on a device looks up the array's device
-// address (cudaGetSymbolAddress, with that device current) and keeps it; make that first call
-// before any stream capture.
+// Calls share it and leave the last call's contents in it; only the input check's two status
+// words have to start at zero, and every call clears them (the tables are rewritten by every call
+// and each carry row is written before it is read).  Calls whose kernels overlap on the GPU
+// (different streams, or different host threads) race on it: the caller must order them.  The
+// first call on a device looks up the array's device address (cudaGetSymbolAddress, with that
+// device current) and keeps it; make that first call before any stream capture.  A call runs
+// on cfg->device (made current for the call, the caller's current device restored before it
+// returns) and refuses buffers that are not that device's memory.
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 
@@ -52,49 +55,54 @@ int scratch_address(int device, void** out) {
   return SW_OK;
 }
 
-// Reads offsets [first, last] (device) into a small stack buffer, chunk by chunk, and returns
-// the longest sequence among them; SW_E_ARG on a malformed range.
-int longest(const int64_t* d_off, int first, int last, int* maxlen, cudaStream_t st) {
-  int64_t buf[512];
-  *maxlen = 0;
-  for (int k = first; k <= last; k += 511) {
-    const int n = std::min(512, last + 2 - k);
-    if (cudaMemcpyAsync(buf, d_off + k, sizeof(int64_t) * (size_t)n, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess) {
-      cudaGetLastError();
-      return SW_E_CUDA;
+// Status words of the input check, in the table region past the scores and flags.
+constexpr size_t kStatusOffset = size_t(48) << 10;
+enum { kBadLength = 1, kTooLong = 2, kBadResidue = 4 };
+
+// One warp per sequence of the block's row and column ranges: its length (non-negative, at most
+// 16,383 residues) and residues (inside the 127-entry scoring table); status[0] collects the
+// problems found, status[1] the longest length.
+__global__ void static_check_kernel(const uint8_t* seq, const int64_t* off, int rs, int re, int cs, int ce,
+                                    int* status) {
+  const int lane = threadIdx.x & 31;
+  const long nwarps = (long)gridDim.x * (blockDim.x >> 5);
+  const long nr = (long)re - rs + 1, total = nr + ((long)ce - cs + 1);
+  for (long w = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < total; w += nwarps) {
+    const long k = w < nr ? rs + w : cs + (w - nr);
+    const int64_t lo = off[k], len = off[k + 1] - lo;
+    if (len < 0 || len > 16383) {
+      if (lane == 0) atomicOr(status, len < 0 ? kBadLength : kTooLong);
+      continue;
     }
-    for (int i = 0; i + 1 < n; i++) {
-      const int64_t len = buf[i + 1] - buf[i];
-      if (len < 0 || len > 16383) return len < 0 ? SW_E_ARG : SW_E_UNSUPPORTED;
-      if (len > *maxlen) *maxlen = (int)len;
-    }
+    bool bad = false;
+    for (int64_t x = lane; x < len; x += 32) bad |= seq[lo + x] >= 127;
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(status, kBadResidue);
+    if (lane == 0) atomicMax(status + 1, (int)len);
   }
-  return SW_OK;
 }
 
-// Every residue of sequences [first, last] must index the 127-entry scoring table.
-int residues_in_table(const uint8_t* d_seq, const int64_t* d_off, int first, int last, cudaStream_t st) {
-  int64_t lo_hi[2];
-  if (cudaMemcpyAsync(&lo_hi[0], d_off + first, sizeof(int64_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-      cudaMemcpyAsync(&lo_hi[1], d_off + last + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-      cudaStreamSynchronize(st) != cudaSuccess) {
+// The caller's buffers must be memory this device can address as its own.
+bool on_device(const void* p, int device) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
     cudaGetLastError();
-    return SW_E_CUDA;
+    return false;
   }
-  uint8_t buf[4096];
-  for (int64_t k = lo_hi[0]; k < lo_hi[1]; k += (int64_t)sizeof(buf)) {
-    const size_t n = (size_t)std::min<int64_t>((int64_t)sizeof(buf), lo_hi[1] - k);
-    if (cudaMemcpyAsync(buf, d_seq + k, n, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess) {
-      cudaGetLastError();
-      return SW_E_CUDA;
-    }
-    for (size_t i = 0; i < n; i++)
-      if (buf[i] >= 127) return SW_E_ARG;
-  }
-  return SW_OK;
+  return (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) && at.device == device;
 }
+
+// Makes `device` current for the call and puts the caller's device back when the call returns.
+struct DeviceScope {
+  int prev = -1;
+  bool ok = false;
+  explicit DeviceScope(int device) {
+    if (cudaGetDevice(&prev) != cudaSuccess) return;
+    ok = prev == device || cudaSetDevice(device) == cudaSuccess;
+  }
+  ~DeviceScope() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
 
 }  // namespace
 
@@ -106,6 +114,8 @@ extern "C" int sw_compute_block_static(const sw_config* cfg, const uint8_t* d_re
   if (!cfg || !d_residues || !d_offsets || !d_out || count < 1) return SW_E_ARG;
   if (cfg->mode < 0 || cfg->mode > 2) return SW_E_ARG;
   if (cfg->alignment_type != SW_PROTEIN && cfg->alignment_type != SW_NUCLEIC) return SW_E_ARG;
+  if (cfg->distance_fn < 0 || cfg->distance_fn > 2) return SW_E_ARG;
+  // Kimura2 / JukesCantor (nucleic) need a per-call error report this entry point does not wait for
   if (cfg->distance_fn != SW_DIST_PERCENT_IDENTITY && cfg->alignment_type == SW_NUCLEIC) return SW_E_UNSUPPORTED;
   const float o = cfg->gap_open, e = cfg->gap_extension;
   if (!(o == o && e == e) || o != (float)(int)o || e != (float)(int)e) return SW_E_UNSUPPORTED;
@@ -116,8 +126,13 @@ extern "C" int sw_compute_block_static(const sw_config* cfg, const uint8_t* d_re
   if (tri && (rs != cs || re != ce)) return SW_E_ARG;
   if (ld_out < (int64_t)(ce - cs + 1)) return SW_E_ARG;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  int device = 0;
-  if (cudaGetDevice(&device) != cudaSuccess) return SW_E_CUDA;
+  const int device = cfg->device;
+  const DeviceScope scope(device);
+  if (!scope.ok) {
+    cudaGetLastError();
+    return SW_E_ARG;
+  }
+  if (!on_device(d_residues, device) || !on_device(d_offsets, device) || !on_device(d_out, device)) return SW_E_ARG;
   void* base = nullptr;
   int rc = scratch_address(device, &base);
   if (rc) return rc;
@@ -144,14 +159,29 @@ extern "C" int sw_compute_block_static(const sw_config* cfg, const uint8_t* d_re
       flags[a * 128 + b] = pad ? 0 : (uint8_t)f;
     }
 
-  // inputs: lengths and residues of the block's sequences
-  int ml_r = 0, ml_c = 0;
-  if ((rc = longest(d_offsets, rs, re, &ml_r, st)) || (rc = longest(d_offsets, cs, ce, &ml_c, st))) return rc;
-  const int maxlen = std::max(ml_r, ml_c);
+  // inputs: lengths and residues of the block's sequences, checked by one kernel whose status
+  // words come back in one small copy
+  unsigned char* p = static_cast<unsigned char*>(base);
+  int* d_status = reinterpret_cast<int*>(p + kStatusOffset);
+  int status[2] = {0, 0};
+  if (cudaMemsetAsync(d_status, 0, sizeof(status), st) != cudaSuccess) {
+    cudaGetLastError();
+    return SW_E_CUDA;
+  }
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  static_check_kernel<<<std::max(sms, 1) * 4, 256, 0, st>>>(d_residues, d_offsets, rs, re, cs, ce, d_status);
+  if (cudaGetLastError() != cudaSuccess ||
+      cudaMemcpyAsync(status, d_status, sizeof(status), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess) {
+    cudaGetLastError();
+    return SW_E_CUDA;
+  }
+  if (status[0] & kBadLength) return SW_E_ARG;
+  if (status[0] & kTooLong) return SW_E_UNSUPPORTED;
+  if (status[0] & kBadResidue) return SW_E_ARG;
+  const int maxlen = status[1];
   if ((double)(maxabs + (int)e) * 2.0 * maxlen + o >= 16777216.0) return SW_E_UNSUPPORTED;
-  if ((rc = residues_in_table(d_residues, d_offsets, rs, re, st)) ||
-      (rc = residues_in_table(d_residues, d_offsets, cs, ce, st)))
-    return rc;
 
   const long long R = re - rs + 1, C = ce - cs + 1;
   const long long npairs = tri ? R * (R - 1) / 2 : R * C;
@@ -161,12 +191,9 @@ extern "C" int sw_compute_block_static(const sw_config* cfg, const uint8_t* d_re
   const size_t per_thread = swg::plain_carry_bytes(cfg->mode == SW_MODE_NW ? swg::kModeNw : swg::kModeSwgMpi, 1, maxlen);
   long threads = (long)((kScratchBytes - kTableRegion) / per_thread) / kBlockThreads * kBlockThreads;
   if (threads < kBlockThreads) return SW_E_UNSUPPORTED;
-  int sms = 0;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   threads = std::min<long>(threads, (long)std::max(sms, 1) * 8 * kBlockThreads);
   threads = std::min<long>(threads, (long)((npairs + kBlockThreads - 1) / kBlockThreads) * kBlockThreads);
 
-  unsigned char* p = static_cast<unsigned char*>(base);
   if (cudaMemcpyAsync(p, scores, sizeof(scores), cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(p + sizeof(scores), flags, sizeof(flags), cudaMemcpyHostToDevice, st) != cudaSuccess) {
     cudaGetLastError();

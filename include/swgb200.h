@@ -191,17 +191,22 @@ int sw_query(sw_ctx* ctx, const char* key, int64_t* value);
 /* No counterpart in the reference: this entry point serves callers that cannot allocate device
  * memory (a host that gives all GPU memory to its own pool allocator, a plug-in whose process
  * has a fixed device-memory budget).  It aligns the pairs of one block like
- * sw_compute_block_device, with the same ranges, modes, orientation and mirror rule, but needs
- * no context: the configuration comes in cfg, the residues and offsets (sw_upload_sequences'
- * layout) and the output are the caller's device buffers, and the work is ordered on `stream`
- * (a cudaStream_t, NULL = the legacy default stream).  It calls no cudaMalloc or cudaFree: the
- * kernel's scratch is a 64 MiB array in the library's device image, present on every GPU that
- * loads the library until the process exits.  Sequences up to 16,383 residues: a longer one in the
- * block returns SW_E_UNSUPPORTED before anything is launched.  The first call
- * on a device looks up that array's address with the device current; make that first call before
- * any stream capture.  Calls share the array: calls whose kernels overlap on the GPU race and
- * must be ordered by the caller.  The call waits for its input checks (small copies of the
- * block's offsets and residues) and does not wait for the kernel. */
+ * sw_compute_block_device, with the same ranges, orientation and mirror rule, in all three
+ * modes, with PercentIdentity for nucleic input and PercentSimilarity for protein (nucleic
+ * Kimura2 / JukesCantor are SW_E_UNSUPPORTED here; distance_fn outside 0..2 is SW_E_ARG).  It
+ * needs no context: the configuration comes in cfg, the residues and offsets
+ * (sw_upload_sequences' layout: d_residues holds d_offsets[count] bytes) and the output are the
+ * caller's device buffers, and the work is ordered on `stream` (a cudaStream_t of cfg->device,
+ * NULL = the legacy default stream).  The call runs on cfg->device, made current for the call;
+ * the caller's current device is current again when it returns.  Buffers that are not
+ * cfg->device's memory are SW_E_ARG.  It calls no cudaMalloc or cudaFree: the kernels' scratch is
+ * a 64 MiB array in the library's device image, present on every GPU that loads the library
+ * until the process exits.  Sequences up to 16,383 residues: a longer one in the block returns
+ * SW_E_UNSUPPORTED before the alignment kernel is launched.  The first call on a device looks up
+ * that array's address with the device current; make that first call before any stream capture.
+ * Calls share the array: calls whose kernels overlap on the GPU race and must be ordered by the
+ * caller.  The call waits for its input check (one small kernel over the block's sequences and a
+ * copy of its two status words) and does not wait for the alignment kernel. */
 int sw_compute_block_static(const sw_config* cfg, const uint8_t* d_residues,
                             const int64_t* d_offsets, int32_t count, int32_t row_start,
                             int32_t row_end, int32_t col_start, int32_t col_end,
