@@ -41,8 +41,8 @@ P = C.c_void_p
 def build():
     """Compile liboracle.so (and oracle/_ref when the reference sources are present)."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
-    ref_src = Path(os.environ.get("SWG_REFERENCE_ROOT", "/root/reference")) / "SalsaTPL"
-    if ref_src.exists():
+    from . import cs2cpp  # the recipe owns where the reference sources are read from
+    if cs2cpp.DEFAULT_REF.exists():
         subprocess.run(["python3", str(HERE / "cs2cpp.py"), "--out", str(HERE / "_ref")],
                        check=True, stdout=subprocess.DEVNULL)
 
