@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <new>
 #include <string>
 #include <vector>
@@ -42,6 +43,8 @@ struct sw_ctx {
   cudaStream_t own_stream = nullptr;  // the context's stream while a caller's stream is in use
   int64_t last_pairs = 0, last_cells = 0;
   int* d_throws = nullptr;  // set by a SWG-MPI JukesCantor pair whose log argument is <= 0
+  int block_engine = 1;     // block handler: 1 engine for large blocks, 2 always, 0 plain kernel only
+  uint64_t letters[2] = {0, 0};  // residue bytes present in the uploaded set
   // serving (query batches against the uploaded sequences)
   swg::Server* server = nullptr;
   swg::ServeOptions serve_opt;
@@ -201,9 +204,12 @@ int sw_upload_sequences(sw_ctx* ctx, const uint8_t* concat, const int64_t* offse
     maxlen = std::max(maxlen, (int)len);
   }
   const int64_t total = offsets[count];
-  for (int64_t k = 0; k < total; k++)
+  uint64_t letters[2] = {0, 0};
+  for (int64_t k = 0; k < total; k++) {
     if (concat[k] >= 127)  // ScoringMatrix.Scores is [127,127]: the reference throws
       return fail(ctx, SW_E_ARG, "residue byte outside the 127-entry scoring table");
+    letters[concat[k] >> 6] |= 1ull << (concat[k] & 63);
+  }
   // The reference's float DP is exact while every value stays below 2^24.
   const double bound = (double)(ctx->max_abs_score + ctx->e) * 2.0 * maxlen + ctx->o;
   if (bound >= 16777216.0) return fail(ctx, SW_E_UNSUPPORTED, "scores could exceed float's exact range");
@@ -211,6 +217,21 @@ int sw_upload_sequences(sw_ctx* ctx, const uint8_t* concat, const int64_t* offse
   delete ctx->server;  // the database changes: jobs still running end with SW_E_STATE
   ctx->server = nullptr;
   cudaStreamSynchronize(ctx->stream);
+  // the same lengths and letters as the resident set: the engine's plans and graphs stay, only the
+  // residues (and the engine's codes of them) are replaced
+  if (ctx->d_seq && count == ctx->nseq && ctx->h_off.size() == (size_t)count + 1 &&
+      std::equal(offsets, offsets + count + 1, ctx->h_off.begin()) && letters[0] == ctx->letters[0] &&
+      letters[1] == ctx->letters[1]) {
+    if (total) CK(cudaMemcpyAsync(ctx->d_seq, concat, (size_t)total, cudaMemcpyHostToDevice, ctx->stream), "upload sequences");
+    if (ctx->engine) {
+      std::string msg;
+      const int rc = ctx->engine->refresh_codes(ctx->d_seq, total, ctx->stream, &msg);
+      if (rc) return fail(ctx, rc, msg);
+    }
+    CK(cudaStreamSynchronize(ctx->stream), "upload");
+    ctx->h_seq.assign(concat, concat + total);
+    return SW_OK;
+  }
   cudaFree(ctx->d_seq);
   cudaFree(ctx->d_off);
   ctx->d_seq = nullptr;
@@ -228,6 +249,8 @@ int sw_upload_sequences(sw_ctx* ctx, const uint8_t* concat, const int64_t* offse
   ctx->h_seq.assign(concat, concat + total);
   ctx->nseq = count;
   ctx->maxlen = maxlen;
+  ctx->letters[0] = letters[0];
+  ctx->letters[1] = letters[1];
   if (ctx->engine) ctx->engine->invalidate();
   return SW_OK;
 }
@@ -269,6 +292,57 @@ static int check_throws(sw_ctx* ctx) {
   return fail(ctx, SW_E_THROWS, "JukesCantor: the reference throws for Log(Zero) on a pair of this job");
 }
 
+static swg::EngineParams db_params(sw_ctx* ctx);
+
+// One engine job: the queries row_lo..row_hi of a `ranks`-rank run, or (block 1 / 2) the diagonal /
+// off-diagonal block of those rows by the columns col_lo..col_hi, with d_out pointing at the
+// block's element (0, 0).
+static int run_engine(sw_ctx* ctx, int32_t ranks, int row_lo, int row_hi, int16_t* d_out,
+                      int64_t ld, int64_t* pairs, int64_t* cells, int block = 0, int col_lo = 0,
+                      int col_hi = -1) {
+  if (!ctx->d_seq) return fail(ctx, SW_E_STATE, "no sequences uploaded");
+  if (!d_out || ranks < 1 || (!block && ld < ctx->nseq)) return fail(ctx, SW_E_ARG, "bad arguments");
+  cudaSetDevice(ctx->cfg.device);
+  if (!ctx->engine) {
+    ctx->engine = swg::Engine::create();
+    if (!ctx->engine) return fail(ctx, SW_E_OOM, "engine");
+  }
+  swg::EngineParams P;
+  P.seq = ctx->d_seq; P.off = ctx->d_off;
+  P.h_off = ctx->h_off.data(); P.h_seq = ctx->h_seq.data();
+  P.nseq = ctx->nseq; P.maxlen = ctx->maxlen;
+  P.scores = ctx->d_scores; P.flags = ctx->d_flags;
+  P.h_scores = &ctx->h_scores[0][0]; P.h_flags = &ctx->h_flags[0][0];
+  P.max_score = ctx->max_score; P.max_abs_score = ctx->max_abs_score;
+  P.o = ctx->o; P.e = ctx->e;
+  P.mode = ctx->cfg.mode;
+  P.protein = ctx->cfg.alignment_type == SW_PROTEIN;
+  P.lanes = ctx->cfg.lanes;
+  P.dist_fn = ctx->cfg.distance_fn;
+  P.throws = ctx->d_throws;
+  P.ranks = ranks;
+  P.row_lo = row_lo;
+  P.row_hi = row_hi;
+  P.block = block;
+  P.col_lo = col_lo;
+  P.col_hi = col_hi;
+  P.out = d_out; P.ld = ld;
+  if (block)  // the kernels index the output by global (s1, s2): shift the base to the block's corner
+    P.out = reinterpret_cast<int16_t*>(reinterpret_cast<intptr_t>(d_out) -
+                                       ((intptr_t)row_lo * ld + col_lo) * (intptr_t)sizeof(int16_t));
+  P.sms = ctx->sms;
+  P.stream = ctx->stream;
+  std::string msg;
+  int64_t np = 0, nc = 0;
+  int rc = ctx->engine->run(P, &np, &nc, &ctx->last_reruns, &msg);
+  if (rc) return fail(ctx, rc, msg);
+  ctx->last_pairs = np;
+  ctx->last_cells = nc;
+  if (pairs) *pairs = np;
+  if (cells) *cells = nc;
+  return SW_OK;
+}
+
 static int run_plain(sw_ctx* ctx, swg::PlainJob& J) {
   const int block = 128;
   long threads = (long)ctx->sms * 8 * block;
@@ -283,6 +357,24 @@ static int run_plain(sw_ctx* ctx, swg::PlainJob& J) {
   return SW_OK;
 }
 
+// The pairs of one block into device memory: the batched engine for blocks of at least
+// kBlockEngineMin pairs (option "block_engine" 1, the default; 2: every block; 0: never), else the
+// plain kernel (one thread per pair).
+constexpr int64_t kBlockEngineMin = 4096;
+
+static int block_device(sw_ctx* ctx, swg::PlainJob& J, int16_t* d_out, int64_t ld) {
+  const bool engine = ctx->block_engine == 2 || (ctx->block_engine == 1 && J.npairs >= kBlockEngineMin);
+  if (engine && J.npairs > 0) {
+    int64_t np = 0, nc = 0;
+    return run_engine(ctx, 1, J.rs, J.re, d_out, ld, &np, &nc, J.tri ? 1 : 2, J.cs, J.ce);
+  }
+  J.out = d_out;
+  J.ld = ld;
+  J.out_r0 = J.rs;
+  J.out_c0 = J.cs;
+  return run_plain(ctx, J);
+}
+
 int sw_compute_block_device(sw_ctx* ctx, int32_t rs, int32_t re, int32_t cs, int32_t ce,
                             int32_t diag, int16_t* d_out, int64_t ld, int64_t* pairs) {
   if (!ctx) return SW_E_ARG;
@@ -291,11 +383,7 @@ int sw_compute_block_device(sw_ctx* ctx, int32_t rs, int32_t re, int32_t cs, int
   swg::PlainJob J;
   int rc = block_job(ctx, rs, re, cs, ce, diag, &J);
   if (rc) return rc;
-  J.out = d_out;
-  J.ld = ld;
-  J.out_r0 = rs;
-  J.out_c0 = cs;
-  if ((rc = run_plain(ctx, J))) return rc;
+  if ((rc = block_device(ctx, J, d_out, ld))) return rc;
   if (pairs) *pairs = J.npairs;
   return SW_OK;
 }
@@ -315,15 +403,15 @@ int sw_compute_block(sw_ctx* ctx, int32_t rs, int32_t re, int32_t cs, int32_t ce
     return rc;
   }
   ctx->d_stage = static_cast<int16_t*>(stage);
-  // Start from the caller's values: the handler only writes the pairs it aligns.
-  CK(cudaMemcpy2DAsync(ctx->d_stage, Cc * 2, out, (size_t)ld * 2, Cc * 2, R, cudaMemcpyHostToDevice, ctx->stream), "stage block in");
-  J.out = ctx->d_stage;
-  J.ld = (long long)Cc;
-  J.out_r0 = rs;
-  J.out_c0 = cs;
-  if ((rc = run_plain(ctx, J))) return rc;
+  // Every entry of the block is written except the diagonal of a triangular block, which the
+  // handler leaves as the caller had it: keep those values and put them back after the copy.
+  std::vector<int16_t> keep;
+  if (J.tri)
+    for (size_t k = 0; k < R; k++) keep.push_back(out[k * (size_t)ld + k]);
+  if ((rc = block_device(ctx, J, ctx->d_stage, (int64_t)Cc))) return rc;
   CK(cudaMemcpy2DAsync(out, (size_t)ld * 2, ctx->d_stage, Cc * 2, Cc * 2, R, cudaMemcpyDeviceToHost, ctx->stream), "copy block out");
   CK(cudaStreamSynchronize(ctx->stream), "compute block");
+  for (size_t k = 0; k < keep.size(); k++) out[k * (size_t)ld + k] = keep[k];
   if (pairs) *pairs = J.npairs;
   return check_throws(ctx);
 }
@@ -428,47 +516,6 @@ int sw_last_rerun_count(const sw_ctx* ctx_, int64_t* count) {
   return rc ? fail(ctx, rc, msg) : SW_OK;
 }
 
-static swg::EngineParams db_params(sw_ctx* ctx);
-
-static int run_engine(sw_ctx* ctx, int32_t ranks, int row_lo, int row_hi, int16_t* d_out,
-                      int64_t ld, int64_t* pairs, int64_t* cells) {
-  if (!ctx->d_seq) return fail(ctx, SW_E_STATE, "no sequences uploaded");
-  if (!d_out || ld < ctx->nseq || ranks < 1) return fail(ctx, SW_E_ARG, "bad arguments");
-  cudaSetDevice(ctx->cfg.device);
-  if (!ctx->engine) {
-    ctx->engine = swg::Engine::create();
-    if (!ctx->engine) return fail(ctx, SW_E_OOM, "engine");
-  }
-  swg::EngineParams P;
-  P.seq = ctx->d_seq; P.off = ctx->d_off;
-  P.h_off = ctx->h_off.data(); P.h_seq = ctx->h_seq.data();
-  P.nseq = ctx->nseq; P.maxlen = ctx->maxlen;
-  P.scores = ctx->d_scores; P.flags = ctx->d_flags;
-  P.h_scores = &ctx->h_scores[0][0]; P.h_flags = &ctx->h_flags[0][0];
-  P.max_score = ctx->max_score; P.max_abs_score = ctx->max_abs_score;
-  P.o = ctx->o; P.e = ctx->e;
-  P.mode = ctx->cfg.mode;
-  P.protein = ctx->cfg.alignment_type == SW_PROTEIN;
-  P.lanes = ctx->cfg.lanes;
-  P.dist_fn = ctx->cfg.distance_fn;
-  P.throws = ctx->d_throws;
-  P.ranks = ranks;
-  P.row_lo = row_lo;
-  P.row_hi = row_hi;
-  P.out = d_out; P.ld = ld;
-  P.sms = ctx->sms;
-  P.stream = ctx->stream;
-  std::string msg;
-  int64_t np = 0, nc = 0;
-  int rc = ctx->engine->run(P, &np, &nc, &ctx->last_reruns, &msg);
-  if (rc) return fail(ctx, rc, msg);
-  ctx->last_pairs = np;
-  ctx->last_cells = nc;
-  if (pairs) *pairs = np;
-  if (cells) *cells = nc;
-  return SW_OK;
-}
-
 int sw_all_pairs_device(sw_ctx* ctx, int32_t ranks, int16_t* d_out, int64_t ld, int64_t* pairs,
                         int64_t* cells) {
   if (!ctx) return SW_E_ARG;
@@ -534,6 +581,11 @@ int sw_set_option(sw_ctx* ctx, const char* key, int64_t value) {
     cudaStreamSynchronize(ctx->stream);
     if (!ctx->own_stream) ctx->own_stream = ctx->stream;
     ctx->stream = value ? reinterpret_cast<cudaStream_t>(value) : ctx->own_stream;
+    return SW_OK;
+  }
+  if (k == "block_engine") {
+    if (value < 0 || value > 2) return fail(ctx, SW_E_ARG, "block_engine must be 0, 1 or 2");
+    ctx->block_engine = (int)value;
     return SW_OK;
   }
   if (k == "plan_only") {

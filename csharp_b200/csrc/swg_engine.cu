@@ -29,6 +29,7 @@
 #include <cstdio>
 #include <cstring>
 #include <numeric>
+#include <tuple>
 #include <type_traits>
 #include <vector>
 
@@ -71,6 +72,7 @@ struct EngineJob {
   const uint32_t* flagtab;  // [(A+1)*(A+1)] counted-column flags
   int A, o, e, bias, thresh;
   int mode, ranks, nseq, rb_a, rb_b;
+  int blk_mode, col_lo, col_hi;  // one block of the pair matrix: 1 diagonal, 2 off-diagonal (0: a job)
   int16_t* out;
   long long ld;
   uint32_t* scratch;        // per (CTA, warp) slot: maxcol * (kScrWords or kScrWordsNw) words
@@ -103,7 +105,10 @@ __device__ __forceinline__ int block_of(int x, int a, int b) {
 }
 
 __device__ __forceinline__ bool oriented(const EngineJob& J, int q, int d) {
-  if (J.qmode || J.mode == kModeSwgMs) return true;
+  if (J.qmode) return true;
+  if (J.blk_mode)  // the block's columns; a diagonal block of SWG-MPI / NW only below its diagonal
+    return d >= J.col_lo && d <= J.col_hi && (J.blk_mode == 2 || J.mode == kModeSwgMs || d < q);
+  if (J.mode == kModeSwgMs) return true;
   if (q == d) return false;
   const int bq = block_of(q, J.rb_a, J.rb_b), bd = block_of(d, J.rb_a, J.rb_b);
   if (bq == bd) return q > d;
@@ -855,6 +860,16 @@ size_t engine_smem(int A, int mpad, int maxcol, int K, int kind = 0) {
 
 __global__ void set_int_kernel(int* p, int v) { *p = v; }
 
+struct CodeLut {
+  uint8_t v[128];
+};
+
+// Dense codes of residue bytes (refresh_codes).
+__global__ void recode_kernel(const uint8_t* __restrict__ seq, uint8_t* __restrict__ code, int64_t n, CodeLut lut) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    code[k] = lut.v[seq[k] & 127];
+}
+
 // Calls fn(std::integral_constant<int, K>) for the engine instantiation of K rows per lane.
 template <class Fn>
 auto with_k(int K, Fn fn) {
@@ -991,6 +1006,7 @@ struct Base {
   size_t scratch_bytes = 0;
   void* d_carry = nullptr;
   long carry_threads = 0;
+  CodeLut lut;  // residue byte -> dense code of d_code
   // two-pass SW: the first pass's box records (pair, best score, best cell) with the threshold
   // codes of the rows above each best cell, the box step's band classes and the pairs it hands to
   // the warp box kernel, and the score kernels' per-warp row bounds
@@ -1023,6 +1039,7 @@ int build_base(Base& B, const EngineParams& P, std::string* msg) {
   const int64_t total = P.h_off[N];
   int code_of[128];
   std::fill(code_of, code_of + 128, -1);
+  // (the dense code of every byte, for refresh_codes: bytes of no letter map to the pad code)
   std::vector<int> letters;
   for (int64_t k = 0; k < total; k++) {
     const int b = P.h_seq[k];
@@ -1080,6 +1097,7 @@ int build_base(Base& B, const EngineParams& P, std::string* msg) {
       lettab[(size_t)a * A1 + c] = s + P.o;
       flagtab[(size_t)a * A1 + c] = f;
     }
+  for (int x = 0; x < 128; x++) B.lut.v[x] = (uint8_t)(code_of[x] < 0 ? A : code_of[x]);
   std::vector<uint8_t> code((size_t)total + 64, (uint8_t)A);
   for (int64_t k = 0; k < total; k++) code[(size_t)k] = (uint8_t)code_of[P.h_seq[k]];
   if ((rc = upload_vec(&B.d_code, code, msg, "codes"))) return rc;
@@ -1114,13 +1132,14 @@ struct Plan {
   }
 };
 
+// A job's pairs: the queries row_lo..row_hi with the orientation of a `ranks`-rank run (block 0),
+// or one block of the pair matrix, rows row_lo..row_hi by columns col_lo..col_hi (block 1: a
+// diagonal block, block 2: off-diagonal).
 struct PlanKey {
-  int mode, ranks, row_lo, row_hi;
+  int mode, ranks, row_lo, row_hi, block, col_lo, col_hi;
   bool operator<(const PlanKey& o) const {
-    if (mode != o.mode) return mode < o.mode;
-    if (ranks != o.ranks) return ranks < o.ranks;
-    if (row_lo != o.row_lo) return row_lo < o.row_lo;
-    return row_hi < o.row_hi;
+    return std::tie(mode, ranks, row_lo, row_hi, block, col_lo, col_hi) <
+           std::tie(o.mode, o.ranks, o.row_lo, o.row_hi, o.block, o.col_lo, o.col_hi);
   }
 };
 
@@ -1135,6 +1154,13 @@ bool oriented_host(int mode, const std::vector<int>& blk, int q, int d) {
 class EngineImpl : public Engine {
  public:
   ~EngineImpl() override { invalidate(); release_streams(); }
+  int refresh_codes(const uint8_t* d_seq, int64_t total, cudaStream_t st, std::string* msg) override {
+    if (!base_ || !base_->d_code || total <= 0) return SW_OK;
+    recode_kernel<<<(int)std::min<int64_t>((total + 255) / 256, 4096), 256, 0, st>>>(d_seq, base_->d_code, total, base_->lut);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { *msg = std::string("recode: ") + cudaGetErrorString(e); return SW_E_CUDA; }
+    return SW_OK;
+  }
   void invalidate() override {
     plans_.clear();
     base_.reset();
@@ -1203,7 +1229,7 @@ class EngineImpl : public Engine {
     P.ranks = 1;
     P.row_lo = N - R;
     P.row_hi = N - 1;
-    const PlanKey key{P.mode, 1, P.row_lo, P.row_hi};
+    const PlanKey key{P.mode, 1, P.row_lo, P.row_hi, 0, 0, -1};
     const int saved = opt_.k_override;
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
@@ -1286,7 +1312,8 @@ class EngineImpl : public Engine {
       if ((rc = build_base(*base_, P, msg))) { base_.reset(); return rc; }
     }
     const int N = P.nseq;
-    PlanKey key{P.mode, P.ranks, std::max(0, P.row_lo), P.row_hi < 0 ? N - 1 : std::min(N - 1, P.row_hi)};
+    PlanKey key{P.mode, P.ranks, std::max(0, P.row_lo), P.row_hi < 0 ? N - 1 : std::min(N - 1, P.row_hi),
+                P.block, P.block ? P.col_lo : 0, P.block ? P.col_hi : -1};
     auto it = plans_.find(key);
     if (it == plans_.end()) {
       std::unique_ptr<Plan> pl(new Plan());
@@ -1336,6 +1363,12 @@ class EngineImpl : public Engine {
     for (int r = 0; r < P.ranks; r++)
       for (int x = starts[r]; x <= ends[r]; x++) blk[x] = r;
     int rc;
+    // the pairs (s1 = q, s2 = d) of the job or block, and the columns d ranges over
+    auto allowed = [&](int q, int d) {
+      if (key.block) return d >= key.col_lo && d <= key.col_hi && (key.block == 2 || P.mode == kModeSwgMs || d < q);
+      return oriented_host(P.mode, blk, q, d);
+    };
+    const int dlo = key.block ? key.col_lo : 0, dhi = key.block ? key.col_hi : N - 1;
     const bool nw = P.mode == kModeNw;
     const bool kim = P.dist_fn != 0 && !P.protein;  // Kimura2 / JukesCantor: 32-bit lanes
     pl.plain_only = B.alpha > kMaxAlpha16 || (nw && !B.nw16) || kim || P.lanes == SW_LANES_32;
@@ -1354,8 +1387,8 @@ class EngineImpl : public Engine {
     std::vector<int2> big;
     if (pl.plain_only) {
       for (int q = key.row_lo; q <= key.row_hi; q++)
-        for (int d = 0; d < N; d++) {
-          if (!oriented_host(P.mode, blk, q, d)) continue;
+        for (int d = dlo; d <= dhi; d++) {
+          if (!allowed(q, d)) continue;
           big.push_back(make_int2(q, d));
           pl.ncells += (int64_t)B.len[q] * B.len[d];
         }
@@ -1403,7 +1436,10 @@ class EngineImpl : public Engine {
           cnt += (long)(b - a);
           lsum += csum[c][b] - csum[c][a];
         };
-        if (P.mode == kModeSwgMs) {
+        if (key.block) {
+          const bool below = key.block == 1 && P.mode != kModeSwgMs;
+          range_count(key.col_lo, below ? std::min(q, key.col_hi + 1) : key.col_hi + 1);
+        } else if (P.mode == kModeSwgMs) {
           range_count(0, N);
         } else {
           for (int r = 0; r < P.ranks; r++) {
@@ -1423,7 +1459,7 @@ class EngineImpl : public Engine {
           // 16-bit lanes cannot hold this item's scores: its pairs go to 32-bit lanes
           for (int k = c * chunk; k < std::min(N, (c + 1) * chunk); k++) {
             const int d = B.sorted_h[k];
-            if (oriented_host(P.mode, blk, q, d)) big.push_back(make_int2(q, d));
+            if (allowed(q, d)) big.push_back(make_int2(q, d));
           }
           continue;
         }
@@ -1534,7 +1570,7 @@ class EngineImpl : public Engine {
                       cudaEvent_t bins_t1 = nullptr) {
     Base& B = *base_;
     cudaError_t e;
-    pl.zeroes_diagonal = P.mode != kModeSwgMs && P.nseq > 0 && key.row_lo == 0 && key.row_hi == P.nseq - 1;
+    pl.zeroes_diagonal = !key.block && P.mode != kModeSwgMs && P.nseq > 0 && key.row_lo == 0 && key.row_hi == P.nseq - 1;
     if (pl.zeroes_diagonal)
       zero_diagonal_kernel<<<(P.nseq + 255) / 256, 256, 0, P.stream>>>(P.out, P.ld, P.nseq);
     set_int_kernel<<<1, 1, 0, P.stream>>>(pl.d_rerun_count, pl.big_count);
@@ -1550,6 +1586,7 @@ class EngineImpl : public Engine {
       J.A = B.alpha; J.o = P.o; J.e = P.e; J.bias = B.bias; J.thresh = pl.thresh;
       J.mode = P.mode; J.ranks = P.ranks; J.nseq = P.nseq; J.protein = P.protein;
       J.rb_a = P.nseq / P.ranks; J.rb_b = P.nseq % P.ranks;
+      J.blk_mode = key.block; J.col_lo = key.col_lo; J.col_hi = key.col_hi;
       J.out = P.out; J.ld = P.ld;
       J.scratch = B.d_scratch; J.maxcol = B.maxcol;
       J.rerun = pl.d_rerun; J.rerun_count = pl.d_rerun_count; J.rerun_cap = pl.rerun_cap;

@@ -24,6 +24,8 @@ struct EngineParams {
   int* throws = nullptr;   // device flag: SWG-MPI JukesCantor met log(0)
   int ranks;
   int row_lo = 0, row_hi = -1;  // queries (s1 indices) aligned; row_hi < 0: all
+  int block = 0;                // 1 / 2: only the diagonal / off-diagonal block of rows row_lo..row_hi
+  int col_lo = 0, col_hi = -1;  // and columns col_lo..col_hi (out points at element (0, 0))
   int16_t* out;
   long long ld;
   int sms;
@@ -49,6 +51,9 @@ class Engine {
   static Engine* create();
   virtual ~Engine() {}
   virtual void invalidate() = 0;
+  // The set's residues changed but not its lengths or letters: the plans and graphs stay valid;
+  // the dense residue codes are rebuilt on the device from d_seq (ordered on st).
+  virtual int refresh_codes(const uint8_t* d_seq, int64_t total, cudaStream_t st, std::string* msg) = 0;
   virtual EngineOptions& options() = 0;
   virtual void set_plan_only(int v) = 0;  // keeps the plans (options() drops them)
   // Returns an SW_* status.

@@ -91,7 +91,9 @@ const char* sw_version(void);
 
 /* Replaces the parsed FASTA list _sequences (Salsa.SmithWatermanMPI/Program.cs:94-95): the
  * sequences stay resident on the device for every later call.  concat holds all residues,
- * sequence k is concat[offsets[k] .. offsets[k+1]).  Lengths up to 32767. */
+ * sequence k is concat[offsets[k] .. offsets[k+1]).  Lengths up to 32767.  A set with the same
+ * lengths and the same residue letters as the resident one replaces its residues in place and keeps
+ * the engine's work plans and captured graphs (they depend on the lengths and letters only). */
 int sw_upload_sequences(sw_ctx* ctx, const uint8_t* concat, const int64_t* offsets, int32_t count);
 
 /* ---- the block handler (drop-in) ---------------------------------------------------------- */

@@ -52,10 +52,13 @@ def _golden_engine(cs, z, mode=0, lanes=0):
 
 
 @pytest.mark.parametrize("name", ["mpi_p1.npz", "mpi_p3.npz", "mpi_p4.npz", "protein_mpi.npz", "identity_mpi.npz"])
-def test_plain_block_kernel_matches_reference_block_driver(cs, name):
-    """One drop-in call per block of the reference's driver, mirrored like Scatter."""
+@pytest.mark.parametrize("block_engine", [0, 2])
+def test_block_handler_matches_reference_block_driver(cs, name, block_engine):
+    """One drop-in call per block of the reference's driver, mirrored like Scatter: the plain
+    per-block kernel (block_engine 0) and the batched engine (2) give the reference's values."""
     z = load_npz(name)
     eng = _golden_engine(cs, z)
+    eng.set_option("block_engine", block_engine)
     N, P = len(z["offsets"]) - 1, int(z["ranks"])
     rr = cs.range_partition(N, P)
     full = np.zeros((N, N), dtype=np.int16)
@@ -72,6 +75,7 @@ def test_plain_block_kernel_matches_reference_block_driver(cs, name):
                 full[b.StartIndex:b.EndIndex + 1, a.StartIndex:a.EndIndex + 1] = blk.T
     assert pairs == int(z["pairs"])
     np.testing.assert_array_equal(full, z["distances"])
+    eng.set_option("block_engine", 1)
 
 
 @pytest.mark.parametrize("name", ["mpi_p1.npz", "mpi_p3.npz", "mpi_p4.npz", "protein_mpi.npz", "identity_mpi.npz"])
@@ -84,13 +88,58 @@ def test_engine_matches_reference_driver(cs, name, lanes):
     np.testing.assert_array_equal(full, z["distances"])
 
 
-def test_block_handler_leaves_unaligned_entries_alone(cs):
+@pytest.mark.parametrize("block_engine", [0, 2])
+def test_block_handler_leaves_unaligned_entries_alone(cs, block_engine):
     z = load_npz("mpi_p1.npz")
     eng = _golden_engine(cs, z)
-    out = np.full((10, 10), 1234, dtype=np.int16)
-    eng.compute_block(3, 12, 3, 12, True, out=out)
-    assert (np.diag(out) == 1234).all()
-    np.testing.assert_array_equal(out[~np.eye(10, dtype=bool)], z["distances"][3:13, 3:13][~np.eye(10, dtype=bool)])
+    eng.set_option("block_engine", block_engine)
+    out = np.full((10, 14), 1234, dtype=np.int16)  # the block in a wider buffer (ld 14)
+    blk = out[:, :10]
+    eng.compute_block(3, 12, 3, 12, True, out=blk)
+    assert (np.diag(blk) == 1234).all()
+    assert (out[:, 10:] == 1234).all()
+    np.testing.assert_array_equal(blk[~np.eye(10, dtype=bool)], z["distances"][3:13, 3:13][~np.eye(10, dtype=bool)])
+    eng.set_option("block_engine", 1)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("matrix", ["EDNAFULL", "BLOSUM62"])
+def test_engine_block_handler_equals_plain_kernel(cs, mode, matrix):
+    """The block handler on the batched engine (large blocks) against the plain per-block kernel:
+    diagonal and off-diagonal blocks of an uneven set, host and device output, every mode."""
+    from csharp_b200 import synth
+    import torch
+    rng = np.random.default_rng(40 + mode)
+    N = 260
+    lens = synth.lognormal_lengths(N, 300, 0.6, 20, 900, rng)
+    if matrix == "BLOSUM62":
+        seqs = [s.tobytes() for s in synth.protein_family(N, 12, lens, 5, cs.ScoringMatrix.Load("BLOSUM62").Scores)]
+        o, e, atype = 10, 1, cs.PROTEIN
+    else:
+        seqs = [s.tobytes() for s in synth.dna_family(N, 20, lens, seed=6)]
+        o, e, atype = 16, 4, cs.NUCLEIC
+    m = cs.ScoringMatrix.Load(matrix)
+    plain = cs.Engine(m, o, e, mode=mode, alignment_type=atype).upload(seqs)
+    plain.set_option("block_engine", 0)
+    eng = cs.Engine(m, o, e, mode=mode, alignment_type=atype).upload(seqs)
+    for rs, re_, cs_, ce, diag in [(0, 129, 0, 129, True), (130, 259, 0, 129, False), (20, 200, 140, 259, False),
+                                   (130, 259, 130, 259, True)]:
+        want, n0 = plain.compute_block(rs, re_, cs_, ce, diag)
+        got, n1 = eng.compute_block(rs, re_, cs_, ce, diag)
+        assert n0 == n1
+        assert eng.query("launches") >= 3  # the engine ran, not the plain kernel
+        np.testing.assert_array_equal(got, want)
+        R, Cc = re_ - rs + 1, ce - cs_ + 1
+        d = torch.zeros((R, Cc + 3), dtype=torch.int16, device="cuda")
+        eng.compute_block_device(rs, re_, cs_, ce, diag, d.data_ptr(), Cc + 3)
+        eng.synchronize()
+        dd = d.cpu().numpy()
+        assert (dd[:, Cc:] == 0).all()
+        tri = diag and mode != 1
+        mask = ~np.eye(R, dtype=bool) if tri else np.ones((R, Cc), dtype=bool)
+        np.testing.assert_array_equal(dd[:, :Cc][mask], want[mask])
+    plain.close()
+    eng.close()
 
 
 @pytest.mark.parametrize("name,mode", [("nw_restated.npz", 2), ("ms_restated.npz", 1),
@@ -464,3 +513,28 @@ def test_register_box_step_on_uneven_lengths(cs, oracle_mod, o, e):
     pr = np.stack([ii, jj], 1).astype(np.int32)
     ref = _oracle_distances(oracle_mod, seqs, pr, "EDNAFULL", float(o), float(e))
     np.testing.assert_array_equal(res["reg"][pr[:, 0], pr[:, 1]], ref)
+
+
+def test_reupload_of_same_shaped_set_keeps_plans_and_uses_new_residues(cs):
+    """A second upload with the same lengths and letters keeps the engine's plans and graphs but
+    must align the new residues: every result equals a fresh engine's on the new set."""
+    from csharp_b200 import synth
+    rng = np.random.default_rng(12)
+    lens = synth.lognormal_lengths(300, 300, 0.6, 30, 900, rng)
+    a = [s.tobytes() for s in synth.dna_family(300, 30, lens, seed=1)]
+    b = [s.tobytes() for s in synth.dna_family(300, 30, lens, seed=2)]
+    m = cs.ScoringMatrix.Load("EDNAFULL")
+    eng = cs.Engine(m, 16, 4).upload(a)
+    got_a, _, _ = eng.all_pairs(3)
+    blk_a, _ = eng.compute_block(0, 149, 0, 149, True)
+    eng.upload(b)
+    got_b, _, _ = eng.all_pairs(3)
+    blk_b, _ = eng.compute_block(0, 149, 0, 149, True)
+    fresh = cs.Engine(m, 16, 4).upload(b)
+    want_b, _, _ = fresh.all_pairs(3)
+    np.testing.assert_array_equal(got_b, want_b)
+    off = ~np.eye(150, dtype=bool)
+    np.testing.assert_array_equal(blk_b[off], want_b[:150, :150][off])
+    assert not np.array_equal(got_a, got_b)
+    eng.close()
+    fresh.close()
