@@ -67,6 +67,8 @@ def lib():
         L.nwo_distance_i16.argtypes = [P, P, C.c_int, P, C.c_int, C.POINTER(C.c_int16)]
         L.swo_pairs.argtypes = [P, P, P, P, C.c_long, P, C.c_float, C.c_float, C.c_int, P, C.c_int]
         L.swo_pairs.restype = C.c_long
+        L.nwo_pairs.argtypes = [P, P, P, P, C.c_long, P, C.c_float, C.c_float, C.c_int, P, C.c_int]
+        L.nwo_pairs.restype = C.c_long
         _lib = L
     return _lib
 
@@ -204,6 +206,21 @@ def pairs(seqs, offsets, rows, cols, scores, o, e, alignment_type=ALN_NUCLEIC, t
     out = np.zeros(len(r), dtype=np.int16)
     bad = lib().swo_pairs(sq.ctypes.data, of.ctypes.data, r.ctypes.data, c.ctypes.data, len(r),
                           sc.ctypes.data, o, e, alignment_type, out.ctypes.data, threads or os.cpu_count())
+    if bad:
+        raise MemoryError
+    return out
+
+
+def nw_pairs(seqs, offsets, rows, cols, scores, o, e, protein=False, threads=None):
+    """NW distances of many pairs with the traceback restatement, OpenMP over host cores."""
+    sq = np.ascontiguousarray(seqs, dtype=np.uint8)
+    of = np.ascontiguousarray(offsets, dtype=np.int64)
+    r = np.ascontiguousarray(rows, dtype=np.int32)
+    c = np.ascontiguousarray(cols, dtype=np.int32)
+    sc = np.ascontiguousarray(scores, dtype=np.float32)
+    out = np.zeros(len(r), dtype=np.int16)
+    bad = lib().nwo_pairs(sq.ctypes.data, of.ctypes.data, r.ctypes.data, c.ctypes.data, len(r),
+                          sc.ctypes.data, o, e, int(protein), out.ctypes.data, threads or os.cpu_count())
     if bad:
         raise MemoryError
     return out

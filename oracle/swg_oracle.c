@@ -445,6 +445,31 @@ int nwo_distance_i16(const char* a, const char* b, int len, const float* scores,
   return 0;
 }
 
+/* NW distances of many pairs (s1 = sequence rows[k], s2 = cols[k]), OpenMP over host cores:
+ * nwo_align then nwo_distance_i16 per pair.  Returns the number of pairs that failed. */
+long nwo_pairs(const uint8_t* seqs, const int64_t* offsets, const int32_t* rows, const int32_t* cols,
+               long npairs, const float* scores, float o, float e, int protein, int16_t* out,
+               int threads) {
+  long bad = 0;
+#pragma omp parallel for schedule(dynamic, 8) num_threads(threads) reduction(+ : bad)
+  for (long k = 0; k < npairs; k++) {
+    const int i = rows[k], j = cols[k];
+    const int mi = (int)(offsets[i + 1] - offsets[i]), nj = (int)(offsets[j + 1] - offsets[j]);
+    char* a = (char*)malloc((size_t)(mi + nj) + 1);
+    char* b = (char*)malloc((size_t)(mi + nj) + 1);
+    float score;
+    int len = 0;
+    if (!a || !b || nwo_align(seqs + offsets[i], mi, seqs + offsets[j], nj, scores, o, e, &score, a, b, &len)) {
+      bad++;
+    } else {
+      nwo_distance_i16(a, b, len, scores, protein, &out[k]);
+    }
+    free(a);
+    free(b);
+  }
+  return bad;
+}
+
 /* ---- In-DP integer formulation (what the CUDA kernels compute) ---------------------------------
  * Row-major Gotoh over int32 scores with, per state X in {V, G(up), H(left)}, the counters of the
  * path that reaches X: identity, similarity, aligned columns, DP start cell.  G/H take the
