@@ -69,6 +69,10 @@ def lib():
         L.swo_pairs.restype = C.c_long
         L.nwo_pairs.argtypes = [P, P, P, P, C.c_long, P, C.c_float, C.c_float, C.c_int, P, C.c_int]
         L.nwo_pairs.restype = C.c_long
+        L.swo_indp_pairs.argtypes = [P, P, P, P, C.c_long, P, C.c_int, C.c_int, C.c_int, P, C.c_int]
+        L.swo_indp_pairs.restype = C.c_long
+        L.swo_count_pairs.argtypes = [P, P, P, P, C.c_long, P, C.c_int, C.c_int, C.c_int, P, C.c_int]
+        L.swo_count_pairs.restype = C.c_long
         _lib = L
     return _lib
 
@@ -206,6 +210,23 @@ def pairs(seqs, offsets, rows, cols, scores, o, e, alignment_type=ALN_NUCLEIC, t
     out = np.zeros(len(r), dtype=np.int16)
     bad = lib().swo_pairs(sq.ctypes.data, of.ctypes.data, r.ctypes.data, c.ctypes.data, len(r),
                           sc.ctypes.data, o, e, alignment_type, out.ctypes.data, threads or os.cpu_count())
+    if bad:
+        raise MemoryError
+    return out
+
+
+def indp_pairs(seqs, offsets, rows, cols, iscores, o, e, alignment_type=ALN_NUCLEIC, threads=None, fast=False):
+    """SWG-MPI distances of many pairs with the in-DP integer formulation, OpenMP over host
+    cores (integer scores and penalties); fast: one packed counter word per state."""
+    sq = np.ascontiguousarray(seqs, dtype=np.uint8)
+    of = np.ascontiguousarray(offsets, dtype=np.int64)
+    r = np.ascontiguousarray(rows, dtype=np.int32)
+    c = np.ascontiguousarray(cols, dtype=np.int32)
+    sc = np.ascontiguousarray(iscores, dtype=np.int32)
+    out = np.zeros(len(r), dtype=np.int16)
+    fn = lib().swo_count_pairs if fast else lib().swo_indp_pairs
+    bad = fn(sq.ctypes.data, of.ctypes.data, r.ctypes.data, c.ctypes.data, len(r), sc.ctypes.data, int(o), int(e),
+             alignment_type, out.ctypes.data, threads or os.cpu_count())
     if bad:
         raise MemoryError
     return out

@@ -563,3 +563,91 @@ long swo_pairs(const uint8_t* seqs, const int64_t* offsets, const int32_t* rows,
   }
   return bad;
 }
+
+/* SWG-MPI distances of many pairs with the in-DP integer formulation (pinned to the traceback
+ * restatement and to the reference's golden vectors by the tests), OpenMP over host cores: the
+ * fast checker for whole configurations.  Returns the number of pairs that failed. */
+long swo_indp_pairs(const uint8_t* seqs, const int64_t* offsets, const int32_t* rows, const int32_t* cols,
+                    long npairs, const int* iscores, int o, int e, int alignment_type, int16_t* out,
+                    int threads) {
+  long bad = 0;
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads) reduction(+ : bad)
+  for (long k = 0; k < npairs; k++) {
+    const int i = rows[k], j = cols[k];
+    const int mi = (int)(offsets[i + 1] - offsets[i]), nj = (int)(offsets[j + 1] - offsets[j]);
+    swo_result r;
+    if (swo_indp_align(seqs + offsets[i], mi, seqs + offsets[j], nj, iscores, o, e, &r)) {
+      bad++;
+      continue;
+    }
+    swo_distance_i16(&r, NULL, NULL, alignment_type, DF_PERCENT_IDENTITY, &out[k]);
+  }
+  return bad;
+}
+
+/* The same in-DP formulation with one counter word per state (aligned columns << 16 | counted
+ * columns, counted = identical for nucleic, identical or positive-scoring for protein: the columns
+ * ComputeDistance divides, SWG-MPI Program.cs:259-285), for checking whole configurations fast.
+ * Pinned to swo_indp_align and the traceback restatement by the tests. */
+long swo_count_pairs(const uint8_t* seqs, const int64_t* offsets, const int32_t* rows, const int32_t* cols,
+                     long npairs, const int* iscores, int o, int e, int alignment_type, int16_t* out,
+                     int threads) {
+  long bad = 0;
+  const int NEG = -(1 << 28);
+#pragma omp parallel for schedule(dynamic, 16) num_threads(threads) reduction(+ : bad)
+  for (long k = 0; k < npairs; k++) {
+    const uint8_t* s1 = seqs + offsets[rows[k]];
+    const uint8_t* s2 = seqs + offsets[cols[k]];
+    const int m = (int)(offsets[rows[k] + 1] - offsets[rows[k]]), n = (int)(offsets[cols[k] + 1] - offsets[cols[k]]);
+    int* V = (int*)malloc(sizeof(int) * (size_t)(n + 1));
+    int* G = (int*)malloc(sizeof(int) * (size_t)(n + 1));
+    uint32_t* CV = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(n + 1));
+    uint32_t* CG = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(n + 1));
+    if (!V || !G || !CV || !CG) {
+      bad++;
+      free(V); free(G); free(CV); free(CG);
+      continue;
+    }
+    for (int j = 0; j <= n; j++) { V[j] = 0; G[j] = NEG; CV[j] = CG[j] = 0u; }
+    int best = NEG;
+    uint32_t bc = 0u;
+    for (int i = 1; i <= m; i++) {
+      const int a = s1[i - 1];
+      const int* row = iscores + a * SWO_SIZE;
+      int vdiag = 0, vleft = 0, h = NEG;
+      uint32_t cdiag = 0u, cleft = 0u, ch = 0u;
+      for (int j = 1; j <= n; j++) {
+        const int b = s2[j - 1], sc = row[b];
+        const uint32_t fl = (a == b || (alignment_type == ALN_PROTEIN && sc > 0)) ? 1u : 0u;
+        const int f = vdiag + sc;
+        const uint32_t cf = cdiag + 0x10000u + fl;
+        /* selects written as masks: the data-dependent decisions do not branch */
+        const int g1 = G[j] - e, g2 = V[j] - o;
+        const uint32_t mg = 0u - (uint32_t)(g1 > g2);
+        const int g = (int)(((uint32_t)g1 & mg) | ((uint32_t)g2 & ~mg));
+        const uint32_t cg = ((CG[j] & mg) | (CV[j] & ~mg)) + 0x10000u;
+        const int h1 = h - e, h2 = vleft - o;
+        const uint32_t mh = 0u - (uint32_t)(h1 > h2);
+        h = (int)(((uint32_t)h1 & mh) | ((uint32_t)h2 & ~mh));
+        ch = ((ch & mh) | (cleft & ~mh)) + 0x10000u;
+        int v = f > g ? f : g;
+        v = v > h ? v : h;
+        v = v > 0 ? v : 0;
+        const uint32_t mf = 0u - (uint32_t)(v == f), mgv = 0u - (uint32_t)(v == g), mz = 0u - (uint32_t)(v != 0);
+        const uint32_t cv = ((cf & mf) | (((cg & mgv) | (ch & ~mgv)) & ~mf)) & mz;
+        vdiag = V[j]; cdiag = CV[j];
+        V[j] = v; G[j] = g; CV[j] = cv; CG[j] = cg;
+        vleft = v; cleft = cv;
+        if (v > best) { best = v; bc = cv; }
+      }
+    }
+    swo_result r;
+    memset(&r, 0, sizeof(r));
+    r.score = (m == 0 || n == 0) ? -INFINITY : (float)best;
+    r.identity = r.similarity = (int)(bc & 0xFFFFu);
+    r.length = (int)(bc >> 16);
+    swo_distance_i16(&r, NULL, NULL, alignment_type, DF_PERCENT_IDENTITY, &out[k]);
+    free(V); free(G); free(CV); free(CG);
+  }
+  return bad;
+}

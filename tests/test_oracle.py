@@ -130,3 +130,30 @@ def test_builtin_matrices_equal_reference_files(oracle_mod):
         np.testing.assert_array_equal(mine.astype(np.float32), ref, err_msg=name)
         parsed = ScoringMatrix.Parse(oracle_mod.matrix_text(name)).Scores[:127, :127]
         np.testing.assert_array_equal(parsed, mine, err_msg=name)
+
+
+def test_batched_integer_checkers_equal_traceback_restatement(kats, oracle_mod):
+    """The two batched in-DP checkers (cnt5 counters; one packed counter word) used for whole
+    configurations give the traceback restatement's distances: the KAT pairs, uneven DNA
+    families, tie-heavy {A, C} sequences and BLOSUM62 protein (exact Int16)."""
+    import csharp_b200 as cs
+    from csharp_b200 import synth
+    rng = np.random.default_rng(17)
+    kat = [k for k in kats if float(k["o"]).is_integer() and float(k["e"]).is_integer() and k["matrix"] != "IDENTITY"]
+    cases = []
+    for k in kat[:120]:
+        cases.append(([k["s1"].encode(), k["s2"].encode()], [(0, 1)], k["matrix"], int(k["o"]), int(k["e"]), k["alignment_type"]))
+    dna = [s.tobytes() for s in synth.dna_family(60, 6, synth.lognormal_lengths(60, 200, 0.6, 1, 600, rng), seed=3)]
+    cases.append((dna, [(i, j) for i in range(60) for j in range(i)][::3], "EDNAFULL", 16, 4, 1))
+    ac = [bytes(rng.choice([65, 67], int(rng.integers(1, 50))).astype(np.uint8)) for _ in range(50)]
+    cases.append((ac, [(i, j) for i in range(50) for j in range(50) if i != j][::4], "EDNAFULL", 4, 2, 1))
+    prot = [s.tobytes() for s in synth.protein_family(40, 5, rng.integers(20, 200, 40), 9, cs.ScoringMatrix.Load("BLOSUM62").Scores)]
+    cases.append((prot, [(i, j) for i in range(40) for j in range(40) if i != j][::3], "BLOSUM62", 10, 1, 0))
+    for seqs, pairs, matrix, o, e, atype in cases:
+        concat, off = cs.pack_sequences(seqs)
+        r = np.array([p[0] for p in pairs]); c = np.array([p[1] for p in pairs])
+        m = cs.ScoringMatrix.Load(matrix).Scores[:127, :127]
+        want = oracle_mod.pairs(concat, off, r, c, m.astype(np.float32), float(o), float(e), alignment_type=atype)
+        for fast in (False, True):
+            got = oracle_mod.indp_pairs(concat, off, r, c, m.astype(np.int32), o, e, alignment_type=atype, fast=fast)
+            np.testing.assert_array_equal(got, want)
