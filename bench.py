@@ -9,12 +9,20 @@ whole job once on one GPU.  With N GPUs (torchrun) each rank takes a different s
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Besides the headline value (inputs resident in HBM), the line carries: e2e (the same job driven
-through host buffers, copies inside the timed region), the integer-pipe roofline of the engine
-kernels (peak measured live by a calibration kernel), a CPU baseline (the reference's own
-aligner and ComputeDistance, transliterated from its C# and run on the host cores), a parity
-spot check of that sample against the GPU matrix, the plain one-launch-per-block kernel versus
-the batched engine on the same 2,000-sequence block, and the SM clocks sampled while timing.
+Besides the headline value (inputs resident in HBM, one engine call per share), the line carries:
+  e2e              the same shares through the reference-facing C ABI with host buffers: per step
+                   sw_upload_sequences from pinned memory, then one sw_compute_block call per block
+                   of the share in the reference driver's order, each copying its block to the host
+  roofline         the engine kernels' cell rate against the integer-pipe peak measured live
+  cpu_baseline     the reference's own aligner and ComputeDistance (transliterated from its C#)
+                   on the host cores, over a uniform sample of the job's pairs, with its parity
+  plain_vs_batched one 8-rank share block by block: the plain one-thread-per-pair kernel against
+                   the engine behind the same block handler, identical results required
+  configs          configurations 1, 2 and 4 on the engine, each checked against the oracle
+                   (cfg1 every pair, cfg2 and cfg4 uniform samples) by CPU workers that run while
+                   the GPU legs run
+  serving          configuration 5: Poisson query batches against a 100,000-sequence database
+  clocks           the SM clocks sampled while timing
 """
 import argparse
 import json
@@ -35,7 +43,8 @@ WORKLOAD = dict(n=20000, median=400, sigma=0.6, lo=50, hi=1500, roots=200, seed=
 OPS_PER_CELL = 11      # algorithmic integer ops of one SW-Gotoh cell (E, F, H, running best)
 LANES_PER_OP = 2       # the engine's score registers hold two 16-bit lanes
 SHARES = 8             # steps per whole job: the shares of an 8-rank run
-SERVE = dict(db=100000, qmin=1, qmax=512, load=0.7, seconds=40.0, seed=6)
+SERVE = dict(db=100000, qmin=1, qmax=512, load=0.7, jobs=100, seed=6)
+PARITY_SAMPLE = 100000  # pairs of configurations 2 and 4 checked against the oracle
 ENGINE_OPTIONS = {}    # engine knobs from the command line (sw_set_option), applied to every engine
 
 
@@ -53,17 +62,44 @@ def workload_sequences(n):
     return pack_sequences(seqs)
 
 
+# ---- the reference driver's partition (RangePartitioner.cs:17-55, Program.cs:628-642), in Python
+# so that the reference arm loads nothing of this repository's library
+def ranges(n, parts):
+    """Inclusive (start, end) of each part: the first n % parts parts get one more element."""
+    q, r = divmod(n, parts)
+    out, s = [], 0
+    for k in range(parts):
+        ln = q + (1 if k < r else 0)
+        out.append((s, s + ln - 1))
+        s += ln
+    return out
+
+
+def block_computed(r, c):
+    """Rank r computes block (r, c) (the SWG-MPI checkerboard)."""
+    return (r > c and (r + c) % 2 == 0) or (r < c and (r + c) % 2 == 1)
+
+
+def share_blocks(n, share, parts=SHARES):
+    """The blocks rank `share` of a `parts`-rank run hands to its block handler, in the order
+    MPIComputeLowerTriangularBlocked.Compute calls it: (row start, row end, col start, col end,
+    diagonal)."""
+    rr = ranges(n, parts)
+    rs, re_ = rr[share]
+    return [(rs, re_, cs, ce, c == share) for c, (cs, ce) in enumerate(rr)
+            if c == share or block_computed(share, c)]
+
+
 def sample_pairs(n, count, rng):
     """`count` pairs drawn uniformly from the job, oriented (s1, s2) as the SHARES-rank run
     orients them: diagonal blocks align (s_i, s_j) for i > j; block (r, c) is aligned by the rank
     the checkerboard names, with s1 from its rows."""
-    from csharp_b200 import block_is_computed, range_partition
     ii = rng.integers(1, n, count)
     jj = (rng.random(count) * ii).astype(np.int64)
     blk = np.zeros(n, dtype=np.int64)
-    for r, x in enumerate(range_partition(n, SHARES)):
-        blk[x.StartIndex:x.EndIndex + 1] = r
-    flip = np.array([bi != bj and not block_is_computed(bi, bj) for bi, bj in zip(blk[ii], blk[jj])], dtype=bool)
+    for r, (a, b) in enumerate(ranges(n, SHARES)):
+        blk[a:b + 1] = r
+    flip = np.array([bi != bj and not block_computed(bi, bj) for bi, bj in zip(blk[ii], blk[jj])], dtype=bool)
     return np.where(flip, jj, ii), np.where(flip, ii, jj), blk
 
 
@@ -110,6 +146,7 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+# ---- CPU legs (spawned worker processes; the oracle is the checker and the timed CPU reference) --
 def _cpu_worker(args):
     concat, off, rows, cols = args
     import oracle
@@ -135,6 +172,51 @@ def reference_available():
     return oracle.ref_available()
 
 
+_PARITY_SETS = {}
+
+
+def _parity_init(sets):
+    _PARITY_SETS.update(sets)
+
+
+def _parity_task(args):
+    """One chunk of a parity check: (set name, checker, pairs) -> the oracle's distances."""
+    name, kind, rows, cols = args
+    import oracle
+    concat, off, scores, o, e, atype = _PARITY_SETS[name]
+    if kind == "count":    # the in-DP integer checker, one counter word (pinned by the tests)
+        return oracle.indp_pairs(concat, off, rows, cols, scores.astype(np.int32), o, e, atype, threads=1, fast=True)
+    if kind == "nw":       # the NW traceback restatement
+        return oracle.nw_pairs(concat, off, rows, cols, scores.astype(np.float32), float(o), float(e),
+                               protein=atype == 0, threads=1)
+    return oracle.ref_distances("BLOSUM62" if atype == 0 else "EDNAFULL", atype, 0, float(o), float(e),
+                                concat, off, rows, cols)  # the transliterated reference
+
+
+class Parity:
+    """Oracle checks of whole configurations on the host cores, in spawned workers that run while
+    the GPU legs run.  submit(name, kind, rows, cols) queues one check; result(name) waits."""
+
+    def __init__(self, sets, workers):
+        import multiprocessing as mp
+        self.pool = mp.get_context("spawn").Pool(max(1, workers), initializer=_parity_init, initargs=(sets,))
+        self.jobs = {}
+        self.t0 = time.perf_counter()
+
+    def submit(self, name, kind, rows, cols, chunk=1500):
+        idx = np.array_split(np.arange(len(rows)), max(1, len(rows) // chunk))
+        self.jobs[name] = (kind, self.pool.map_async(_parity_task, [(name, kind, rows[c], cols[c]) for c in idx if len(c)]))
+
+    def result(self, name):
+        kind, r = self.jobs[name]
+        return kind, np.concatenate(r.get())
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+        return time.perf_counter() - self.t0
+
+
 def run_reference_arm(a):
     """--impl reference: the reference's CPU path on this host's cores, same metric/workload."""
     rank = int(os.environ.get("RANK", "0"))
@@ -153,7 +235,7 @@ def run_reference_arm(a):
             _, dt = cpu_reference(concat, off, r, c, threads)
         else:
             import oracle
-            from csharp_b200 import ScoringMatrix
+            from csharp_b200 import ScoringMatrix  # only without the transliterated reference
             sc = ScoringMatrix.Load("EDNAFULL").Scores[:127, :127].astype(np.float32)
             t = time.perf_counter()
             oracle.pairs(concat, off, r, c, sc, 16.0, 4.0, threads=threads)
@@ -175,19 +257,20 @@ def run_reference_arm(a):
     return 0
 
 
-def serving(cs, device, seconds, load):
+# ---- GPU legs -----------------------------------------------------------------------------------
+def serving(cs, device, jobs, load):
     """Serving workload: a device-resident database of 100,000 DNA sequences (lognormal median
-    500, sigma 0.6, clipped 50-2,000), a Poisson stream of query batches (sizes log-uniform in
-    1-512, query lengths from the same distribution) aligned SW-Gotoh against the whole database.
-    The arrival rate is set from a calibration job so that the offered load is `load` of the GPU.
-    Latency of a job = its completion (results in host memory) minus its submission."""
+    500, sigma 0.6, clipped 50-2,000), a Poisson stream of `jobs` query batches (sizes log-uniform
+    in 1-512, query lengths from the same distribution) aligned SW-Gotoh against the whole
+    database.  The arrival rate is set from a calibration job so that the offered load is `load`
+    of the GPU.  Latency of a job = its completion (results in host memory) minus its submission."""
     from csharp_b200 import pack_sequences, synth
     db = synth.config5_db(SERVE["db"])
     concat, off = pack_sequences(db)
     dblen = float(off[-1])
     rng = np.random.default_rng(SERVE["seed"])
     pool = synth.dna_family(4000, 40, synth.lognormal_lengths(4000, 500, 0.6, 50, 2000, rng), SERVE["seed"])
-    eng = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4, device=device)
+    eng = with_options(cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4, device=device))
     eng.upload(concat=concat, offsets=off)
     # calibration (also builds the database state): 64 queries alone
     cal = [pool[k].tobytes() for k in range(64)]
@@ -196,9 +279,8 @@ def serving(cs, device, seconds, load):
     mean_q = (SERVE["qmax"] - SERVE["qmin"]) / np.log(SERVE["qmax"] / SERVE["qmin"])
     mean_cells = mean_q * float(np.mean([len(p) for p in pool])) * dblen
     lam = load * cal_rate / mean_cells           # batches per second
-    arrivals = np.cumsum(rng.exponential(1.0 / lam, 10000))
-    arrivals = arrivals[arrivals < seconds]
-    sizes = np.exp(rng.uniform(np.log(SERVE["qmin"]), np.log(SERVE["qmax"] + 1), len(arrivals))).astype(int)
+    arrivals = np.cumsum(rng.exponential(1.0 / lam, jobs))
+    sizes = np.exp(rng.uniform(np.log(SERVE["qmin"]), np.log(SERVE["qmax"] + 1), jobs)).astype(int)
     sizes = np.clip(sizes, SERVE["qmin"], SERVE["qmax"])
     batches = [[pool[k].tobytes() for k in rng.integers(0, len(pool), n)] for n in sizes]
     outstanding, results = {}, []
@@ -226,69 +308,84 @@ def serving(cs, device, seconds, load):
     return {"workload": "cfg5 serving: 100,000 DNA database lognormal(median 500, sigma 0.6) clipped 50-2000, "
                         "Poisson batches of 1-512 queries (log-uniform sizes), EDNAFULL, open 16 / extend 4",
             "jobs": len(results), "queries": int(sizes.sum()), "offered_load": load,
-            "arrival_rate_per_s": round(lam, 3), "p50_ms": round(float(np.percentile(lat, 50)), 1),
-            "p99_ms": round(float(np.percentile(lat, 99)), 1), "mean_ms": round(float(lat.mean()), 1),
-            "gcups": round(cells / span / 1e9, 1), "calibration_gcups": round(cal_rate / 1e9, 1),
-            "max_admitted": st["max_active"], "waves": st["waves"], "all_ok": ok}
+            "arrival_rate_per_s": round(lam, 3), "span_s": round(span, 1),
+            "p50_ms": round(float(np.percentile(lat, 50)), 1), "p99_ms": round(float(np.percentile(lat, 99)), 1),
+            "mean_ms": round(float(lat.mean()), 1), "gcups": round(cells / span / 1e9, 1),
+            "calibration_gcups": round(cal_rate / 1e9, 1), "max_admitted": st["max_active"], "waves": st["waves"],
+            "all_ok": ok}
 
 
-def other_configs(cs, device, stream, flush):
-    """The other benchmark configurations, each timed with inputs resident (CUDA events, L2
-    flushed): the 16-bit engine on the whole job and, on a subset, the same pairs on 32-bit
-    lanes (results compared entry by entry; parity with the reference is the tests' job)."""
+def _timed(stream, fn):
+    """fn() between two CUDA events on `stream`, waited for; returns milliseconds."""
     import torch
-    from csharp_b200 import pack_sequences, synth
-    out = {}
-    specs = [
+    b, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    b.record(stream)
+    fn()
+    e.record(stream)
+    torch.cuda.synchronize()
+    return b.elapsed_time(e)
+
+
+def config_sets(cs):
+    """Configurations 1, 2 and 4: (name, description, sequences, matrix, open, extend, mode, type)."""
+    from csharp_b200 import synth
+    bl = cs.ScoringMatrix.Load("BLOSUM62").Scores
+    return [
         ("cfg1", "plain SW-Gotoh: 1,000 DNA, 20 roots of 500 nt, lengths 200-600, EDNAFULL 16/4",
-         lambda: synth.config1(), "EDNAFULL", 16, 4, cs.SWG_MPI, cs.NUCLEIC, 1000),
+         synth.config1(), "EDNAFULL", 16, 4, cs.SWG_MPI, cs.NUCLEIC),
         ("cfg2", "NW global: 10,000 DNA, lengths uniform 300-500, 100 roots, EDNAFULL 16/4",
-         lambda: synth.config2(), "EDNAFULL", 16, 4, cs.NW, cs.NUCLEIC, 1500),
-        ("cfg4", "protein SW-Gotoh: 5,000 of the 20,000-sequence set (20 amino acids, lengths 100-1000, "
-                 "500 roots), BLOSUM62 10/1",
-         lambda: synth.config4(cs.ScoringMatrix.Load("BLOSUM62").Scores, n=5000), "BLOSUM62", 10, 1,
-         cs.SWG_MPI, cs.PROTEIN, 1000),
+         synth.config2(), "EDNAFULL", 16, 4, cs.NW, cs.NUCLEIC),
+        ("cfg4", "protein SW-Gotoh: 20,000 sequences (20 amino acids, lengths 100-1000, 500 roots), BLOSUM62 10/1",
+         synth.config4(bl), "BLOSUM62", 10, 1, cs.SWG_MPI, cs.PROTEIN),
     ]
 
-    def timed(eng, n, dst):
-        eng.all_pairs_device(dst.data_ptr(), n, 1)
-        torch.cuda.synchronize()
-        flush.zero_()
-        b, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        b.record(stream)
-        eng.all_pairs_device(dst.data_ptr(), n, 1)
-        e.record(stream)
-        torch.cuda.synchronize()
-        return b.elapsed_time(e), eng.query("cells")
 
-    for name, desc, gen, matrix, o, e, mode, atype, sub in specs:
-        seqs = gen()
-        concat, off = pack_sequences(seqs)
+def config_parity_pairs(n, name, rng):
+    """The pairs a configuration's check covers: every pair of cfg1, a uniform sample of the others
+    (s1 = the larger index, as a 1-rank run orients them)."""
+    if name == "cfg1":
+        ii, jj = np.tril_indices(n, -1)
+        return ii.astype(np.int64), jj.astype(np.int64)
+    ii = rng.integers(1, n, PARITY_SAMPLE)
+    jj = (rng.random(PARITY_SAMPLE) * ii).astype(np.int64)
+    return ii, jj
+
+
+def run_configs(cs, device, stream, flush, sets, picks, parity):
+    """Each configuration as one whole-job engine call (inputs resident, planned before timing),
+    and the oracle's verdict on its checked pairs."""
+    import torch
+    out, got = {}, {}
+    for name, desc, seqs, matrix, o, e, mode, atype in sets:
+        concat, off = cs.pack_sequences(seqs)
         n = len(seqs)
         eng = with_options(cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=mode, alignment_type=atype, device=device))
         eng.upload(concat=concat, offsets=off)
         eng.use_stream(stream.cuda_stream)
         full = torch.zeros((n, n), dtype=torch.int16, device="cuda")
-        ms, cells = timed(eng, n, full)
-        m = min(sub, n)
-        a16 = with_options(cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=mode, alignment_type=atype, device=device))
-        a32 = with_options(cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=mode, alignment_type=atype, device=device,
-                                     lanes=32))
-        r = {}
-        for tag, x in (("lanes16", a16), ("lanes32", a32)):
-            x.upload(concat=concat[: off[m]], offsets=off[: m + 1])
-            x.use_stream(stream.cuda_stream)
-            d = torch.zeros((m, m), dtype=torch.int16, device="cuda")
-            t, c = timed(x, m, d)
-            r[tag] = (t, c, d)
-        out[name] = {"workload": desc, "gcups": round(cells / (ms * 1e-3) / 1e9, 1), "ms": round(ms, 1),
-                     "cells": int(cells), "pairs": n * (n - 1) // 2,
-                     "subset": f"first {m} sequences: 16-bit lanes {r['lanes16'][1] / (r['lanes16'][0] * 1e-3) / 1e9:.1f}"
-                               f" vs 32-bit lanes {r['lanes32'][1] / (r['lanes32'][0] * 1e-3) / 1e9:.1f} GCUPS",
-                     "subset_identical": bool(torch.equal(r["lanes16"][2], r["lanes32"][2]))}
-        for x in (eng, a16, a32):
-            x.close()
+        t = time.perf_counter()
+        eng.set_option("plan_only", 1)
+        eng.all_pairs_device(full.data_ptr(), n, 1)
+        eng.set_option("plan_only", 0)
+        plan_s = time.perf_counter() - t
+        flush.zero_()
+        ms = _timed(stream, lambda: eng.all_pairs_device(full.data_ptr(), n, 1))
+        cells = eng.query("cells")
+        ii, jj = picks[name]
+        gi, gj = torch.from_numpy(ii).cuda(), torch.from_numpy(jj).cuda()
+        got[name] = full[gi, gj].cpu().numpy()
+        eng.close()
         del full
+        out[name] = {"workload": desc, "gcups": round(cells / (ms * 1e-3) / 1e9, 1), "ms": round(ms, 1),
+                     "cells": int(cells), "pairs": n * (n - 1) // 2, "plan_s": round(plan_s, 2)}
+    for name in got:  # the CPU checks were running meanwhile
+        kind, want = parity.result(name)
+        out[name]["parity"] = {"pairs_checked": int(len(want)), "mismatches": int((got[name] != want).sum()),
+                               "checker": {"count": "oracle in-DP integer restatement (every pair)",
+                                           "nw": "oracle NW traceback restatement (uniform sample)",
+                                           "ref": "transliterated reference oracle/_ref (uniform sample)"}[kind],
+                               "tolerance": "exact Int16"}
     return out
 
 
@@ -306,26 +403,32 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="built-in rows-per-lane costs instead of measured ones")
     ap.add_argument("--serving-only", action="store_true", help="only the serving workload (one JSON line)")
     ap.add_argument("--configs-only", action="store_true", help="only configurations 1, 2 and 4 (one JSON line)")
-    ap.add_argument("--serve-seconds", type=float, default=SERVE["seconds"])
+    ap.add_argument("--serve-jobs", type=int, default=SERVE["jobs"])
     ap.add_argument("--box-reg", type=int, default=-1, choices=[-1, 0, 1],
                     help="two-pass box step: 1 register box step first, 0 warp box kernel only (-1: engine default)")
     a = ap.parse_args()
     if a.box_reg >= 0:
         ENGINE_OPTIONS["box_reg"] = a.box_reg
+    if a.impl == "reference":
+        return run_reference_arm(a)
+    threads = os.cpu_count() or 1
     if a.serving_only:
         import csharp_b200 as cs
-        print(json.dumps({"serving": serving(cs, 0, a.serve_seconds, SERVE["load"])}))
+        print(json.dumps({"serving": serving(cs, 0, a.serve_jobs, SERVE["load"])}))
         return 0
     if a.configs_only:
         import torch
         import csharp_b200 as cs
+        sets = config_sets(cs)
+        picks = {s[0]: config_parity_pairs(len(s[2]), s[0], np.random.default_rng(21)) for s in sets}
+        parity = start_parity(cs, sets, picks, threads)
         st = torch.cuda.Stream()
         torch.cuda.set_stream(st)
         fl = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-        print(json.dumps({"configs": other_configs(cs, 0, st, fl)}))
+        res = run_configs(cs, 0, st, fl, sets, picks, parity)
+        parity.close()
+        print(json.dumps({"configs": res}))
         return 0
-    if a.impl == "reference":
-        return run_reference_arm(a)
 
     import torch
     import torch.distributed as dist
@@ -356,11 +459,13 @@ def main():
     # the autotuner times each rows-per-lane choice on a sample of this job (before any timing)
     tuned = None if (a.no_autotune or a.rows_per_lane) else eng.autotune(out.data_ptr(), N)
     share_cells = {}
+    t_plan = time.perf_counter()
     eng.set_option("plan_only", 1)  # plan and capture every share before timing; launch nothing
     for s in range(SHARES):
         eng.rank_blocks_device(s, SHARES, out.data_ptr(), N)
         share_cells[s] = eng.query("cells")
     eng.set_option("plan_only", 0)
+    plan_s = time.perf_counter() - t_plan
     torch.cuda.synchronize()
 
     for w in range(a.warmup):
@@ -408,6 +513,7 @@ def main():
                          "step": f"one rank's share of an {SHARES}-rank MPI run of the job (whole job = {SHARES} steps)",
                          "l2": "flushed (256 MB write) before every timed step",
                          "cells_per_job": int(sum(share_cells.values())), "pairs_per_job": N * (N - 1) // 2,
+                         "plan_s": round(plan_s, 2),
                          "engine_options": dict(ENGINE_OPTIONS) or "defaults",
                          "rows_per_lane_costs": (tuned if tuned and any(tuned.values()) else
                                                  "built-in" + (" (kept by the autotuner)" if tuned else ""))},
@@ -426,88 +532,8 @@ def main():
                               "peak_basis": f"measured max.s32 {peak_max / 1e12:.2f} Tops/s x {LANES_PER_OP} lanes / {OPS_PER_CELL} ops per cell",
                               "kernel_ms": round(kernel_ms, 2)}
     if not a.skip_extras and rank == 0:
-        # e2e: the same shares through host buffers: H2D of the sequences, D2H of the matrix
-        pin_seq = torch.from_numpy(concat).pin_memory()
-        pin_out = torch.empty((N, N), dtype=torch.int16).pin_memory()
-        d_seq = torch.empty_like(pin_seq, device="cuda")
-        e_cells, e_ms = 0, 0.0
-        for k in range(3):
-            s = share_of(k)
-            b, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize()
-            b.record(stream)
-            d_seq.copy_(pin_seq, non_blocking=True)
-            eng.rank_blocks_device(s, SHARES, out.data_ptr(), N)
-            pin_out.copy_(out, non_blocking=True)
-            e.record(stream)
-            torch.cuda.synchronize()
-            if k >= 1:
-                e_ms += b.elapsed_time(e)
-                e_cells += share_cells[s]
-        result["e2e"] = {"value": round(e_cells / (e_ms * 1e-3) / 1e9, 3), "unit": "GCUPS",
-                         "h2d_bytes_per_step": int(concat.nbytes), "d2h_bytes_per_step": int(N * N * 2),
-                         "note": "per step: sequences H2D from pinned host, one rank share, full Int16 matrix D2H"}
-        # the shares of all steps so far cover the whole job: the matrix of an 8-rank run
-        torch.cuda.synchronize()
-        full = pin_out.numpy().copy()
-        covered = {share_of(k) for k in range(a.warmup + a.steps)} | {share_of(k) for k in range(3)}
-        # CPU baseline: the reference's aligner on a uniform sample of the job's pairs, oriented
-        # as the 8-rank run orients them (s1 = the row of the share that aligns the pair)
-        threads = os.cpu_count() or 1
-        ii, jj, blk = sample_pairs(N, 200000, np.random.default_rng(5))
-        keep = np.isin(blk[ii], list(covered))
-        ii, jj = ii[keep], jj[keep]
-        per_pair = float(np.mean(lens[ii] * lens[jj]))
-        npairs = int(max(threads * 4, min(len(ii), a.cpu_seconds * threads * 0.12e9 / per_pair)))
-        ii, jj = ii[:npairs], jj[:npairs]
-        kind = "reference" if reference_available() else "port"
-        if kind == "reference":
-            d_cpu, dt = cpu_reference(concat, off, ii, jj, threads)
-        else:
-            import oracle
-            sc = cs.ScoringMatrix.Load("EDNAFULL").Scores[:127, :127].astype(np.float32)
-            t = time.perf_counter()
-            d_cpu = oracle.pairs(concat, off, ii, jj, sc, 16.0, 4.0, threads=threads)
-            dt = time.perf_counter() - t
-        cpu_cells = float((lens[ii] * lens[jj]).sum())
-        result["cpu_baseline"] = {"value": round(cpu_cells / dt / 1e9, 4), "unit": "GCUPS", "cores": threads,
-                                  "kind": kind,
-                                  "sample": f"{npairs} pairs (i > j) drawn uniformly from the {N}-sequence job, "
-                                            f"{cpu_cells:.3g} cells, {dt:.1f} s"}
-        mism = int((full[ii, jj] != d_cpu).sum())
-        result["parity"] = {"pairs_checked_vs_cpu_reference": npairs, "mismatches": mism,
-                            "tolerance": "exact Int16"}
-        # plain one-launch-per-block kernel vs the batched engine on the same 2,000-sequence block
-        M = min(2000, N)
-        sub = with_options(cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4, device=local))
-        sub.upload(concat=concat[: off[M]], offsets=off[: M + 1])
-        sub.use_stream(stream.cuda_stream)
-        o2 = torch.zeros((M, M), dtype=torch.int16, device="cuda")
-        o3 = torch.zeros((M, M), dtype=torch.int16, device="cuda")
-        sub.all_pairs_device(o2.data_ptr(), M)
-        sub.compute_block_device(0, M - 1, 0, M - 1, True, o3.data_ptr(), M)
-        torch.cuda.synchronize()
-        sub_cells = float(np.tril(np.outer(lens[:M], lens[:M]), -1).sum())
-        times = {}
-        for name, fn in (("batched", lambda: sub.all_pairs_device(o2.data_ptr(), M)),
-                         ("plain", lambda: sub.compute_block_device(0, M - 1, 0, M - 1, True, o3.data_ptr(), M))):
-            b, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            flush.zero_()
-            b.record(stream)
-            fn()
-            e.record(stream)
-            torch.cuda.synchronize()
-            times[name] = b.elapsed_time(e)
-        a2, a3 = o2.cpu().numpy(), o3.cpu().numpy()
-        offd = ~np.eye(M, dtype=bool)
-        result["plain_vs_batched"] = {"block": f"diagonal block of {M} sequences ({M * (M - 1) // 2} pairs)",
-                                      "plain_gcups": round(sub_cells / (times["plain"] * 1e-3) / 1e9, 2),
-                                      "batched_gcups": round(sub_cells / (times["batched"] * 1e-3) / 1e9, 2),
-                                      "speedup": round(times["plain"] / times["batched"], 2),
-                                      "identical": bool(np.array_equal(a2[offd], a3[offd]))}
-        sub.close()
-        result["configs"] = other_configs(cs, local, stream, flush)
-        result["serving"] = serving(cs, local, a.serve_seconds, SERVE["load"])
+        covered = {share_of(k) for k in range(a.warmup + a.steps)}
+        extras(a, cs, eng, stream, flush, out, concat, off, lens, N, share_cells, threads, result, covered)
     if rank == 0:
         print(json.dumps(result))
     if world > 1:
@@ -515,6 +541,125 @@ def main():
         dist.destroy_process_group()
     eng.close()
     return 0
+
+
+def start_parity(cs, sets, picks, threads):
+    """Queue the oracle checks of configurations 1, 2 and 4 on all but two host cores."""
+    tables = {}
+    for name, _, seqs, matrix, o, e, mode, atype in sets:
+        concat, off = cs.pack_sequences(seqs)
+        tables[name] = (concat, off, cs.ScoringMatrix.Load(matrix).Scores[:127, :127].copy(), o, e, atype)
+    parity = Parity(tables, threads - 2)
+    for name, _, seqs, matrix, o, e, mode, atype in sets:
+        ii, jj = picks[name]
+        kind = "nw" if mode == cs.NW else ("ref" if (atype == cs.PROTEIN and reference_available()) else "count")
+        parity.submit(name, kind, ii, jj)
+    return parity
+
+
+def extras(a, cs, eng, stream, flush, out, concat, off, lens, N, share_cells, threads, result, covered):
+    import torch
+    # ---- CPU baseline: the reference's aligner on a uniform sample of the job's pairs, oriented
+    # as the 8-rank run orients them (s1 = the row of the share that aligns the pair), alone on the
+    # host cores; its distances against the GPU matrix of the shares the timed run computed
+    ii, jj, blk = sample_pairs(N, 200000, np.random.default_rng(5))
+    keep = np.isin(blk[ii], list(covered))
+    ii, jj = ii[keep], jj[keep]
+    per_pair = float(np.mean(lens[ii] * lens[jj]))
+    npairs = int(max(threads * 4, min(len(ii), a.cpu_seconds * threads * 0.12e9 / per_pair)))
+    ii, jj = ii[:npairs], jj[:npairs]
+    kind = "reference" if reference_available() else "port"
+    if kind == "reference":
+        d_cpu, dt = cpu_reference(concat, off, ii, jj, threads)
+    else:
+        import oracle
+        sc = cs.ScoringMatrix.Load("EDNAFULL").Scores[:127, :127].astype(np.float32)
+        t = time.perf_counter()
+        d_cpu = oracle.pairs(concat, off, ii, jj, sc, 16.0, 4.0, threads=threads)
+        dt = time.perf_counter() - t
+    cpu_cells = float((lens[ii] * lens[jj]).sum())
+    result["cpu_baseline"] = {"value": round(cpu_cells / dt / 1e9, 4), "unit": "GCUPS", "cores": threads,
+                              "kind": kind,
+                              "sample": f"{npairs} pairs (i > j) drawn uniformly from the {N}-sequence job, "
+                                        f"{cpu_cells:.3g} cells, {dt:.1f} s"}
+    got = out[torch.from_numpy(ii).cuda(), torch.from_numpy(jj).cuda()].cpu().numpy()
+    result["parity"] = {"pairs_checked_vs_cpu_reference": npairs, "mismatches": int((got != d_cpu).sum()),
+                        "tolerance": "exact Int16"}
+
+    # ---- e2e: the reference-facing C ABI with host buffers.  Per step: sw_upload_sequences of the
+    # set from pinned host memory (same lengths and letters: the engine keeps its plans), then one
+    # sw_compute_block call per block of the share, in the reference driver's order, each copying
+    # its block into the rank's row slab in pinned host memory
+    pin_seq = torch.from_numpy(concat).pin_memory().numpy()
+    rows = max(b - a_ + 1 for a_, b in ranges(N, SHARES))
+    slab = torch.empty((rows, N), dtype=torch.int16).pin_memory().numpy()
+    t = time.perf_counter()
+    eng.set_option("plan_only", 1)
+    for s in range(SHARES):
+        r0 = ranges(N, SHARES)[s][0]
+        for rs, re_, cs_, ce, diag in share_blocks(N, s):
+            eng.compute_block(rs, re_, cs_, ce, diag, out=slab[rs - r0:re_ - r0 + 1, cs_:ce + 1])
+    eng.set_option("plan_only", 0)
+    e2e_plan_s = time.perf_counter() - t
+    e_cells, e_s, h2d, d2h = 0, 0.0, 0, 0
+    for k in range(-1, SHARES):  # one untimed step, then the whole job
+        s = max(k, 0)
+        r0 = ranges(N, SHARES)[s][0]
+        t = time.perf_counter()
+        eng.upload(concat=pin_seq, offsets=off)
+        for rs, re_, cs_, ce, diag in share_blocks(N, s):
+            eng.compute_block(rs, re_, cs_, ce, diag, out=slab[rs - r0:re_ - r0 + 1, cs_:ce + 1])
+        dt = time.perf_counter() - t
+        if k >= 0:
+            e_s += dt
+            e_cells += share_cells[s]
+            h2d += concat.nbytes + off.nbytes
+            d2h += sum((re_ - rs + 1) * (ce - cs_ + 1) * 2 for rs, re_, cs_, ce, _ in share_blocks(N, s))
+    result["e2e"] = {"value": round(e_cells / e_s / 1e9, 3), "unit": "GCUPS",
+                     "h2d_bytes_per_step": int(h2d // SHARES), "d2h_bytes_per_step": int(d2h // SHARES),
+                     "note": "per step (one 8-rank share): sw_upload_sequences from pinned host memory, then one "
+                             "sw_compute_block per block of the share (host output) in the reference driver's order; "
+                             "host wall clock; the 8 steps are the whole job",
+                     "plan_s": round(e2e_plan_s, 2)}
+
+    # ---- the parity checks of configurations 1, 2 and 4 run on the host cores from here on
+    sets = config_sets(cs)
+    picks = {s[0]: config_parity_pairs(len(s[2]), s[0], np.random.default_rng(21)) for s in sets}
+    parity = start_parity(cs, sets, picks, threads)
+
+    # ---- plain one-launch-per-block kernel vs the engine behind the same block handler, on one
+    # whole 8-rank share, block by block in the driver's order, device output
+    share = 0
+    r0, r1 = ranges(N, SHARES)[share]
+    d_plain = torch.zeros((r1 - r0 + 1, N), dtype=torch.int16, device="cuda")
+    d_eng = torch.zeros_like(d_plain)
+    blocks = share_blocks(N, share)
+
+    def handler_calls(dst):
+        for rs, re_, cs_, ce, diag in blocks:
+            eng.compute_block_device(rs, re_, cs_, ce, diag, dst.data_ptr() + ((rs - r0) * N + cs_) * 2, N)
+
+    eng.set_option("plan_only", 1)
+    handler_calls(d_eng)
+    eng.set_option("plan_only", 0)
+    times = {}
+    for name, mode, dst in (("batched", 1, d_eng), ("plain", 0, d_plain)):
+        eng.set_option("block_engine", mode)
+        flush.zero_()
+        times[name] = _timed(stream, lambda: handler_calls(dst))
+    eng.set_option("block_engine", 1)
+    sc = float(share_cells[share])
+    result["plain_vs_batched"] = {"share": f"rank {share} of an {SHARES}-rank run: {len(blocks)} blocks, "
+                                           f"{sc:.3g} cells, one block-handler call per block",
+                                  "plain_gcups": round(sc / (times["plain"] * 1e-3) / 1e9, 2),
+                                  "batched_gcups": round(sc / (times["batched"] * 1e-3) / 1e9, 2),
+                                  "speedup": round(times["plain"] / times["batched"], 2),
+                                  "identical": bool(torch.equal(d_plain, d_eng))}
+    del d_plain, d_eng
+
+    result["configs"] = run_configs(cs, 0, stream, flush, sets, picks, parity)
+    result["configs"]["parity_workers_s"] = round(parity.close(), 1)
+    result["serving"] = serving(cs, 0, a.serve_jobs, SERVE["load"])
 
 
 if __name__ == "__main__":
