@@ -9,10 +9,10 @@ block-handler interface over that ABI.
 from .core import (Block, Engine, NUCLEIC, NW, PROTEIN, PairwiseAlignment, Range, ScoringMatrix,
                    SmithWatermanGotoh, SWG_MPI, SWG_MS, block_is_computed, block_partition,
                    measure_int_peak, pack_sequences, range_partition)
-from .core import JUKES_CANTOR, KIMURA2, PERCENT_IDENTITY
+from .core import JUKES_CANTOR, KIMURA2, MIN_MAX_NORM_SCORE, PERCENT_IDENTITY
 from .lib import SwError
 
 __all__ = ["Block", "Engine", "NUCLEIC", "NW", "PROTEIN", "PairwiseAlignment", "Range",
            "ScoringMatrix", "SmithWatermanGotoh", "SWG_MPI", "SWG_MS", "block_is_computed",
            "block_partition", "measure_int_peak", "pack_sequences", "range_partition",
-           "PERCENT_IDENTITY", "KIMURA2", "JUKES_CANTOR", "SwError"]
+           "PERCENT_IDENTITY", "KIMURA2", "JUKES_CANTOR", "MIN_MAX_NORM_SCORE", "SwError"]

@@ -18,7 +18,8 @@ import numpy as np
 from . import lib as L
 
 PROTEIN, NUCLEIC = L.SW_PROTEIN, L.SW_NUCLEIC
-PERCENT_IDENTITY, KIMURA2, JUKES_CANTOR = L.SW_DIST_PERCENT_IDENTITY, L.SW_DIST_KIMURA2, L.SW_DIST_JUKES_CANTOR
+PERCENT_IDENTITY, KIMURA2, JUKES_CANTOR, MIN_MAX_NORM_SCORE = (L.SW_DIST_PERCENT_IDENTITY, L.SW_DIST_KIMURA2,
+                                                          L.SW_DIST_JUKES_CANTOR, L.SW_DIST_MIN_MAX_NORM_SCORE)
 SWG_MPI, SWG_MS, NW = L.SW_MODE_SWG_MPI, L.SW_MODE_SWG_MS, L.SW_MODE_NW
 
 

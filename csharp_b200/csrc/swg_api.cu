@@ -126,12 +126,8 @@ int sw_create(const sw_config* cfg, sw_ctx** out) {
   *out = nullptr;
   if (cfg->mode < 0 || cfg->mode > 2) return SW_E_ARG;
   if (cfg->alignment_type != SW_PROTEIN && cfg->alignment_type != SW_NUCLEIC) return SW_E_ARG;
-  if (cfg->distance_fn < 0 || cfg->distance_fn > 2) return SW_E_ARG;
+  if (cfg->distance_fn < 0 || cfg->distance_fn > 3) return SW_E_ARG;
   if (cfg->lanes != SW_LANES_AUTO && cfg->lanes != SW_LANES_16 && cfg->lanes != SW_LANES_32) return SW_E_ARG;
-  // Kimura2 / JukesCantor of NW alignments are not restated here (SWG-MPI and SWG-MS are).
-  if (cfg->distance_fn != SW_DIST_PERCENT_IDENTITY && cfg->alignment_type == SW_NUCLEIC &&
-      cfg->mode == SW_MODE_NW)
-    return SW_E_UNSUPPORTED;
   const float o = cfg->gap_open, e = cfg->gap_extension;
   if (!(std::isfinite(o) && std::isfinite(e))) return SW_E_ARG;
   if (o != std::floor(o) || e != std::floor(e)) return SW_E_UNSUPPORTED;
@@ -453,6 +449,19 @@ int sw_align_pair(sw_ctx* ctx, const uint8_t* s1, int32_t m, const uint8_t* s2, 
   out->identity = r.identity; out->similarity = r.similarity;
   out->gaps = r.gaps; out->length = r.length;
   out->reserved = 0;
+  if (ctx->cfg.alignment_type == SW_NUCLEIC && ctx->cfg.distance_fn == SW_DIST_MIN_MAX_NORM_SCORE) {
+    // MinMaxNormScore (SWG-MS Program.cs:544-553) in binary64; SWG-MPI has no case for it: 0
+    if (ctx->cfg.mode != SW_MODE_SWG_MS) { out->distance = 0; return SW_OK; }
+    long long self1 = 0, self2 = 0;
+    for (int k = 0; k < m; k++) self1 += ctx->h_scores[s1[k]][s1[k]];
+    for (int k = 0; k < n; k++) self2 += ctx->h_scores[s2[k]][s2[k]];
+    const long long s = (m == 0 || n == 0) ? 0 : r.score;
+    volatile double x = (double)s / (double)std::max(self1, self2);
+    volatile double v = (1.0 - x) * 32767.0;
+    const double vv = v;
+    out->distance = (vv > -2147483649.0 && vv < 2147483648.0) ? (int16_t)(uint16_t)(uint32_t)(int32_t)vv : 0;
+    return SW_OK;
+  }
   if (ctx->cfg.alignment_type == SW_NUCLEIC && ctx->cfg.distance_fn != SW_DIST_PERCENT_IDENTITY) {
     // Kimura2 / JukesCantor (Alignment.cs:254-348) in binary64, as the device epilogue
     const double eps = 4.9406564584124654e-324;  // System.Double.Epsilon

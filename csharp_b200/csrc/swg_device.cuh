@@ -193,4 +193,19 @@ __device__ __forceinline__ int16_t kim_distance(const KimCnt::T& c, int dist_fn,
   return cs_conv_i2_d(__dmul_rn(v, 32767.0));
 }
 
+// MinMaxNormScore of an alignment scoring s between sequences whose self scores (the sum of the
+// matrix's diagonal over their residues) are self1 and self2: (1 - (s - minS) / (maxS - minS)) *
+// 32767 in binary64, maxS = max(self1, self2), minS = 0 for SWG-MS (Salsa.SmithWatermanMS/
+// Program.cs:544-553) and 2 open + (m + n) extend for NW (Salsa.NeedlemanWunschTPL/Program.cs:
+// 573-581).  SWG-MPI's ComputeDistance has no case for it (Program.cs:259-285): its result stays 0.
+// mode: 0 SWG-MPI, 1 SWG-MS, 2 NW.
+__device__ __forceinline__ int16_t minmax_distance(long long s, int self1, int self2, int m, int n, int o, int e,
+                                                   int mode) {
+  if (mode == 0) return 0;
+  const long long maxS = self1 > self2 ? self1 : self2;
+  const long long minS = mode == 2 ? 2LL * o + (long long)(m + n) * e : 0LL;
+  const double x = __ddiv_rn((double)(s - minS), (double)(maxS - minS));
+  return cs_conv_i2_d(__dmul_rn(__dsub_rn(1.0, x), 32767.0));
+}
+
 }  // namespace swg

@@ -158,6 +158,13 @@ __device__ __forceinline__ int16_t nw_distance(const NwCnt::T& c, int m, int n, 
   return fraction_distance(count, trimmed);
 }
 
+// Sum of the matrix's diagonal over a sequence's residues (MinMaxNormScore's self score).
+__device__ __forceinline__ int self_score(const uint8_t* s, int n, const int16_t* sc) {
+  int t = 0;
+  for (int k = 0; k < n; k++) t += sc[(int)s[k] * (kTable + 1)];
+  return t;
+}
+
 template <bool LOCAL, class CP, int K>
 __global__ void __launch_bounds__(128) plain_block_kernel(PlainJob J) {
   __shared__ int16_t sc[kTable * kTable];
@@ -182,28 +189,35 @@ __global__ void __launch_bounds__(128) plain_block_kernel(PlainJob J) {
     const int m = J.qoff ? J.qlen[i] : (int)(J.off[i + 1] - J.off[i]);
     const int n = (int)(J.off[j + 1] - J.off[j]);
     int16_t d;
-    if (LOCAL) {
-      if constexpr (std::is_same<CP, KimCnt>::value) {
-        KimCnt::T c = KimCnt::origin();
-        if (m > 0 && n > 0) c = dp_pair<LOCAL, CP, K, false>(s1, m, s2, n, sc, fl, J.o, J.e, carry, stride).c;
-        d = kim_distance(c, J.dist_fn, J.mode == kModeSwgMs, J.throws);
-      } else if (m == 0 || n == 0) {
-        d = fraction_distance(0, 0);
+    const bool minmax = J.dist_fn == 3 && !J.protein;  // MinMaxNormScore: from the score alone
+    if constexpr (std::is_same<CP, KimCnt>::value) {
+      // Kimura2 / JukesCantor; SWG-MS and NW cap them at 10 (and JukesCantor's Log(Zero) is 10)
+      KimCnt::T c = KimCnt::origin();
+      if (m > 0 && n > 0) c = dp_pair<LOCAL, CP, K, false>(s1, m, s2, n, sc, fl, J.o, J.e, carry, stride).c;
+      d = kim_distance(c, J.dist_fn, J.mode != kModeSwgMpi, J.throws);
+    } else if (LOCAL) {
+      if (m == 0 || n == 0) {
+        d = minmax ? minmax_distance(0, self_score(s1, m, sc), self_score(s2, n, sc), m, n, J.o, J.e, J.mode)
+                   : fraction_distance(0, 0);
       } else {
         DpResult<CP> r = dp_pair<LOCAL, CP, K, false>(s1, m, s2, n, sc, fl, J.o, J.e, carry, stride);
         const uint32_t w = *reinterpret_cast<const uint32_t*>(&r.c);
-        d = fraction_distance((int)(w & 0xFFFFu), (int)(w >> 16));
+        d = minmax ? minmax_distance(r.best, self_score(s1, m, sc), self_score(s2, n, sc), m, n, J.o, J.e, J.mode)
+                   : fraction_distance((int)(w & 0xFFFFu), (int)(w >> 16));
       }
     } else if constexpr (std::is_same<CP, NwCnt>::value) {
       NwCnt::T c;
-      if (m == 0 && n == 0) c = NwCnt::origin();
-      else if (m == 0) c = NwCnt::row0(n);
-      else if (n == 0) c = NwCnt::col0(m);
+      long long score;  // V(m, n): the global alignment's score
+      if (m == 0 && n == 0) { c = NwCnt::origin(); score = 0; }
+      else if (m == 0) { c = NwCnt::row0(n); score = -(long long)J.o - (long long)(n - 1) * J.e; }
+      else if (n == 0) { c = NwCnt::col0(m); score = -(long long)J.o - (long long)(m - 1) * J.e; }
       else {
         DpResult<CP> r = dp_pair<LOCAL, CP, K, false>(s1, m, s2, n, sc, fl, J.o, J.e, carry, stride);
         c = *reinterpret_cast<const NwCnt::T*>(&r.c);
+        score = r.best;
       }
-      d = nw_distance(c, m, n, J.protein);
+      d = minmax ? minmax_distance(score, self_score(s1, m, sc), self_score(s2, n, sc), m, n, J.o, J.e, J.mode)
+                 : nw_distance(c, m, n, J.protein);
     }
     if (J.qoff) {
       J.qout[i][j] = d;
@@ -565,15 +579,17 @@ __global__ void __launch_bounds__(32) align_pair_kernel(PairJob J) {
 
 // ---- launchers -----------------------------------------------------------------------------
 size_t plain_carry_bytes(int mode, long threads, int maxlen, int dist_fn) {
-  const size_t per = (mode == kModeNw) ? sizeof(Carry<NwCnt>)
-                     : dist_fn ? sizeof(Carry<KimCnt>) : sizeof(Carry<SwCnt>);
+  static_assert(sizeof(Carry<KimCnt>) >= sizeof(Carry<NwCnt>), "carry sizes");
+  const size_t per = dist_fn ? sizeof(Carry<KimCnt>) : (mode == kModeNw) ? sizeof(Carry<NwCnt>) : sizeof(Carry<SwCnt>);
   return per * (size_t)threads * (size_t)(maxlen + 1);
 }
 
 cudaError_t launch_plain_block(const PlainJob& J, int grid, int block, cudaStream_t st) {
   if (J.npairs == 0) return cudaSuccess;
-  if (J.mode == kModeNw) plain_block_kernel<false, NwCnt, 8><<<grid, block, 0, st>>>(J);
-  else if (J.dist_fn && !J.protein) plain_block_kernel<true, KimCnt, 8><<<grid, block, 0, st>>>(J);
+  const bool kim = (J.dist_fn == 1 || J.dist_fn == 2) && !J.protein;
+  if (J.mode == kModeNw && kim) plain_block_kernel<false, KimCnt, 8><<<grid, block, 0, st>>>(J);
+  else if (J.mode == kModeNw) plain_block_kernel<false, NwCnt, 8><<<grid, block, 0, st>>>(J);
+  else if (kim) plain_block_kernel<true, KimCnt, 8><<<grid, block, 0, st>>>(J);
   else plain_block_kernel<true, SwCnt, 8><<<grid, block, 0, st>>>(J);
   return cudaGetLastError();
 }

@@ -114,8 +114,8 @@ extern "C" int sw_compute_block_static(const sw_config* cfg, const uint8_t* d_re
   if (!cfg || !d_residues || !d_offsets || !d_out || count < 1) return SW_E_ARG;
   if (cfg->mode < 0 || cfg->mode > 2) return SW_E_ARG;
   if (cfg->alignment_type != SW_PROTEIN && cfg->alignment_type != SW_NUCLEIC) return SW_E_ARG;
-  if (cfg->distance_fn < 0 || cfg->distance_fn > 2) return SW_E_ARG;
-  // Kimura2 / JukesCantor (nucleic) need a per-call error report this entry point does not wait for
+  if (cfg->distance_fn < 0 || cfg->distance_fn > 3) return SW_E_ARG;
+  // Kimura2 / JukesCantor / MinMaxNormScore (nucleic) are the allocating entry points' work
   if (cfg->distance_fn != SW_DIST_PERCENT_IDENTITY && cfg->alignment_type == SW_NUCLEIC) return SW_E_UNSUPPORTED;
   const float o = cfg->gap_open, e = cfg->gap_extension;
   if (!(o == o && e == e) || o != (float)(int)o || e != (float)(int)e) return SW_E_UNSUPPORTED;

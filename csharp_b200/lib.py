@@ -13,7 +13,7 @@ LIB_PATH = PKG / "libswgb200.so"
 
 SW_OK, SW_E_ARG, SW_E_OOM, SW_E_CUDA, SW_E_TIMEOUT, SW_E_UNSUPPORTED, SW_E_STATE, SW_E_IO, SW_E_THROWS = range(9)
 SW_PROTEIN, SW_NUCLEIC = 0, 1
-SW_DIST_PERCENT_IDENTITY, SW_DIST_KIMURA2, SW_DIST_JUKES_CANTOR = 0, 1, 2
+SW_DIST_PERCENT_IDENTITY, SW_DIST_KIMURA2, SW_DIST_JUKES_CANTOR, SW_DIST_MIN_MAX_NORM_SCORE = 0, 1, 2, 3
 SW_MODE_SWG_MPI, SW_MODE_SWG_MS, SW_MODE_NW = 0, 1, 2
 SW_LANES_AUTO, SW_LANES_16, SW_LANES_32 = 0, 16, 32
 

@@ -40,6 +40,7 @@ extern "C" {
 #define SW_DIST_PERCENT_IDENTITY 0
 #define SW_DIST_KIMURA2 1
 #define SW_DIST_JUKES_CANTOR 2
+#define SW_DIST_MIN_MAX_NORM_SCORE 3  /* SWG-MS and NW: from the alignment score and the self scores */
 
 /* Which reference application's semantics a context reproduces. */
 #define SW_MODE_SWG_MPI 0 /* Salsa.SmithWatermanMPI: NAligner SW-Gotoh, diagonal blocks j < i */
@@ -83,7 +84,11 @@ typedef struct {
  * _scoringMatrixName, _alignmentType and _distanceFunction that ComputeBlock reads
  * (Salsa.SmithWatermanMPI/Program.cs:58-62, :206-207; Salsa.SmithWatermanMS/Program.cs:275-276;
  * Salsa.NeedlemanWunschTPL/Program.cs:210-213).  Non-integer penalties are SW_E_UNSUPPORTED:
- * the reference's float DP is exact only on integers, which the integer kernels reproduce. */
+ * the reference's float DP is exact only on integers, which the integer kernels reproduce.
+ * distance_fn applies to nucleic input (protein uses PercentSimilarity, as the reference does):
+ * Kimura2 / JukesCantor in every mode (SWG-MS and NW cap them at 10, as their Program.cs does),
+ * MinMaxNormScore in SWG-MS and NW (SWG-MPI's ComputeDistance has no case for it, so its
+ * distances are 0, as the reference's are). */
 int sw_create(const sw_config* cfg, sw_ctx** out);
 int sw_destroy(sw_ctx* ctx);
 const char* sw_last_error(const sw_ctx* ctx);
@@ -195,7 +200,8 @@ int sw_query(sw_ctx* ctx, const char* key, int64_t* value);
  * has a fixed device-memory budget).  It aligns the pairs of one block like
  * sw_compute_block_device, with the same ranges, orientation and mirror rule, in all three
  * modes, with PercentIdentity for nucleic input and PercentSimilarity for protein (nucleic
- * Kimura2 / JukesCantor are SW_E_UNSUPPORTED here; distance_fn outside 0..2 is SW_E_ARG).  It
+ * Kimura2 / JukesCantor / MinMaxNormScore are SW_E_UNSUPPORTED here; distance_fn outside 0..3 is
+ * SW_E_ARG).  It
  * needs no context: the configuration comes in cfg, the residues and offsets
  * (sw_upload_sequences' layout: d_residues holds d_offsets[count] bytes) and the output are the
  * caller's device buffers, and the work is ordered on `stream` (a cudaStream_t of cfg->device,

@@ -298,3 +298,25 @@ def ref_distances(matrix_name, alignment_type, dist_fn, o, e, seqs, offsets, row
     if n < 0:
         raise RuntimeError("reference aligner raised")
     return out
+
+
+def _conv_i2_double(v):
+    """.NET x64 conv.i2 of a double: truncate through int32 (NaN and out-of-range give 0x80000000),
+    then the low 16 bits."""
+    if not (-2147483649.0 < v < 2147483648.0):
+        return 0
+    return int(np.array(int(v) & 0xFFFF, dtype=np.uint16).view(np.int16))
+
+
+def minmax_distance_i16(score, self1, self2, m, n, o, e, mode):
+    """MinMaxNormScore's Int16 distance: (1 - (s - minS) / (maxS - minS)) * 32767 in binary64 with
+    maxS = max of the self scores, minS = 0 (SWG-MS, Program.cs:544-553) or 2 open + (m + n)
+    extend (NW, Program.cs:573-581); SWG-MPI's ComputeDistance has no case for it: 0."""
+    if mode == 0:
+        return 0
+    mx = max(self1, self2)
+    mn = 2 * o + (m + n) * e if mode == 2 else 0
+    with np.errstate(all="ignore"):
+        x = np.float64(score - mn) * 1.0 / np.float64(mx - mn)
+        v = (np.float64(1.0) - x) * np.float64(32767.0)
+    return _conv_i2_double(float(v))

@@ -538,3 +538,64 @@ def test_reupload_of_same_shaped_set_keeps_plans_and_uses_new_residues(cs):
     assert not np.array_equal(got_a, got_b)
     eng.close()
     fresh.close()
+
+
+def _self_score(seq, scores):
+    return int(sum(int(scores[c, c]) for c in seq))
+
+
+@pytest.mark.parametrize("dist_fn", [1, 2, 3])
+def test_nw_kimura_jukes_cantor_minmax_against_oracle(cs, oracle_mod, dist_fn):
+    """NW with Kimura2, JukesCantor (capped at 10, NW Program.cs:606-719) and MinMaxNormScore
+    (:573-581) on the 32-bit lanes: every pair against the oracle's NW alignment (exact Int16)."""
+    from csharp_b200 import synth
+    rng = np.random.default_rng(50 + dist_fn)
+    lens = np.concatenate([rng.integers(1, 300, 36), [0, 1]])
+    seqs = [s.tobytes() for s in synth.dna_family(len(lens), 3, lens, seed=51)]
+    sm = cs.ScoringMatrix.Load("EDNAFULL")
+    eng = cs.Engine(sm, 16, 4, mode=cs.NW, distance_fn=dist_fn).upload(seqs)
+    full, _, _ = eng.all_pairs(1)
+    sc = sm.Scores[:127, :127].astype(np.float32)
+    N = len(seqs)
+    for i in range(N):
+        for j in range(i):
+            a = oracle_mod.nw_align(seqs[i], seqs[j], sc, 16.0, 4.0)
+            if dist_fn == 3:
+                want = oracle_mod.minmax_distance_i16(int(a["score"]), _self_score(seqs[i], sm.Scores),
+                                                      _self_score(seqs[j], sm.Scores), len(seqs[i]), len(seqs[j]),
+                                                      16, 4, 2)
+            else:
+                want = oracle_mod.ms_distance_i16(a["aln1"], a["aln2"], sc, False, dist_fn)
+            assert full[i, j] == want and full[j, i] == want, (i, j, dist_fn)
+    eng.close()
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_minmax_norm_score_smith_waterman(cs, oracle_mod, mode):
+    """MinMaxNormScore in SWG-MS (score over the larger self score) and in SWG-MPI, whose
+    ComputeDistance has no case for it (every distance 0); also through the single-pair call."""
+    from csharp_b200 import synth
+    rng = np.random.default_rng(60 + mode)
+    lens = np.concatenate([rng.integers(1, 400, 40), [0, 1]])
+    seqs = [s.tobytes() for s in synth.dna_family(len(lens), 4, lens, seed=61)]
+    sm = cs.ScoringMatrix.Load("EDNAFULL")
+    eng = cs.Engine(sm, 16, 4, mode=mode, distance_fn=cs.MIN_MAX_NORM_SCORE).upload(seqs)
+    full, _, _ = eng.all_pairs(1)
+    sc = sm.Scores[:127, :127].astype(np.float32)
+    N = len(seqs)
+    for i in range(N):
+        for j in range(N):
+            if mode == 0 and j >= i:
+                continue
+            if mode == 0:
+                want = 0
+            else:
+                a = oracle_mod.align(seqs[i], seqs[j], sc, 16.0, 4.0)
+                s = 0 if not (len(seqs[i]) and len(seqs[j])) else int(a["score"])
+                want = oracle_mod.minmax_distance_i16(s, _self_score(seqs[i], sm.Scores), _self_score(seqs[j], sm.Scores),
+                                                      len(seqs[i]), len(seqs[j]), 16, 4, 1)
+            assert full[i, j] == want, (i, j)
+    if mode == 1:
+        for i, j in [(3, 5), (0, 40), (7, 7)]:
+            assert eng.align(seqs[i], seqs[j]).Distance == full[i, j]
+    eng.close()

@@ -117,7 +117,7 @@ def _cfg(**kw):
     (dict(mode=7), 1), (dict(alignment_type=3), 1), (dict(lanes=8), 1),
     (dict(gap_open=14.5), 5), (dict(gap_extension=0.25), 5), (dict(gap_open=0.0), 5),
     (dict(gap_extension=-1.0), 5), (dict(mode=2, gap_open=4.0, gap_extension=4.0), 5),
-    (dict(mode=2, distance_fn=1), 5),
+    (dict(distance_fn=4), 1), (dict(distance_fn=-1), 1),
 ])
 def test_create_rejects_configs_before_touching_a_device(kw, status):
     from csharp_b200 import lib
