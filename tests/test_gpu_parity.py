@@ -4,6 +4,8 @@ Golden vectors come from the reference's own aligner and block driver (tests/gol
 inputs are checked against the oracle (the CPU restatement, itself pinned to those vectors).
 Tolerance: exact Int16 equality everywhere.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -598,4 +600,37 @@ def test_minmax_norm_score_smith_waterman(cs, oracle_mod, mode):
     if mode == 1:
         for i, j in [(3, 5), (0, 40), (7, 7)]:
             assert eng.align(seqs[i], seqs[j]).Distance == full[i, j]
+    eng.close()
+
+
+def test_ms_block_files_from_the_engine_match_the_oracle_run(cs, oracle_mod, tmp_path):
+    """SWG-MS driver with the engine as block handler: every block file equals, byte for byte, the
+    file a run with the oracle's block handler writes."""
+    from csharp_b200 import synth
+    from csharp_b200.msdriver import MSBlockRun, engine_handler
+    rng = np.random.default_rng(81)
+    N, W = 90, 4
+    seqs = [s.tobytes() for s in synth.dna_family(N, 5, rng.integers(1, 400, N), seed=82)]
+    ids = [f"s{k}" for k in range(N)]
+    m = cs.ScoringMatrix.Load("EDNAFULL")
+    eng = cs.Engine(m, 16, 4, mode=cs.SWG_MS).upload(seqs)
+    eng.set_option("block_engine", 2)
+    concat, off = cs.pack_sequences(seqs)
+    sc = m.Scores[:127, :127].astype(np.float32)
+
+    def oracle_handler(block, pm, diag, rank):
+        rr, cr = block.RowRange, block.ColumnRange
+        vals, n = oracle_mod.block(concat, off, rr.StartIndex, rr.EndIndex, cr.StartIndex, cr.EndIndex, diag, 1, sc, 16.0, 4.0)
+        pm.block_view(block)[...] = vals
+        return n
+    for tag, h in (("gpu", engine_handler(eng)), ("cpu", oracle_handler)):
+        d = tmp_path / tag
+        d.mkdir()
+        for r in range(W):
+            MSBlockRun(N, h, r, W, str(d), 1, ids).Compute()
+    a, b = tmp_path / "gpu", tmp_path / "cpu"
+    names = sorted(os.listdir(b))
+    assert sorted(os.listdir(a)) == names and names
+    for f in names:
+        assert (a / f).read_bytes() == (b / f).read_bytes(), f
     eng.close()
