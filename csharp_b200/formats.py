@@ -80,3 +80,34 @@ def read_restart_file(path):
                 a, b = ln.replace("\t", " ").split()[:2]
                 entries.append((int(a), int(b)))
     return world, entries
+
+
+def write_row_files(directory, prefix, ext, rows_of, size, parts):
+    """The partial-matrix files the pairwise-clustering loader reads (PWCParallelism.cs:107-150,
+    MatrixBinaryReader.cs:191-217): the size points are split into `parts` ranges (RangePartitioner;
+    parts = processes x threads of the reader), and file {prefix}_{i}{ext} holds the rows of range i
+    over all size columns, raw little-endian Int16.  rows_of(start, end) returns those rows (a host
+    array, or a device tensor, which is copied to the host one range at a time)."""
+    from .core import range_partition
+    paths = []
+    for i, r in enumerate(range_partition(size, parts)):
+        if r.Length <= 0:
+            continue
+        rows = rows_of(r.StartIndex, r.EndIndex)
+        if hasattr(rows, "cpu"):
+            rows = rows.cpu().numpy()
+        path = os.path.join(directory, f"{prefix}_{i}{ext}")
+        write_full_matrix(path, rows)
+        paths.append(path)
+    return paths
+
+
+def read_row_files(directory, prefix, ext, start, end, size, parts):
+    """MatrixBinaryReader.ReadInt16(path, prefix, ext, startIndex, endIndex, ranges): the rows of
+    files start..end stacked, size columns each."""
+    from .core import range_partition
+    rr = range_partition(size, parts)
+    out = []
+    for i in range(start, end + 1):
+        out.append(np.fromfile(os.path.join(directory, f"{prefix}_{i}{ext}"), dtype="<i2").reshape(rr[i].Length, size))
+    return np.concatenate(out, axis=0)

@@ -133,3 +133,20 @@ def test_synthetic_generator_is_seeded():
     assert all(np.array_equal(x, y) for x, y in zip(a, b))
     assert all(len(x) == 120 for x in a)
     assert set(np.concatenate(a).tobytes()) <= set(b"ACGT")
+
+
+def test_row_files_for_the_clustering_loader(tmp_path):
+    """Row files {prefix}_{i}{ext} over RangePartitioner ranges (MatrixBinaryReader.cs:191-217): a
+    reader with the same parallelism gets back exactly its rows of the matrix."""
+    from csharp_b200.formats import read_row_files, write_row_files
+    rng = np.random.default_rng(4)
+    n, procs, threads = 37, 3, 2
+    m = rng.integers(-32768, 32767, (n, n)).astype(np.int16)
+    paths = write_row_files(str(tmp_path), "dist", ".bin", lambda a, b: m[a:b + 1], n, procs * threads)
+    assert len(paths) == procs * threads
+    from csharp_b200 import range_partition
+    tr = range_partition(n, procs * threads)
+    for p in range(procs):  # process p reads its threads' files
+        got = read_row_files(str(tmp_path), "dist", ".bin", p * threads, p * threads + threads - 1, n, procs * threads)
+        np.testing.assert_array_equal(got, m[tr[p * threads].StartIndex:tr[p * threads + threads - 1].EndIndex + 1])
+    assert (tmp_path / "dist_0.bin").stat().st_size == tr[0].Length * n * 2
