@@ -221,6 +221,31 @@ class Engine:
         return PairwiseAlignment(r.score, r.start1, r.start2, r.end1, r.end2, r.identity, r.similarity,
                                  r.gaps, r.length, r.distance)
 
+    def align_strings(self, pairs):
+        """Alignment strings of explicit pairs (s1 index, s2 index) of the uploaded set, as the
+        applications print them with WriteAlignments: a list of (aligned s1, aligned s2,
+        PairwiseAlignment) with '-' for gaps."""
+        pairs = np.asarray(pairs, dtype=np.int32).reshape(-1, 2)
+        rows, cols = np.ascontiguousarray(pairs[:, 0]), np.ascontiguousarray(pairs[:, 1])
+        n = len(pairs)
+        if n and (rows.min() < 0 or cols.min() < 0 or rows.max() >= self.nseq or cols.max() >= self.nseq):
+            raise L.SwError(L.SW_E_ARG, "pair outside the uploaded sequences")
+        off = np.zeros(n + 1, dtype=np.int64)
+        if n:
+            np.cumsum(self.lengths[rows] + self.lengths[cols], out=off[1:])
+        a = np.zeros(max(int(off[-1]), 1), dtype=np.uint8)
+        b = np.zeros_like(a)
+        res = (L.sw_pair_result * max(n, 1))()
+        self._ck(L.load().sw_align_strings(self._h, L.ptr(rows), L.ptr(cols), n, L.ptr(a), L.ptr(b), L.ptr(off), res))
+        out = []
+        for k in range(n):
+            r = res[k]
+            s1 = a[off[k]:off[k] + r.length].tobytes()
+            s2 = b[off[k]:off[k] + r.length].tobytes()
+            out.append((s1, s2, PairwiseAlignment(r.score, r.start1, r.start2, r.end1, r.end2, r.identity,
+                                                  r.similarity, r.gaps, r.length, r.distance)))
+        return out
+
     def all_pairs(self, ranks=1):
         """Whole job to a host N x N Int16 matrix; returns (matrix, pairs, cells)."""
         out = np.zeros((self.nseq, self.nseq), dtype=np.int16)

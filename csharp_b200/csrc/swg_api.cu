@@ -507,6 +507,175 @@ int sw_align_pair(sw_ctx* ctx, const uint8_t* s1, int32_t m, const uint8_t* s2, 
   return SW_OK;
 }
 
+// Int16 distance of one traced alignment under the context's rules (the same arithmetic as the
+// kernels' epilogues): a, b are the aligned strings of len columns.
+static int16_t traced_distance(const sw_ctx* ctx, const char* a, const char* b, int len,
+                               const swg::TraceResult& r, int m, int n, long long self1, long long self2,
+                               int* throws) {
+  const bool protein = ctx->cfg.alignment_type == SW_PROTEIN;
+  const int mode = ctx->cfg.mode, fn = ctx->cfg.distance_fn;
+  auto conv_f = [](float x) -> int16_t { return (x > -2147483648.0f && x < 2147483648.0f) ? (int16_t)(int32_t)x : 0; };
+  auto conv_d = [](double x) -> int16_t {
+    return (x > -2147483649.0 && x < 2147483648.0) ? (int16_t)(uint16_t)(uint32_t)(int32_t)x : 0;
+  };
+  auto fraction = [&](int count, int cols) { volatile float p = (float)count / (float)cols; return conv_f((1.0f - p) * 32767.0f); };
+  if (!protein && fn == SW_DIST_MIN_MAX_NORM_SCORE) {  // SWG-MS :544-553, NW :573-581
+    if (mode == SW_MODE_SWG_MPI) return 0;               // no case in SWG-MPI's ComputeDistance
+    const long long sc = r.valid ? r.score : 0;
+    const long long maxS = std::max(self1, self2);
+    const long long minS = mode == SW_MODE_NW ? 2LL * ctx->o + (long long)(m + n) * ctx->e : 0LL;
+    volatile double x = (double)(sc - minS) / (double)(maxS - minS);
+    volatile double v = (1.0 - x) * 32767.0;
+    return conv_d(v);
+  }
+  if (!protein && (fn == SW_DIST_KIMURA2 || fn == SW_DIST_JUKES_CANTOR)) {
+    const double eps = 4.9406564584124654e-324;  // System.Double.Epsilon
+    const bool capped = mode != SW_MODE_SWG_MPI;
+    const double nongap = (double)r.diag;
+    double v;
+    if (fn == SW_DIST_KIMURA2) {
+      volatile double P = (double)r.transitions / nongap, Q = (double)r.transversions / nongap;
+      volatile double t1 = 1.0 - (2.0 * P + Q), t2 = 1.0 - 2.0 * Q;
+      if (t1 <= eps || t2 <= eps) v = 10.0;
+      else {
+        volatile double l1 = -0.5 * std::log(1.0 - 2.0 * P - Q), l2 = 0.25 * std::log(t2);
+        v = l1 - l2;
+      }
+      if (capped && v > 10.0) v = 10.0;
+    } else {
+      volatile double d = 1.0 - (4.0 / 3.0) * ((double)(r.diag - r.identity) / nongap);
+      if (d <= eps) {
+        if (!capped) { *throws = 1; return 0; }
+        v = 10.0;
+      } else {
+        v = -0.75 * std::log(d);
+      }
+    }
+    volatile double x = v * 32767.0;
+    return conv_d(x);
+  }
+  if (mode == SW_MODE_NW) {
+    if (protein) {  // MBF similarity: non-gap pairs with a positive score, over every column
+      int sim = 0;
+      for (int k = 0; k < len; k++)
+        if (a[k] != '-' && b[k] != '-' && ctx->h_scores[(uint8_t)a[k]][(uint8_t)b[k]] > 0) sim++;
+      return fraction(sim, len);
+    }
+    // identity between the last leading and the first trailing end gap (Program.cs:547-571)
+    int fa = -1, fb = -1, la = -1, lb = -1;
+    for (int k = 0; k < len && fa < 0; k++) if (a[k] != '-') fa = k;
+    for (int k = 0; k < len && fb < 0; k++) if (b[k] != '-') fb = k;
+    for (int k = len - 1; k >= 0 && la < 0; k--) if (a[k] != '-') la = k;
+    for (int k = len - 1; k >= 0 && lb < 0; k--) if (b[k] != '-') lb = k;
+    const int first = std::max(fa, fb), last = std::min(la, lb);
+    int id = 0;
+    for (int k = first; k <= last && k >= 0; k++) if (a[k] == b[k]) id++;
+    return fraction(id, last - first + 1);
+  }
+  if (protein) {
+    if (mode == SW_MODE_SWG_MPI) return fraction(r.similarity, r.length);
+    int sim = 0;
+    for (int k = 0; k < len; k++)
+      if (a[k] != '-' && b[k] != '-' && ctx->h_scores[(uint8_t)a[k]][(uint8_t)b[k]] > 0) sim++;
+    return fraction(sim, len);
+  }
+  return fraction(r.identity, r.length);
+}
+
+int sw_align_strings(sw_ctx* ctx, const int32_t* rows, const int32_t* cols, int32_t npairs, char* aln1,
+                     char* aln2, const int64_t* offsets, sw_pair_result* results) {
+  if (!ctx) return SW_E_ARG;
+  if (npairs < 0 || (npairs > 0 && (!rows || !cols || !aln1 || !aln2 || !offsets || !results)))
+    return fail(ctx, SW_E_ARG, "bad arguments");
+  if (!ctx->d_seq) return fail(ctx, SW_E_STATE, "no sequences uploaded");
+  // every pair's room: offsets[k + 1] - offsets[k] >= m + n (the longest alignment)
+  std::vector<int> len_m(npairs), len_n(npairs);
+  for (int32_t k = 0; k < npairs; k++) {
+    if (rows[k] < 0 || rows[k] >= ctx->nseq || cols[k] < 0 || cols[k] >= ctx->nseq)
+      return fail(ctx, SW_E_ARG, "pair outside the uploaded sequences");
+    len_m[k] = (int)(ctx->h_off[rows[k] + 1] - ctx->h_off[rows[k]]);
+    len_n[k] = (int)(ctx->h_off[cols[k] + 1] - ctx->h_off[cols[k]]);
+    if (offsets[k] < 0 || offsets[k + 1] - offsets[k] < (int64_t)len_m[k] + len_n[k])
+      return fail(ctx, SW_E_ARG, "offsets leave less than m + n characters for a pair");
+  }
+  cudaSetDevice(ctx->cfg.device);
+  const bool local = ctx->cfg.mode != SW_MODE_NW;
+  constexpr size_t kBudget = size_t(512) << 20;  // scratch of one batch of pairs
+  int throws = 0;
+  int32_t k0 = 0;
+  while (k0 < npairs) {
+    // the batch: pairs while their decision bytes and rows fit the budget (at least one pair)
+    const long row_ints = 2L * (ctx->maxlen + 1);
+    size_t dir_stride = 0;
+    int32_t k1 = k0;
+    while (k1 < npairs) {
+      const size_t st = std::max(dir_stride, (size_t)len_m[k1] * (size_t)len_n[k1]);
+      if (k1 > k0 && (st + row_ints * 4) * (size_t)(k1 - k0 + 1) > kBudget) break;
+      dir_stride = st;
+      k1++;
+    }
+    dir_stride = (dir_stride + 15) / 16 * 16;
+    const int32_t nb = k1 - k0;
+    const size_t chars = (size_t)(offsets[k1] - offsets[k0]);
+    std::vector<int64_t> rel(nb);
+    for (int32_t k = 0; k < nb; k++) rel[k] = offsets[k0 + k] - offsets[k0];
+    uint8_t* d_dirs = nullptr;
+    int* d_rows = nullptr;
+    int32_t* d_pairs = nullptr;
+    char* d_a = nullptr;
+    int64_t* d_rel = nullptr;
+    swg::TraceResult* d_res = nullptr;
+    auto release = [&]() {
+      cudaFree(d_dirs); cudaFree(d_rows); cudaFree(d_pairs); cudaFree(d_a); cudaFree(d_rel); cudaFree(d_res);
+    };
+    if (cudaMalloc(&d_dirs, std::max<size_t>(dir_stride * nb, 16)) != cudaSuccess ||
+        cudaMalloc(&d_rows, sizeof(int) * (size_t)row_ints * nb) != cudaSuccess ||
+        cudaMalloc(&d_pairs, sizeof(int32_t) * 2 * (size_t)nb) != cudaSuccess ||
+        cudaMalloc(&d_a, std::max<size_t>(2 * chars, 16)) != cudaSuccess ||
+        cudaMalloc(&d_rel, sizeof(int64_t) * (size_t)nb) != cudaSuccess ||
+        cudaMalloc(&d_res, sizeof(swg::TraceResult) * (size_t)nb) != cudaSuccess) {
+      release();
+      cudaGetLastError();
+      return fail(ctx, SW_E_OOM, "cudaMalloc alignment strings");
+    }
+    cudaError_t e = cudaMemcpyAsync(d_pairs, rows + k0, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_pairs + nb, cols + k0, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_rel, rel.data(), sizeof(int64_t) * nb, cudaMemcpyHostToDevice, ctx->stream);
+    swg::TraceJob J;
+    std::memset(&J, 0, sizeof(J));
+    J.seq = ctx->d_seq; J.off = ctx->d_off;
+    J.rows = d_pairs; J.cols = d_pairs + nb; J.npairs = nb;
+    J.scores = ctx->d_scores; J.o = ctx->o; J.e = ctx->e;
+    J.dirs = d_dirs; J.dir_stride = (long long)dir_stride;
+    J.vrow = d_rows; J.row_stride = row_ints;
+    J.aln1 = d_a; J.aln2 = d_a + chars; J.out_off = d_rel; J.out = d_res;
+    if (e == cudaSuccess) e = swg::launch_traceback(J, local, ctx->stream);
+    std::vector<swg::TraceResult> res(nb);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(aln1 + offsets[k0], d_a, chars, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(aln2 + offsets[k0], d_a + chars, chars, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(res.data(), d_res, sizeof(swg::TraceResult) * nb, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    release();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "alignment strings");
+    for (int32_t k = 0; k < nb; k++) {
+      const swg::TraceResult& r = res[k];
+      sw_pair_result& o = results[k0 + k];
+      o.score = r.valid ? (float)r.score : -INFINITY;
+      o.end1 = r.end1; o.end2 = r.end2; o.start1 = r.start1; o.start2 = r.start2;
+      o.identity = r.identity; o.similarity = r.similarity; o.gaps = r.gaps; o.length = r.length;
+      o.reserved = 0;
+      long long self1 = 0, self2 = 0;  // MinMaxNormScore's self scores of the two sequences
+      for (int64_t x = ctx->h_off[rows[k0 + k]]; x < ctx->h_off[rows[k0 + k] + 1]; x++) self1 += ctx->h_scores[ctx->h_seq[x]][ctx->h_seq[x]];
+      for (int64_t x = ctx->h_off[cols[k0 + k]]; x < ctx->h_off[cols[k0 + k] + 1]; x++) self2 += ctx->h_scores[ctx->h_seq[x]][ctx->h_seq[x]];
+      o.distance = traced_distance(ctx, aln1 + offsets[k0 + k], aln2 + offsets[k0 + k], r.length, r,
+                                   len_m[k0 + k], len_n[k0 + k], self1, self2, &throws);
+    }
+    k0 = k1;
+  }
+  if (throws) return fail(ctx, SW_E_THROWS, "JukesCantor: the reference throws for Log(Zero) on a pair of this call");
+  return SW_OK;
+}
+
 int sw_synchronize(sw_ctx* ctx) {
   if (!ctx) return SW_E_ARG;
   cudaSetDevice(ctx->cfg.device);

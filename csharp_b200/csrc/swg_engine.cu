@@ -75,6 +75,7 @@ struct EngineJob {
   int blk_mode, col_lo, col_hi;  // one block of the pair matrix: 1 diagonal, 2 off-diagonal (0: a job)
   int16_t* out;
   long long ld;
+  int mirror;               // also write (d, q): symmetric jobs and diagonal blocks, never other blocks
   uint32_t* scratch;        // per (CTA, warp) slot: maxcol * (kScrWords or kScrWordsNw) words
   int maxcol;               // longest database sequence
   int2* rerun;              // pairs to redo with 32-bit lanes
@@ -609,7 +610,7 @@ __device__ __forceinline__ void emit(const EngineJob& J, int q, int d, int16_t d
     return;
   }
   J.out[(long long)q * J.ld + d] = dist;
-  if (J.mode != kModeSwgMs) J.out[(long long)d * J.ld + q] = dist;
+  if (J.mirror) J.out[(long long)d * J.ld + q] = dist;
 }
 
 // What a kernel instantiation computes per pair.
@@ -1571,6 +1572,9 @@ class EngineImpl : public Engine {
     Base& B = *base_;
     cudaError_t e;
     pl.zeroes_diagonal = !key.block && P.mode != kModeSwgMs && P.nseq > 0 && key.row_lo == 0 && key.row_hi == P.nseq - 1;
+    // the mirrored entry (s2, s1) of each pair: a symmetric job's, or a diagonal block's (inside the
+    // block); an off-diagonal block's mirror lies outside the block and is the caller's to fill
+    const int mirror = key.block ? (key.block == 1 ? 1 : 0) : (P.mode != kModeSwgMs ? 1 : 0);
     if (pl.zeroes_diagonal)
       zero_diagonal_kernel<<<(P.nseq + 255) / 256, 256, 0, P.stream>>>(P.out, P.ld, P.nseq);
     set_int_kernel<<<1, 1, 0, P.stream>>>(pl.d_rerun_count, pl.big_count);
@@ -1587,7 +1591,7 @@ class EngineImpl : public Engine {
       J.mode = P.mode; J.ranks = P.ranks; J.nseq = P.nseq; J.protein = P.protein;
       J.rb_a = P.nseq / P.ranks; J.rb_b = P.nseq % P.ranks;
       J.blk_mode = key.block; J.col_lo = key.col_lo; J.col_hi = key.col_hi;
-      J.out = P.out; J.ld = P.ld;
+      J.out = P.out; J.ld = P.ld; J.mirror = mirror;
       J.scratch = B.d_scratch; J.maxcol = B.maxcol;
       J.rerun = pl.d_rerun; J.rerun_count = pl.d_rerun_count; J.rerun_cap = pl.rerun_cap;
       J.stats = pl.d_stats;
@@ -1625,7 +1629,7 @@ class EngineImpl : public Engine {
       X.seq = B.d_code; X.off = P.off;
       X.list = B.d_box; X.count = B.d_counts; X.win = B.d_boxwin;
       X.cls[0] = B.d_cls[0]; X.cls[1] = B.d_cls[1]; X.cls_count = B.d_counts + 2;
-      X.out = P.out; X.ld = P.ld; X.mirror = P.mode != kModeSwgMs;
+      X.out = P.out; X.ld = P.ld; X.mirror = mirror;
       X.lettab = B.d_lettab; X.flagtab = B.d_flagtab; X.A = B.alpha; X.o = P.o; X.e = P.e;
       X.maxlen = B.maxcol;
       X.rerun = pl.d_rerun; X.rerun_count = pl.d_rerun_count; X.rerun_cap = pl.rerun_cap;
@@ -1652,7 +1656,7 @@ class EngineImpl : public Engine {
     R.list = pl.d_rerun; R.list_count = pl.d_rerun_count;
     R.npairs = pl.rerun_cap;
     R.out = P.out; R.ld = P.ld; R.out_r0 = 0; R.out_c0 = 0;
-    R.mirror = P.mode != kModeSwgMs;
+    R.mirror = mirror;
     R.scores = P.scores; R.flags = P.flags;
     R.o = P.o; R.e = P.e; R.mode = P.mode; R.protein = P.protein;
     R.dist_fn = P.dist_fn; R.throws = P.throws;

@@ -97,6 +97,34 @@ cudaError_t launch_box_band(const BoxJob& J, int c, int sms, cudaStream_t st);
 // Warp per pair (reverse scan on 64-column shuffle windows, box DP as a 32-row wavefront).
 cudaError_t launch_box(const BoxJob& J, int grid, int block, cudaStream_t st);
 
+// Alignment strings of a list of pairs (swg_trace.cu): one thread per pair, a decision byte per
+// DP cell in dirs (dir_stride bytes per pair), two int rows of row_stride / 2 ints in vrow.
+struct TraceResult {
+  int score, valid, end1, end2, start1, start2;
+  int identity, similarity, gaps, length, diag, transitions, transversions;
+};
+
+struct TraceJob {
+  const uint8_t* seq;      // residues (the context's), offsets as uploaded
+  const int64_t* off;
+  const int32_t* rows;     // s1 index of pair k
+  const int32_t* cols;     // s2 index of pair k
+  long long npairs;
+  const int16_t* scores;   // [128 * 128]
+  int o, e;
+  uint8_t* dirs;
+  long long dir_stride;
+  int* vrow;
+  long row_stride;
+  char* aln1;              // aligned strings of pair k at aln1 + out_off[k] (and aln2)
+  char* aln2;
+  const int64_t* out_off;
+  TraceResult* out;
+};
+
+size_t trace_scratch_bytes(int m, int n);
+cudaError_t launch_traceback(const TraceJob& J, bool local, cudaStream_t st);
+
 size_t plain_carry_bytes(int mode, long threads, int maxlen, int dist_fn = 0);
 cudaError_t launch_plain_block(const PlainJob& J, int grid, int block, cudaStream_t st);
 size_t pair_carry_bytes(int n);

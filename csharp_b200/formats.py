@@ -111,3 +111,61 @@ def read_row_files(directory, prefix, ext, start, end, size, parts):
     for i in range(start, end + 1):
         out.append(np.fromfile(os.path.join(directory, f"{prefix}_{i}{ext}"), dtype="<i2").reshape(rr[i].Length, size))
     return np.concatenate(out, axis=0)
+
+
+def _kimura2(a, b):
+    """Alignment.ComputeKimuraDistance (Salsa.CoreTPL/Bio/Algorithms/Alignment.cs:254-302) over
+    aligned strings."""
+    import math
+    length = gaps = ts = tv = 0.0
+    for x, y in zip(a, b):
+        length += 1
+        if x != y:
+            if x == 45 or y == 45:
+                gaps += 1
+            elif (x, y) in ((65, 71), (71, 65), (67, 84), (84, 67)):
+                ts += 1
+            else:
+                tv += 1
+    with np.errstate(all="ignore"):
+        P = np.float64(ts) / np.float64(length - gaps)
+        Q = np.float64(tv) / np.float64(length - gaps)
+    eps = 4.9406564584124654e-324
+    if 1.0 - (2.0 * P + Q) <= eps or 1.0 - 2.0 * Q <= eps:
+        return 10.0
+    return float(-0.5 * math.log(1.0 - 2.0 * P - Q) - 0.25 * math.log(1.0 - 2.0 * Q))
+
+
+def _jukes_cantor(a, b):
+    """Alignment.ComputeJukesCantorDistance (Alignment.cs:314-348); the reference throws for
+    Log(Zero)."""
+    import math
+    length = gaps = diff = 0.0
+    for x, y in zip(a, b):
+        length += 1
+        if x != y:
+            if x == 45 or y == 45:
+                gaps += 1
+            else:
+                diff += 1
+    with np.errstate(all="ignore"):
+        d = 1.0 - (4.0 / 3.0) * (np.float64(diff) / np.float64(length - gaps))
+    if not d > 4.9406564584124654e-324:
+        raise ValueError("JukesCantor: Log(Zero)")
+    return -0.75 * math.log(d)
+
+
+def write_alignments(path, alignments, names1, names2):
+    """WriteAlignment (Salsa.SmithWatermanMPI/Program.cs:545-556) for each (aligned s1, aligned s2,
+    PairwiseAlignment) of Engine.align_strings: the two names with the Kimura2, JukesCantor and
+    PercentIdentity values (five decimals), the aligned strings, and an empty line."""
+    with open(path, "w") as f:
+        for (a, b, aln), n1, n2 in zip(alignments, names1, names2):
+            k = _kimura2(a, b)
+            jc = _jukes_cantor(a, b)
+            pi = float(np.float32(aln.PercentIdentity))
+            f.write(f">{n1} Kimera: {k:.5f}, JukesCantor: {jc:.5f}, PercentIdentity: {pi:.5f}\n")
+            f.write(a.decode() + "\n")
+            f.write(f">{n2} Kimera: {k:.5f}, JukesCantor: {jc:.5f}, PercentIdentity: {pi:.5f}\n")
+            f.write(b.decode() + "\n")
+            f.write("\n")

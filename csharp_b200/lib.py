@@ -30,7 +30,7 @@ EXPORTS = [
     "sw_write_full_matrix", "sw_write_ms_block", "sw_read_ms_block_dims", "sw_read_ms_block_values",
     "sw_measure_int_peak", "sw_set_option", "sw_compute_rank_blocks", "sw_query",
     "sw_compute_block_static", "sw_submit_job", "sw_poll", "sw_serve_stats", "sw_serve_drain",
-    "sw_autotune",
+    "sw_autotune", "sw_align_strings",
 ]
 
 

@@ -129,6 +129,18 @@ int sw_compute_block_device(sw_ctx* ctx, int32_t row_start, int32_t row_end, int
 int sw_align_pair(sw_ctx* ctx, const uint8_t* s1, int32_t m, const uint8_t* s2, int32_t n,
                   sw_pair_result* out);
 
+/* Alignment strings of explicit pairs: what the applications print with WriteAlignments on
+ * (Salsa.SmithWatermanMPI/Program.cs:223-246 and WriteAlignment :545-556;
+ * Salsa.SmithWatermanMS/Program.cs:682-702; Salsa.NeedlemanWunschTPL/Program.cs:725-735).  Pair k
+ * aligns s1 = sequence rows[k] with s2 = sequence cols[k] under the context's mode and penalties;
+ * aln1 / aln2 receive the aligned residues ('-' for a gap, as Sequence1 / Sequence2 hold them) at
+ * offset offsets[k], results[k].length characters each; offsets has npairs + 1 entries and
+ * offsets[k + 1] - offsets[k] must be at least m + n (the longest alignment).  results[k] holds the
+ * traceback's fields and the context's Int16 distance for the pair.  A GPU thread per pair keeps one
+ * decision byte per DP cell (pairs go in batches of at most 512 MB of such scratch); waits. */
+int sw_align_strings(sw_ctx* ctx, const int32_t* rows, const int32_t* cols, int32_t npairs, char* aln1,
+                     char* aln2, const int64_t* offsets, sw_pair_result* results);
+
 /* ---- whole-job engine ---------------------------------------------------------------------- */
 /* All blocks of one job in one call: the block driver MPIComputeLowerTriangularBlocked.Compute
  * (Salsa.SmithWatermanMPI/Program.cs:618-642) followed by its Scatter (:645-677), which fills

@@ -634,3 +634,51 @@ def test_ms_block_files_from_the_engine_match_the_oracle_run(cs, oracle_mod, tmp
     for f in names:
         assert (a / f).read_bytes() == (b / f).read_bytes(), f
     eng.close()
+
+
+@pytest.mark.parametrize("mode,matrix,o,e,dist_fn", [(0, "EDNAFULL", 16, 4, 0), (1, "EDNAFULL", 16, 4, 0),
+                                                     (2, "EDNAFULL", 16, 4, 0), (0, "BLOSUM62", 10, 1, 0),
+                                                     (2, "BLOSUM62", 10, 1, 0), (0, "EDNAFULL", 5, 2, 1),
+                                                     (1, "EDNAFULL", 16, 4, 3), (2, "EDNAFULL", 16, 4, 3)])
+def test_alignment_strings_match_oracle_traceback(cs, oracle_mod, mode, matrix, o, e, dist_fn):
+    """sw_align_strings against the oracle's traceback (SW: the NAligner restatement, NW: the NW
+    restatement): the aligned strings, the counts and the context's distance (the engine's)."""
+    from csharp_b200 import synth
+    rng = np.random.default_rng(70 + mode)
+    if matrix == "BLOSUM62":
+        seqs = [s.tobytes() for s in synth.protein_family(30, 3, rng.integers(1, 250, 30), 71, cs.ScoringMatrix.Load("BLOSUM62").Scores)]
+    else:
+        seqs = [s.tobytes() for s in synth.dna_family(30, 3, rng.integers(1, 250, 30), seed=71)]
+    seqs += [b"A" if matrix == "EDNAFULL" else b"W", b""]
+    atype = cs.PROTEIN if matrix == "BLOSUM62" else cs.NUCLEIC
+    sm = cs.ScoringMatrix.Load(matrix)
+    eng = cs.Engine(sm, o, e, mode=mode, alignment_type=atype, distance_fn=dist_fn).upload(seqs)
+    full, _, _ = eng.all_pairs(1)
+    N = len(seqs)
+    pairs = [(i, j) for i in range(N) for j in range(i)][::3] + [(N - 2, 0), (N - 1, 3), (5, 5)]
+    got = eng.align_strings(pairs)
+    sc = sm.Scores[:127, :127].astype(np.float32)
+    for (i, j), (a, b, aln) in zip(pairs, got):
+        if mode == 2:
+            want = oracle_mod.nw_align(seqs[i], seqs[j], sc, float(o), float(e))
+        else:
+            want = oracle_mod.align(seqs[i], seqs[j], sc, float(o), float(e), with_strings=True)
+            assert (aln.Identity, aln.Similarity, aln.Gaps, aln.Start1, aln.Start2) == \
+                (want["identity"], want["similarity"], want["gaps"], want["start1"], want["start2"])
+        assert (a, b) == (want["aln1"], want["aln2"]), (i, j)
+        assert aln.Length == len(a)
+        if i != j or mode == 1:
+            assert aln.Distance == full[i, j], (i, j)
+    eng.close()
+
+
+def test_write_alignments_format(cs, tmp_path):
+    from csharp_b200.formats import write_alignments
+    seqs = [b"ACGTACGTTTGA", b"ACGTTCGTTGA", b"GGGACGT"]
+    eng = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4).upload(seqs)
+    got = eng.align_strings([(1, 0), (2, 1)])
+    write_alignments(tmp_path / "a.txt", got, ["s1", "s2"], ["s0", "s1"])
+    lines = (tmp_path / "a.txt").read_text().split("\n")
+    assert lines[0].startswith(">s1 Kimera: ") and ", JukesCantor: " in lines[0] and ", PercentIdentity: " in lines[0]
+    assert lines[1] == got[0][0].decode() and lines[3] == got[0][1].decode() and lines[4] == ""
+    eng.close()
