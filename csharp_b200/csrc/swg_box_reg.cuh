@@ -121,13 +121,14 @@ struct RegBox {
 enum { kRegScanOk = 0, kRegScanWide = 1, kRegScanNone = 2 };
 
 // Reverse scans of pairs list[first], list[first + stride], ... below np, each with its window
-// win + p * kRegWinWords.  seq + off[k] are the residue codes of sequence k (0..A1-2; A1-1 is the
-// padding code); sc[a * A1 + b] the substitution score of codes a and b (the padding code's row
-// and column kRegPadScore).  emit(p, rec, outcome, box) receives each pair's outcome.
+// win + p * kRegWinWords.  aseq + aoff[k] are the residues of s1 = sequence k (a row index of sc),
+// seq + off[k] the codes of s2 = sequence k (0..A1-2; A1-1 is the padding code); sc[a * A1 + b]
+// the substitution score of s1 residue a and s2 code b (the padding code's column
+// kRegPadScore).  emit(p, rec, outcome, box) receives each pair's outcome.
 template <class ScT, class Emit>
 SWG_REG_FN void reg_scan_run(const int4* list, const uint32_t* win, long long first, long long np,
-                             long long stride, const uint8_t* seq, const int64_t* off, const ScT* sc,
-                             int A1, int o, int e, Emit& emit) {
+                             long long stride, const uint8_t* aseq, const int64_t* aoff, const uint8_t* seq,
+                             const int64_t* off, const ScT* sc, int A1, int o, int e, Emit& emit) {
   constexpr int W = kRegWin;
   constexpr int D = kRegDead;
   const uint32_t pad = (uint32_t)(A1 - 1);
@@ -163,7 +164,7 @@ SWG_REG_FN void reg_scan_run(const int4* list, const uint32_t* win, long long fi
       trest = (rec.z >> 16) & 0xFFFF;
       ie = (int)((uint32_t)rec.w >> 16);
       je = rec.w & 0xFFFF;
-      a = seq + off[rec.x];
+      a = aseq + aoff[rec.x];
       b = seq + off[rec.y];
       wp = win + p * kRegWinWords;
 #pragma unroll
@@ -285,13 +286,15 @@ SWG_REG_FN void reg_scan_run(const int4* list, const uint32_t* win, long long fi
 // Band DPs of the records list[idx[k * step]] for k = first, first + stride, ... below np (band
 // width at most B); the scan's result of record r, (ci, cj, blo, bhi), is the first four words of
 // its window win + r * kRegWinWords (the scan writes it there once the thresholds are used).
-// scf[a * A1 + b] = S(a, b) << 8 | counted flag.  emit(r, rec, ok, counters) receives each pair's
+// scf[a * A1 + b] = S(a, b) << 8 | counted flag (a: an s1 residue of aseq, b: an s2 code of seq).
+// emit(r, rec, ok, counters) receives each pair's
 // outcome: ok with counters = aligned columns << 16 | counted columns, or not ok (the value at
 // (ie, je) was not S).
 template <int B, class Emit>
 SWG_REG_FN void reg_band_run(const int* idx, long long step, long long first, long long np, long long stride,
-                             const int4* list, const uint32_t* win, const uint8_t* seq, const int64_t* off,
-                             const int* scf, int A1, int o, int e, Emit& emit) {
+                             const int4* list, const uint32_t* win, const uint8_t* aseq, const int64_t* aoff,
+                             const uint8_t* seq, const int64_t* off, const int* scf, int A1, int o, int e,
+                             Emit& emit) {
   constexpr int D = kRegDead;
   const uint32_t pad = (uint32_t)(A1 - 1);
   int V[B], G[B];
@@ -333,7 +336,7 @@ SWG_REG_FN void reg_band_run(const int* idx, long long step, long long first, lo
       cj = bx.y;
       blo = bx.z;
       bhi = bx.w;
-      a = seq + off[rec.x];
+      a = aseq + aoff[rec.x];
       b = seq + off[rec.y];
 #pragma unroll
       for (int k = 0; k < B; k++) {  // the row above the box: zero boundary

@@ -1706,8 +1706,10 @@ constexpr int kQueryChunk = 256;
 class QueryRunnerImpl : public QueryRunner {
  public:
   ~QueryRunnerImpl() override {
-    cudaFree(d_qtab_); cudaFree(d_qflag_);
+    cudaFree(d_qtab_); cudaFree(d_qflag_); cudaFree(d_qbsc_); cudaFree(d_qbscf_);
     for (auto& w : wb_) {
+      cudaFree(w.d_box); cudaFree(w.d_win); cudaFree(w.d_cls[0]); cudaFree(w.d_cls[1]); cudaFree(w.d_counts);
+      cudaFree(w.d_rowbuf);
       cudaFree(w.d_items); cudaFree(w.d_counters); cudaFree(w.d_stats); cudaFree(w.d_rerun);
       cudaFree(w.d_rerun_count); cudaFreeHost(w.h_items); cudaFreeHost(w.h_rerun); cudaFree(w.d_scratch);
       if (w.fork) cudaEventDestroy(w.fork);
@@ -1774,6 +1776,22 @@ class QueryRunnerImpl : public QueryRunner {
       }
     if ((rc = upload_vec(&d_qtab_, qtab, msg, "query score table"))) return rc;
     if ((rc = upload_vec(&d_qflag_, qflag, msg, "query flag table"))) return rc;
+    // two passes where the engine uses them (the same rule): the score-only kernels, then the box
+    // step with a table row per query residue byte
+    two_ = P.mode != kModeNw && std::min(P.o, P.e) >= 2 && P.o >= 3 * max_s_ && P.e >= 3;
+    if (two_) {
+      std::vector<int32_t> qsc((size_t)128 * A1), qscf((size_t)128 * A1);
+      for (int x = 0; x < 128; x++)
+        for (int c = 0; c < A1; c++) {
+          const bool pad = x == kPadCode || c == A;
+          const int v = pad ? kRegPadScore : P.h_scores[x * 128 + B_.letters[c]];
+          const uint32_t f = pad ? 0u : (P.h_flags[x * 128 + B_.letters[c]] & kFlagCount);
+          qsc[(size_t)x * A1 + c] = v;
+          qscf[(size_t)x * A1 + c] = (int32_t)(((uint32_t)v << 8) | f);
+        }
+      if ((rc = upload_vec(&d_qbsc_, qsc, msg, "query box table"))) return rc;
+      if ((rc = upload_vec(&d_qbscf_, qscf, msg, "query band table"))) return rc;
+    }
     return SW_OK;
   }
 
@@ -1848,20 +1866,25 @@ class QueryRunnerImpl : public QueryRunner {
       ls.push_back(L);
     }
     std::stable_sort(ls.begin(), ls.end(), [&](const Launch& x, const Launch& y) { return bin_cost[x.b] > bin_cost[y.b]; });
-    // per-bin launch shape and scratch (bins run concurrently, each multi-pass bin has its own)
+    // per-bin launch shape and scratch (bins run concurrently, each multi-pass bin has its own;
+    // two passes: each bin its own rows' bounds too)
     const int A = B_.alpha;
-    std::vector<size_t> smem(ls.size()), scr_off(ls.size());
+    const int kind = two_ ? kKindScore : kKindSw;
+    std::vector<size_t> smem(ls.size()), scr_off(ls.size()), row_off(ls.size());
     std::vector<int> grid(ls.size());
-    size_t scr_words = 0;
+    size_t scr_words = 0, row_words = 0;
     for (size_t x = 0; x < ls.size(); x++) {
-      smem[x] = engine_smem(A, ls[x].mpad, B_.maxcol, ls[x].K);
+      smem[x] = engine_smem(A, ls[x].mpad, B_.maxcol, ls[x].K, kind);
       if (smem[x] > 227 * 1024) { *msg = "query profile exceeds shared memory"; return SW_E_UNSUPPORTED; }
-      if (allow_smem_k(ls[x].K, A, kKindSw, smem[x]) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
-      const int occ = std::max(1, occupancy_k(ls[x].K, A, kKindSw, smem[x]));
+      if (allow_smem_k(ls[x].K, A, kind, smem[x]) != cudaSuccess) { cudaGetLastError(); *msg = "shared memory opt-in"; return SW_E_CUDA; }
+      const int occ = std::max(1, occupancy_k(ls[x].K, A, kind, smem[x]));
       grid[x] = std::min(P_.sms * occ, ls[x].count);
       scr_off[x] = scr_words;
-      if (ls[x].max_passes > 1) scr_words += (size_t)grid[x] * warps_of(ls[x].K) * B_.maxcol * kScrWords;
+      if (ls[x].max_passes > 1) scr_words += (size_t)grid[x] * warps_of(ls[x].K, kind) * B_.maxcol * kScrWords;
+      row_off[x] = row_words;
+      if (two_) row_words += (size_t)grid[x] * warps_of(ls[x].K, kind) * ls[x].mpad;
     }
+    if (two_ && (rc = grow_box(W, std::max<size_t>((size_t)pairs16, 1), std::max<size_t>(row_words * 4, 16), msg))) return rc;
     if (scr_words * 4 > W.scratch_bytes) {
       // the earlier wave of this buffer is done; the other buffer's wave may run (own scratch)
       cudaFree(W.d_scratch);
@@ -1874,7 +1897,8 @@ class QueryRunnerImpl : public QueryRunner {
     if (n16 && (e = cudaMemcpyAsync(W.d_items, W.h_items, n16 * sizeof(int4), cudaMemcpyHostToDevice, st)) != cudaSuccess) return cuda_err(e, msg);
     if (big && (e = cudaMemcpyAsync(W.d_rerun, W.h_rerun, big * sizeof(int2), cudaMemcpyHostToDevice, st)) != cudaSuccess) return cuda_err(e, msg);
     if ((e = cudaMemsetAsync(W.d_counters, 0, sizeof(int) * kNumK, st)) != cudaSuccess) return cuda_err(e, msg);
-    if ((e = cudaMemsetAsync(W.d_stats, 0, sizeof(unsigned long long) * 4, st)) != cudaSuccess) return cuda_err(e, msg);
+    if ((e = cudaMemsetAsync(W.d_stats, 0, sizeof(unsigned long long) * kNumStats, st)) != cudaSuccess) return cuda_err(e, msg);
+    if (two_ && (e = cudaMemsetAsync(W.d_counts, 0, sizeof(int) * 8, st)) != cudaSuccess) return cuda_err(e, msg);
     set_int_kernel<<<1, 1, 0, st>>>(W.d_rerun_count, (int)big);
     if (!ls.empty()) {
       EngineJob J;
@@ -1887,6 +1911,10 @@ class QueryRunnerImpl : public QueryRunner {
       J.stats = W.d_stats;
       J.qmode = 1; J.qseq = T.qseq; J.qoff = T.qoff; J.qlen = T.qlen; J.qout = T.qout;
       J.qtab = d_qtab_; J.qflag = d_qflag_;
+      if (two_) {
+        J.box = W.d_box; J.boxwin = W.d_win; J.box_count = W.d_counts;
+        J.box_cap = (int)std::min<size_t>(W.box_cap, 0x7fffffff);
+      }
       const bool fork = ls.size() > 1;
       if (fork && (e = cudaEventRecord(W.fork, st)) != cudaSuccess) return cuda_err(e, msg);
       for (size_t x = 0; x < ls.size(); x++) {
@@ -1897,12 +1925,31 @@ class QueryRunnerImpl : public QueryRunner {
         J.counter = W.d_counters + ls[x].b;
         J.mpad = ls[x].mpad;
         J.scratch = W.d_scratch + scr_off[x];
-        if ((e = launch_engine_k(ls[x].K, kKindSw, J, grid[x], smem[x], s2)) != cudaSuccess) return cuda_err(e, msg);
+        J.rowbuf = two_ ? W.d_rowbuf + row_off[x] : nullptr;
+        if ((e = launch_engine_k(ls[x].K, kind, J, grid[x], smem[x], s2)) != cudaSuccess) return cuda_err(e, msg);
         if (fork) {
           if ((e = cudaEventRecord(W.join[x], s2)) != cudaSuccess) return cuda_err(e, msg);
           if ((e = cudaStreamWaitEvent(st, W.join[x], 0)) != cudaSuccess) return cuda_err(e, msg);
         }
       }
+    }
+    if (two_ && !ls.empty()) {
+      // the box step of the wave's score records: query residues against database codes, distances
+      // to the query rows; pairs it cannot finish go to the 32-bit lanes below
+      BoxJob X;
+      std::memset(&X, 0, sizeof(X));
+      X.seq = B_.d_code; X.off = P_.off;
+      X.qseq = T.qseq; X.qoff = T.qoff; X.qout = T.qout; X.qsc = d_qbsc_; X.qscf = d_qbscf_;
+      X.list = W.d_box; X.count = W.d_counts; X.win = W.d_win;
+      X.cls[0] = W.d_cls[0]; X.cls[1] = W.d_cls[1]; X.cls_count = W.d_counts + 2;
+      X.A = A; X.o = P_.o; X.e = P_.e; X.maxlen = B_.maxcol;
+      X.rerun = W.d_rerun; X.rerun_count = W.d_rerun_count; X.rerun_cap = (int)rerun_cap;
+      X.stats = W.d_stats;
+      X.list_cap = (long long)W.box_cap;
+      X.spill_count = W.d_counts + 1;  // no warp box kernel here: spill_cap 0 sends them on
+      if ((e = launch_box_scan(X, P_.sms, st)) != cudaSuccess) return cuda_err(e, msg);
+      for (int c = 0; c < 4; c++)
+        if ((e = launch_box_band(X, c, P_.sms, st)) != cudaSuccess) return cuda_err(e, msg);
     }
     // 32-bit lanes: pairs routed there by the static guard and 16-bit lanes that tripped
     PlainJob R;
@@ -1943,7 +1990,42 @@ class QueryRunnerImpl : public QueryRunner {
     bool plain_used = false;
     cudaStream_t side[kNumK] = {};
     cudaEvent_t join[kNumK] = {};
+    // two passes: the score kernels' box records, threshold windows and rows' bounds, the band
+    // classes, and the counts ([0] records, [1] spilled, [2..5] classes)
+    int4* d_box = nullptr;
+    uint32_t* d_win = nullptr;
+    int* d_cls[2] = {nullptr, nullptr};
+    int* d_counts = nullptr;
+    size_t box_cap = 0;
+    uint32_t* d_rowbuf = nullptr;
+    size_t rowbuf_bytes = 0;
   };
+
+  // Two-pass buffers of a wave buffer for `pairs` box records and `rowbuf` bytes of rows' bounds.
+  int grow_box(WaveBuf& W, size_t pairs, size_t rowbuf, std::string* msg) {
+    if (!W.d_counts && cudaMalloc(&W.d_counts, sizeof(int) * 8) != cudaSuccess) {
+      cudaGetLastError(); W.d_counts = nullptr; *msg = "cudaMalloc wave box counts"; return SW_E_OOM;
+    }
+    if (pairs > W.box_cap) {
+      const size_t cap = std::max(pairs, W.box_cap * 2);
+      cudaFree(W.d_box); cudaFree(W.d_win); cudaFree(W.d_cls[0]); cudaFree(W.d_cls[1]);
+      W.d_box = nullptr; W.d_win = nullptr; W.d_cls[0] = W.d_cls[1] = nullptr; W.box_cap = 0;
+      if (cudaMalloc(&W.d_box, sizeof(int4) * cap) != cudaSuccess ||
+          cudaMalloc(&W.d_win, sizeof(uint32_t) * kRegWinWords * cap) != cudaSuccess ||
+          cudaMalloc(&W.d_cls[0], sizeof(int) * cap) != cudaSuccess ||
+          cudaMalloc(&W.d_cls[1], sizeof(int) * cap) != cudaSuccess) {
+        cudaGetLastError(); *msg = "cudaMalloc wave box lists"; return SW_E_OOM;
+      }
+      W.box_cap = cap;
+    }
+    if (rowbuf > W.rowbuf_bytes) {
+      cudaFree(W.d_rowbuf);
+      W.d_rowbuf = nullptr; W.rowbuf_bytes = 0;
+      if (cudaMalloc(&W.d_rowbuf, rowbuf) != cudaSuccess) { cudaGetLastError(); *msg = "cudaMalloc wave row bounds"; return SW_E_OOM; }
+      W.rowbuf_bytes = rowbuf;
+    }
+    return SW_OK;
+  }
 
   static int cuda_err(cudaError_t e, std::string* msg) {
     *msg = std::string("query wave: ") + cudaGetErrorString(e);
@@ -1955,7 +2037,7 @@ class QueryRunnerImpl : public QueryRunner {
     if (!W.d_counters) {
       if (cudaMalloc(&W.d_counters, sizeof(int) * kNumK) != cudaSuccess ||
           cudaMalloc(&W.d_rerun_count, sizeof(int)) != cudaSuccess ||
-          cudaMalloc(&W.d_stats, sizeof(unsigned long long) * 4) != cudaSuccess) {
+          cudaMalloc(&W.d_stats, sizeof(unsigned long long) * kNumStats) != cudaSuccess) {
         cudaGetLastError(); *msg = "cudaMalloc wave counters"; return SW_E_OOM;
       }
     }
@@ -1992,6 +2074,9 @@ class QueryRunnerImpl : public QueryRunner {
   std::vector<int64_t> chunk_sum_;
   int32_t* d_qtab_ = nullptr;
   uint32_t* d_qflag_ = nullptr;
+  bool two_ = false;          // SW-Gotoh with gap costs that suit the box step: two passes
+  int32_t* d_qbsc_ = nullptr;   // [128 * (A+1)] box step tables (query residue byte x database code)
+  int32_t* d_qbscf_ = nullptr;
   WaveBuf wb_[2];
 };
 

@@ -66,6 +66,14 @@ struct BoxJob {
   int* cls[2];             // band classes 0..3 (width <= 8, 16, 24, 32): list indices, classes 0 / 2
                            // from the front of cls[0] / cls[1], classes 1 / 3 from the back
   int* cls_count;          // [4]
+  // query mode (serving): s1 = query slot q of qseq / qoff (raw residue bytes), the tables have a
+  // row per residue byte (qsc: S; qscf: S << 8 | counted flag, kRegPadScore in the pad column),
+  // distances go to qout[q][d]
+  const uint8_t* qseq;
+  const int64_t* qoff;
+  int16_t* const* qout;
+  const int* qsc;
+  const int* qscf;
   int16_t* out;
   long long ld;
   int mirror;

@@ -444,12 +444,15 @@ __device__ __forceinline__ void box_give_up(const BoxJob& J, int q, int d) {
   atomicAdd(J.stats + 1, ~0ull);  // no longer finished in 16-bit lanes
 }
 
+// Rows of the box tables: one per residue byte of s1 in query mode, else one per code.
+constexpr int kBoxTabRows = 128;
+
 __global__ void __launch_bounds__(kRegThreads) box_scan_kernel(BoxJob J) {
-  __shared__ int sc[kBoxMaxA1 * kBoxMaxA1];
+  __shared__ int sc[kBoxTabRows * kBoxMaxA1];
   const int A1 = J.A + 1;
-  for (int k = threadIdx.x; k < A1 * A1; k += blockDim.x) {
+  for (int k = threadIdx.x; k < (J.qseq ? kBoxTabRows : A1) * A1; k += blockDim.x) {
     const int a = k / A1, c = k - a * A1;
-    sc[k] = (a == J.A || c == J.A) ? kRegPadScore : J.lettab[k] - J.o;
+    sc[k] = J.qseq ? J.qsc[k] : (a == J.A || c == J.A) ? kRegPadScore : J.lettab[k] - J.o;
   }
   __syncthreads();
   const long long np = min((long long)*J.count, J.list_cap);
@@ -464,7 +467,7 @@ __global__ void __launch_bounds__(kRegThreads) box_scan_kernel(BoxJob J) {
       return;
     }
     // a wider window or band: the warp box kernel (its 64-column windows), else the 32-bit lanes
-    const int w = atomicAdd(J.spill_count, 1);
+    const int w = J.spill_cap > 0 ? atomicAdd(J.spill_count, 1) : 0;
     if (w < J.spill_cap) {
       J.spill[w] = rec;
       atomicAdd(J.stats + 4, 1ull);
@@ -473,16 +476,18 @@ __global__ void __launch_bounds__(kRegThreads) box_scan_kernel(BoxJob J) {
     box_give_up(J, rec.x, rec.y);
   };
   reg_scan_run(J.list, J.win, (long long)blockIdx.x * kRegThreads + threadIdx.x, np,
-               (long long)gridDim.x * kRegThreads, J.seq, J.off, sc, A1, J.o, J.e, emit);
+               (long long)gridDim.x * kRegThreads, J.qseq ? J.qseq : J.seq, J.qseq ? J.qoff : J.off, J.seq,
+               J.off, sc, A1, J.o, J.e, emit);
 }
 
 template <int B>
 __global__ void __launch_bounds__(kRegThreads) box_band_kernel(BoxJob J, int c) {
-  __shared__ int scf[kBoxMaxA1 * kBoxMaxA1];
+  __shared__ int scf[kBoxTabRows * kBoxMaxA1];
   const int A1 = J.A + 1;
-  for (int k = threadIdx.x; k < A1 * A1; k += blockDim.x) {
+  for (int k = threadIdx.x; k < (J.qseq ? kBoxTabRows : A1) * A1; k += blockDim.x) {
     const int a = k / A1, x = k - a * A1;
-    scf[k] = (a == J.A || x == J.A) ? (int)((uint32_t)kRegPadScore << 8)
+    scf[k] = J.qseq ? J.qscf[k]
+           : (a == J.A || x == J.A) ? (int)((uint32_t)kRegPadScore << 8)
                                     : (int)(((uint32_t)(J.lettab[k] - J.o) << 8) | (J.flagtab[k] & kFlagCount));
   }
   __syncthreads();
@@ -494,11 +499,16 @@ __global__ void __launch_bounds__(kRegThreads) box_band_kernel(BoxJob J, int c) 
       return;
     }
     const int16_t dist = fraction_distance((int)(cnt & 0xFFFFu), (int)(cnt >> 16));
+    if (J.qout) {
+      J.qout[rec.x][rec.y] = dist;
+      return;
+    }
     J.out[(long long)rec.x * J.ld + rec.y] = dist;
     if (J.mirror) J.out[(long long)rec.y * J.ld + rec.x] = dist;
   };
   reg_band_run<B>(idx, (c & 1) ? -1 : 1, (long long)blockIdx.x * kRegThreads + threadIdx.x, np,
-                  (long long)gridDim.x * kRegThreads, J.list, J.win, J.seq, J.off, scf, A1, J.o, J.e, emit);
+                  (long long)gridDim.x * kRegThreads, J.list, J.win, J.qseq ? J.qseq : J.seq,
+                  J.qseq ? J.qoff : J.off, J.seq, J.off, scf, A1, J.o, J.e, emit);
 }
 
 // Resident CTAs per SM of a kernel with kRegThreads threads (its registers decide), looked up once.

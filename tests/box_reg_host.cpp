@@ -147,7 +147,7 @@ extern "C" int box_reg_run(const uint8_t* seqs, const int64_t* off, const int32_
       }
       cls[bw <= 8 ? 0 : bw <= 16 ? 1 : bw <= 24 ? 2 : 3].push_back((int)p);
     };
-    swg::reg_scan_run(list.data(), win.data(), t, nl, threads, seqs, off, sc.data(), A1, o, e, emit);
+    swg::reg_scan_run(list.data(), win.data(), t, nl, threads, seqs, off, seqs, off, sc.data(), A1, o, e, emit);
   }
   for (long p = 0; p < nl; p++)
     if (!seen[p]) dup = 1;
@@ -165,10 +165,10 @@ extern "C" int box_reg_run(const uint8_t* seqs, const int64_t* off, const int32_
         counters[src[qi]] = cnt;
       };
       switch (c) {
-        case 0: swg::reg_band_run<8>(cls[c].data(), 1, t, nc, threads, list.data(), win.data(), seqs, off, scf.data(), A1, o, e, emit); break;
-        case 1: swg::reg_band_run<16>(cls[c].data(), 1, t, nc, threads, list.data(), win.data(), seqs, off, scf.data(), A1, o, e, emit); break;
-        case 2: swg::reg_band_run<24>(cls[c].data(), 1, t, nc, threads, list.data(), win.data(), seqs, off, scf.data(), A1, o, e, emit); break;
-        default: swg::reg_band_run<32>(cls[c].data(), 1, t, nc, threads, list.data(), win.data(), seqs, off, scf.data(), A1, o, e, emit); break;
+        case 0: swg::reg_band_run<8>(cls[c].data(), 1, t, nc, threads, list.data(), win.data(), seqs, off, seqs, off, scf.data(), A1, o, e, emit); break;
+        case 1: swg::reg_band_run<16>(cls[c].data(), 1, t, nc, threads, list.data(), win.data(), seqs, off, seqs, off, scf.data(), A1, o, e, emit); break;
+        case 2: swg::reg_band_run<24>(cls[c].data(), 1, t, nc, threads, list.data(), win.data(), seqs, off, seqs, off, scf.data(), A1, o, e, emit); break;
+        default: swg::reg_band_run<32>(cls[c].data(), 1, t, nc, threads, list.data(), win.data(), seqs, off, seqs, off, scf.data(), A1, o, e, emit); break;
       }
     }
   }

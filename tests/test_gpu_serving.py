@@ -95,7 +95,7 @@ def test_admission_waits_for_memory_and_slots(cs, oracle_mod):
         eng.submit(_dna(70, 60, 10, 20))  # more queries than slots
 
 
-def test_protein_database_runs_on_32bit_lanes(cs, oracle_mod):
+def test_protein_database_matches_oracle(cs, oracle_mod):
     from csharp_b200 import synth
     sc = cs.ScoringMatrix.Load("BLOSUM62").Scores
     rng = np.random.default_rng(71)
