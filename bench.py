@@ -517,7 +517,9 @@ def main():
                          "engine_options": dict(ENGINE_OPTIONS) or "defaults",
                          "rows_per_lane_costs": (tuned if tuned and any(tuned.values()) else
                                                  "built-in" + (" (kept by the autotuner)" if tuned else ""))},
-              "gpu_launches": int(launches), "clocks": clk.summary()}
+              "gpu_launches": int(launches), "clocks": clk.summary(),
+              "engine_counters_last_step": {k: eng.query(k) for k in ("pairs", "lane16_pairs", "tripped", "box_spilled",
+                                                                      "box_fallbacks")}}
 
     if rank == 0:
         peak_max, peak_add = cs.measure_int_peak(local)

@@ -535,8 +535,9 @@ def test_reupload_of_same_shaped_set_keeps_plans_and_uses_new_residues(cs):
     fresh = cs.Engine(m, 16, 4).upload(b)
     want_b, _, _ = fresh.all_pairs(3)
     np.testing.assert_array_equal(got_b, want_b)
+    want_blk, _ = fresh.compute_block(0, 149, 0, 149, True)  # s1 = the larger index, like the call above
     off = ~np.eye(150, dtype=bool)
-    np.testing.assert_array_equal(blk_b[off], want_b[:150, :150][off])
+    np.testing.assert_array_equal(blk_b[off], want_blk[off])
     assert not np.array_equal(got_a, got_b)
     eng.close()
     fresh.close()
