@@ -9,13 +9,14 @@ block and the checkerboard half of its off-diagonal blocks through a block handl
 NVLink between GPUs); the handler is the engine's ``compute_block`` or any callable with the
 reference's signature.
 
-``distributed_all_pairs`` is the one-process-per-GPU path: each rank runs the engine over the
-pairs its rank aligns (sw_compute_rank_blocks), the ranks' disjoint entries are summed with one
-all-reduce (bytes, so Int16 needs no NCCL type), and every rank ends with the full matrix.
+``distributed_all_pairs`` is the one-process-per-GPU path: each rank runs the engine over its
+share -- contiguous rows cut at equal DP cells (``balanced_row_ranges``), or the reference's
+checkerboard -- and the ranks' row slabs are merged by one all-gather or one gather to a writer
+(``merge_row_slabs``), the entries nobody sent following from who computed which pair.
 """
 import numpy as np
 
-from .core import Block, block_is_computed, block_partition, range_partition
+from .core import SWG_MS, Block, block_is_computed, block_partition, range_partition
 
 
 class PartialMatrix:
@@ -124,15 +125,99 @@ class MPIComputeLowerTriangularBlocked:
         return full
 
 
-def distributed_all_pairs(engine, out, rank, world_size, group=None):
-    """One process per GPU: this rank's pairs into `out` (a zeroed N x N int16 CUDA tensor),
-    then one byte all-reduce so every rank holds the full matrix.  Returns this rank's pairs."""
+def balanced_row_ranges(lengths, world):
+    """Contiguous query-row ranges of about equal DP cells, one per rank: with s1 = the larger
+    index (a 1-rank run's orientation), row q aligns every d < q and costs m_q * sum of n_d over
+    d < q.  Rank r takes the rows whose cumulative cost ends in (r / world, (r + 1) / world] of
+    the total (inclusive (start, end); end < start: no rows)."""
+    lens = np.asarray(lengths, dtype=np.float64)
+    n = len(lens)
+    before = np.concatenate([[0.0], np.cumsum(lens)[:-1]]) if n else np.zeros(0)
+    cum = np.cumsum(lens * before)
+    total = float(cum[-1]) if n else 0.0
+    cuts = [0]
+    for r in range(1, world):
+        cuts.append(max(cuts[-1], int(np.searchsorted(cum, total * r / world, side="left")) + 1 if n else 0))
+    cuts.append(n)
+    cuts = [min(c, n) for c in cuts]
+    return [(cuts[r], cuts[r + 1] - 1) for r in range(world)]
+
+
+def checkerboard_row_ranges(n, world):
+    return [(r.StartIndex, r.EndIndex) for r in range_partition(n, world)]
+
+
+def merge_row_slabs(out, rank, world, row_ranges, scheme, group=None, dst=None):
+    """Merges the ranks' row slabs of an N x N Int16 tensor into the full matrix on every rank (dst
+    None: one all-gather) or on rank dst (one gather; the writer of WriteFullMatrixOnRank0).
+
+    Rank r contributes only its rows row_ranges[r]: each rank sends 1/world of the matrix instead
+    of the whole matrix a byte all-reduce moves.  The other entries follow from who computed what:
+    "checkerboard" (the reference's P-rank run, Program.cs:618-677): a block (r, c) that rank r did
+    not compute is the transpose of block (c, r) (Scatter); "balanced" (balanced_row_ranges): each
+    pair sits below the diagonal in its s1 row and the upper triangle is its transpose.  Returns
+    True where the full matrix is now in `out`."""
     import torch
     import torch.distributed as dist
+    N = out.shape[0]
+    rows = [max(0, hi - lo + 1) for lo, hi in row_ranges]
+    maxrows = max(max(rows), 1)
+    lo, hi = row_ranges[rank]
+    buf = torch.zeros((maxrows, N), dtype=torch.int16, device=out.device)
+    if rows[rank]:
+        buf[:rows[rank]] = out[lo:hi + 1]
+    if world > 1:
+        if dst is None:
+            parts = [torch.empty_like(buf) for _ in range(world)]
+            dist.all_gather([g.view(torch.uint8) for g in parts], buf.view(torch.uint8), group=group)
+        else:  # bytes: neither gloo nor NCCL has an Int16 type
+            parts = [torch.empty_like(buf) for _ in range(world)] if rank == dst else None
+            dist.gather(buf.view(torch.uint8), [g.view(torch.uint8) for g in parts] if parts else None, dst=dst,
+                        group=group)
+            if rank != dst:
+                return False
+    else:
+        parts = [buf]
+    full = torch.zeros((N, N), dtype=torch.int16, device=out.device)
+    for r, (a, b) in enumerate(row_ranges):
+        if rows[r]:
+            full[a:b + 1] = parts[r][:rows[r]]
+    if scheme == "balanced":
+        low = torch.tril(full, -1)
+        full = low + low.T
+    else:
+        for r, (a, b) in enumerate(row_ranges):
+            for c, (cs, ce) in enumerate(row_ranges):
+                if r != c and not block_is_computed(r, c) and rows[r] and rows[c]:
+                    full[a:b + 1, cs:ce + 1] = full[cs:ce + 1, a:b + 1].T
+    out.copy_(full)
+    return True
+
+
+def distributed_all_pairs(engine, out, rank, world_size, scheme="balanced", group=None, dst=None, share=None):
+    """One process per GPU: this rank's pairs into `out` (a zeroed N x N int16 tensor), then the
+    row-slab merge (merge_row_slabs) so that every rank (dst None) or rank dst holds the full matrix.
+    scheme "balanced": rows cut at equal DP cells, pairs oriented s1 = the larger index (the
+    distances of a 1-rank run); "checkerboard": the reference's world_size-rank run, its
+    orientation included (sw_compute_rank_blocks).  share(rank, world, out) computes this rank's
+    entries (default: the engine; a stand-in for tests).  Returns this rank's pairs."""
     n = out.shape[0]
-    pairs = engine.rank_blocks_device(rank, world_size, out.data_ptr(), out.stride(0))
-    engine.synchronize()
-    if world_size > 1:
-        dist.all_reduce(out.view(torch.uint8).view(-1), op=dist.ReduceOp.SUM, group=group)
-    del n
+    if scheme not in ("balanced", "checkerboard"):
+        raise ValueError(f"distributed_all_pairs: unknown scheme {scheme!r}")
+    if scheme == "balanced" and engine is not None and engine.mode == SWG_MS:
+        raise ValueError("distributed_all_pairs: SWG-MS runs the checkerboard scheme")
+    if scheme == "balanced":
+        ranges = balanced_row_ranges(engine.lengths if engine is not None else share.lengths, world_size)
+    else:
+        ranges = checkerboard_row_ranges(n, world_size)
+    if share is not None:
+        pairs = share(rank, world_size, out, ranges)
+    elif scheme == "balanced":
+        lo, hi = ranges[rank]
+        pairs = engine.rows_device(lo, hi, out.data_ptr(), out.stride(0)) if hi >= lo else 0
+        engine.synchronize()
+    else:
+        pairs = engine.rank_blocks_device(rank, world_size, out.data_ptr(), out.stride(0))
+        engine.synchronize()
+    merge_row_slabs(out, rank, world_size, ranges, scheme, group=group, dst=dst)
     return pairs

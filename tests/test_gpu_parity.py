@@ -254,6 +254,29 @@ def test_rank_blocks_partition_the_job(cs):
     np.testing.assert_array_equal(total.cpu().numpy(), z["distances"])
 
 
+@pytest.mark.parametrize("name", ["mpi_p1.npz", "protein_mpi.npz", "nw_restated.npz"])
+@pytest.mark.parametrize("block_engine", [0, 2])
+def test_balanced_row_shares_give_the_one_rank_matrix(cs, name, block_engine):
+    """The balanced scheme's shares (rows cut at equal DP cells, rows_device) for 1-4 ranks,
+    merged as merge_row_slabs does, give the reference's one-rank matrix."""
+    import torch
+    from csharp_b200.driver import balanced_row_ranges, merge_row_slabs
+    z = load_npz(name)
+    eng = _golden_engine(cs, z, mode=int(z["mode"]) if "mode" in z else 0)
+    eng.set_option("block_engine", block_engine)
+    N = len(z["offsets"]) - 1
+    want = z["distances"].copy()
+    np.fill_diagonal(want, 0)  # the full matrix's diagonal (NW's restatement holds self-distances)
+    for world in (1, 2, 4):
+        ranges = balanced_row_ranges(eng.lengths, world)
+        out = torch.zeros((N, N), dtype=torch.int16, device="cuda")
+        npairs = sum(eng.rows_device(lo, hi, out.data_ptr(), N) for lo, hi in ranges)
+        eng.synchronize()
+        assert npairs == N * (N - 1) // 2
+        merge_row_slabs(out, 0, 1, [(0, N - 1)], "balanced")
+        np.testing.assert_array_equal(out.cpu().numpy(), want)
+
+
 def test_sequence_validation(cs):
     from csharp_b200.lib import SwError
     eng = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4)
