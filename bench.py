@@ -406,9 +406,13 @@ def main():
     ap.add_argument("--serve-jobs", type=int, default=SERVE["jobs"])
     ap.add_argument("--box-reg", type=int, default=-1, choices=[-1, 0, 1],
                     help="two-pass box step: 1 register box step first, 0 warp box kernel only (-1: engine default)")
+    ap.add_argument("--third-pass", type=int, default=-1, choices=[-1, 0, 1],
+                    help="two-pass give-ups: 1 one-pass 16-bit counter kernel, 0 32-bit lanes (-1: engine default)")
     a = ap.parse_args()
     if a.box_reg >= 0:
         ENGINE_OPTIONS["box_reg"] = a.box_reg
+    if a.third_pass >= 0:
+        ENGINE_OPTIONS["third_pass"] = a.third_pass
     if a.impl == "reference":
         return run_reference_arm(a)
     threads = os.cpu_count() or 1
@@ -518,7 +522,7 @@ def main():
                          "rows_per_lane_costs": (tuned if tuned and any(tuned.values()) else
                                                  "built-in" + (" (kept by the autotuner)" if tuned else ""))},
               "gpu_launches": int(launches), "clocks": clk.summary(),
-              "engine_counters_last_step": {k: eng.query(k) for k in ("pairs", "lane16_pairs", "tripped", "box_spilled",
+              "engine_counters_last_step": {k: eng.query(k) for k in ("pairs", "lane16_pairs", "tripped", "box_spilled", "box_third_pass",
                                                                       "box_fallbacks")}}
 
     if rank == 0:

@@ -742,7 +742,8 @@ int sw_query(sw_ctx* ctx, const char* key, int64_t* value) {
     return SW_OK;
   }
   if (k != "launches" && k != "bins" && k != "alphabet" && k != "items" && k != "lane16_pairs" &&
-      k != "tripped" && k != "planned_items" && k != "box_fallbacks" && k != "box_spilled")
+      k != "tripped" && k != "planned_items" && k != "box_fallbacks" && k != "box_spilled" &&
+      k != "box_third_pass")
     return fail(ctx, SW_E_ARG, "unknown counter " + k);
   *value = ctx->engine ? ctx->engine->stat(key) : 0;
   return SW_OK;
@@ -789,6 +790,7 @@ int sw_set_option(sw_ctx* ctx, const char* key, int64_t value) {
     o.two_pass = (int)value;
   }
   else if (k == "box_reg") o.box_reg = value ? 1 : 0;
+  else if (k == "third_pass") o.third_pass = value ? 1 : 0;
   else if (k == "chunk") {
     if (value < 32 || value > 1024) return fail(ctx, SW_E_ARG, "chunk must be in [32, 1024]");
     o.chunk = (int)value;

@@ -84,6 +84,11 @@ struct EngineJob {
   int mpad;                 // profile rows staged (passes * 32 * K of the bin)
   int protein;              // NW distance rule: similarity over the full length
   unsigned long long* stats; // [0] items taken, [1] pairs finished in 16-bit lanes, [2] tripped
+  // third pass (fb_cnt != nullptr): item it is query fb_lo + it with the fb_cnt[it] partners at
+  // sorted[fb_start[it] ..] (the box step's give-ups, bucketed by query)
+  const int* fb_cnt;
+  const int* fb_start;
+  int fb_lo;
   int4* box;                // two-pass: pairs whose counters the box step finds
   uint32_t* boxwin;         // two-pass: per box record, the threshold codes of the 128 rows above ie
   int* box_count;
@@ -641,8 +646,20 @@ __global__ void __launch_bounds__(warps_of(K, KIND) * 32, ctas_of(K, KIND)) engi
     __syncthreads();
     const int it = s_item;
     if (it >= J.nitems) break;
-    const int4 item = J.items[it];
-    const int q = item.x, c0 = item.y, c1 = item.z, passes = item.w;
+    int q, c0, c1, passes;
+    if (J.fb_cnt) {  // third pass: a query's pairs the box step gave up on
+      q = J.fb_lo + it;
+      c0 = J.fb_start[it];
+      c1 = c0 + J.fb_cnt[it];
+      if (c1 == c0) {
+        __syncthreads();  // every thread has read s_item
+        continue;
+      }
+      passes = max(1, (int)((J.off[q + 1] - J.off[q] + 32 * K - 1) / (32 * K)));
+    } else {
+      const int4 item = J.items[it];
+      q = item.x; c0 = item.y; c1 = item.z; passes = item.w;
+    }
     if (threadIdx.x == 0) atomicAdd(J.stats, 1ull);
     const int m = J.qmode ? J.qlen[q] : (int)(J.off[q + 1] - J.off[q]);
     const int mrows = passes * 32 * K;
@@ -668,13 +685,17 @@ __global__ void __launch_bounds__(warps_of(K, KIND) * 32, ctas_of(K, KIND)) engi
         pc[(NP - 1) * J.mpad + pos] = ftab[a * A1 + c];
       }
     }
-    if (threadIdx.x == 0) { s_q = q; s_count = 0; s_next = 0; }
+    if (threadIdx.x == 0) s_q = q;
+    // segments of at most kMaxChunk entries (a chunk is one; a third-pass query may have more)
+    for (int seg0 = c0; seg0 < c1; seg0 += kMaxChunk) {
+    const int seg1 = min(c1, seg0 + kMaxChunk);
+    if (threadIdx.x == 0) { s_count = 0; s_next = 0; }
     __syncthreads();
     // compact the chunk entries this query aligns, keeping the chunk's ascending-length order
-    for (int base = c0; base < c1; base += blockDim.x) {
+    for (int base = seg0; base < seg1; base += blockDim.x) {
       const int k = base + threadIdx.x;
-      const int d = (k < c1) ? J.sorted[k] : -1;
-      const bool ok = d >= 0 && oriented(J, q, d);
+      const int d = (k < seg1) ? J.sorted[k] : -1;
+      const bool ok = d >= 0 && (J.fb_cnt != nullptr || oriented(J, q, d));
       const unsigned bal = __ballot_sync(0xffffffffu, ok);
       if (lane == 0) s_wc[warp] = __popc(bal);
       __syncthreads();
@@ -833,6 +854,47 @@ __global__ void __launch_bounds__(warps_of(K, KIND) * 32, ctas_of(K, KIND)) engi
       __syncwarp();
     }
     __syncthreads();
+    }  // segments
+  }
+}
+
+// ---- third pass: the box step's give-ups bucketed by query (count, offsets, scatter) -----------
+__global__ void fb_count_kernel(const int2* fb, const int* n, long long cap, int lo, int* cnt) {
+  const long long np = min((long long)*n, cap);
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x)
+    atomicAdd(cnt + (fb[p].x - lo), 1);
+}
+
+// Exclusive prefix sums of cnt[0..nq) into start (one CTA of 1024 threads), fill reset to 0.
+__global__ void __launch_bounds__(1024) fb_scan_kernel(const int* cnt, int* start, int* fill, int nq) {
+  __shared__ int part[1024];
+  const int t = threadIdx.x;
+  const int per = (nq + 1023) / 1024, lo = min(nq, t * per), hi = min(nq, lo + per);
+  int sum = 0;
+  for (int k = lo; k < hi; k++) sum += cnt[k];
+  part[t] = sum;
+  __syncthreads();
+  for (int d = 1; d < 1024; d <<= 1) {  // inclusive scan of the per-thread sums
+    const int v = t >= d ? part[t - d] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int run = part[t] - sum;
+  for (int k = lo; k < hi; k++) {
+    start[k] = run;
+    run += cnt[k];
+    fill[k] = 0;
+  }
+}
+
+__global__ void fb_scatter_kernel(const int2* fb, const int* n, long long cap, int lo, const int* start, int* fill,
+                                  int* sorted) {
+  const long long np = min((long long)*n, cap);
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+    const int2 pr = fb[p];
+    const int q = pr.x - lo;
+    sorted[start[q] + atomicAdd(fill + q, 1)] = pr.y;
   }
 }
 
@@ -849,6 +911,7 @@ constexpr int kKs[kNumK] = {4, 6, 8, 10, 12, 14, 16};
 // Engine work counters: items taken, pairs finished in 16-bit lanes, tripped 16-bit lanes, pairs
 // the box step gave up on, pairs handed to the warp box kernel.
 constexpr int kNumStats = 8;
+constexpr int kFbK = 16;  // rows per lane of the third pass (any query length, in passes of 512 rows)
 
 // Largest alphabet of the 16-bit lanes (two-plane profiles beyond 8 letters).
 constexpr int kMaxAlpha16 = 32;
@@ -1020,16 +1083,22 @@ struct Base {
   long long spill_cap = 0;
   uint32_t* d_rowbuf = nullptr;
   size_t rowbuf_bytes = 0;
+  // third pass: the give-ups (pair list, bucketed partners) and per-query counts / offsets / fill
+  int2* d_fb = nullptr;
+  int* d_fbsorted = nullptr;
+  int* d_fbq = nullptr;         // [3 * nseq]: counts, offsets, fill
   void free_box() {
     cudaFree(d_box); cudaFree(d_boxwin); cudaFree(d_cls[0]); cudaFree(d_cls[1]); cudaFree(d_spill);
+    cudaFree(d_fb); cudaFree(d_fbsorted);
     d_box = nullptr; d_boxwin = nullptr; d_cls[0] = d_cls[1] = nullptr; d_spill = nullptr;
+    d_fb = nullptr; d_fbsorted = nullptr;
     box_cap = spill_cap = 0;
   }
   ~Base() {
     cudaFree(d_code); cudaFree(d_sorted); cudaFree(d_lettab); cudaFree(d_flagtab);
     cudaFree(d_scratch); cudaFree(d_carry);
     free_box();
-    cudaFree(d_counts); cudaFree(d_rowbuf);
+    cudaFree(d_counts); cudaFree(d_rowbuf); cudaFree(d_fbq);
   }
 };
 
@@ -1112,6 +1181,9 @@ int build_base(Base& B, const EngineParams& P, std::string* msg) {
 struct Plan {
   bool plain_only = false;
   int kind = kKindSw;       // the bins' kernel: SW with counters, NW, or the two-pass first pass
+  bool fb = false;          // two-pass: the box step's give-ups run on 16-bit lanes (third pass)
+  int fb_mpad = 0, fb_grid = 0;
+  size_t fb_smem = 0;
   bool zeroes_diagonal = false;
   int thresh = 0;
   std::vector<Bin> bins;
@@ -1181,7 +1253,7 @@ class EngineImpl : public Engine {
       int64_t n = 2;  // the 32-bit lane kernel and the rerun-count reset
       for (auto& bn : last_->bins) n += bn.items.empty() ? 0 : 1;
       if (!last_->plain_only && last_->kind == kKindScore)  // the box step: scan, 4 band classes, warp kernel
-        n += opt_.box_reg ? 6 : 1;
+        n += (opt_.box_reg ? 6 : 1) + (last_->fb ? 4 : 0);  // third pass: count, scan, scatter, kernel
       return n + (last_->zeroes_diagonal ? 1 : 0);
     }
     if (k == "bins") {
@@ -1190,12 +1262,14 @@ class EngineImpl : public Engine {
       return n;
     }
     if (k == "alphabet") return base_ ? base_->alpha : 0;
-    if (k == "items" || k == "lane16_pairs" || k == "tripped" || k == "box_fallbacks" || k == "box_spilled") {
+    if (k == "items" || k == "lane16_pairs" || k == "tripped" || k == "box_fallbacks" || k == "box_spilled" ||
+        k == "box_third_pass") {
       if (!last_->d_stats) return 0;
       unsigned long long h[kNumStats] = {};
       cudaDeviceSynchronize();
       cudaMemcpy(h, last_->d_stats, sizeof(h), cudaMemcpyDeviceToHost);
-      return (int64_t)(k == "items" ? h[0] : k == "lane16_pairs" ? h[1] : k == "tripped" ? h[2] : k == "box_fallbacks" ? h[3] : h[4]);
+      return (int64_t)(k == "items" ? h[0] : k == "lane16_pairs" ? h[1] : k == "tripped" ? h[2]
+                       : k == "box_fallbacks" ? h[3] : k == "box_spilled" ? h[4] : h[5]);
     }
     if (k == "planned_items") {
       int64_t n = 0;
@@ -1507,16 +1581,6 @@ class EngineImpl : public Engine {
     // most work first: its CTAs take the SMs, the lighter bins fill in as its queue drains
     std::stable_sort(pl.order.begin(), pl.order.end(),
                      [&](int a, int b) { return pl.bins[a].total_cost > pl.bins[b].total_cost; });
-    const size_t scr = std::max<size_t>(scr_words * 4, 16);
-    if (scr > B.scratch_bytes) {
-      cudaFree(B.d_scratch);
-      B.d_scratch = nullptr;
-      B.scratch_bytes = 0;
-      // every plan's graph holds the scratch pointer: growing it retires them
-      for (auto& kv : plans_) if (kv.second->graph) { cudaGraphExecDestroy(kv.second->graph); kv.second->graph = nullptr; }
-      if (cudaMalloc(&B.d_scratch, scr) != cudaSuccess) { cudaGetLastError(); *msg = "cudaMalloc pass scratch"; return SW_E_OOM; }
-      B.scratch_bytes = scr;
-    }
     pl.big_count = (int)big.size();
     // the two-pass box kernel may give any pair to the 32-bit lanes: room for all of them
     const int64_t spare = pl.kind == kKindScore ? pl.npairs : std::max<int64_t>(1 << 16, pl.npairs / 16);
@@ -1533,6 +1597,8 @@ class EngineImpl : public Engine {
         const size_t n = (size_t)std::max<int64_t>(pl.npairs, 1);
         const size_t nspill = std::max<size_t>(n / 16, 1 << 16);
         if (cudaMalloc(&B.d_box, sizeof(int4) * n) != cudaSuccess ||
+            cudaMalloc(&B.d_fb, sizeof(int2) * n) != cudaSuccess ||
+            cudaMalloc(&B.d_fbsorted, sizeof(int) * n) != cudaSuccess ||
             cudaMalloc(&B.d_boxwin, sizeof(uint32_t) * kRegWinWords * n) != cudaSuccess ||
             cudaMalloc(&B.d_cls[0], sizeof(int) * n) != cudaSuccess ||
             cudaMalloc(&B.d_cls[1], sizeof(int) * n) != cudaSuccess ||
@@ -1548,6 +1614,20 @@ class EngineImpl : public Engine {
       if (!B.d_counts && cudaMalloc(&B.d_counts, sizeof(int) * 8) != cudaSuccess) {
         cudaGetLastError(); B.d_counts = nullptr; *msg = "cudaMalloc two-pass counts"; return SW_E_OOM;
       }
+      if (!B.d_fbq && cudaMalloc(&B.d_fbq, sizeof(int) * 3 * (size_t)std::max(N, 1)) != cudaSuccess) {
+        cudaGetLastError(); B.d_fbq = nullptr; *msg = "cudaMalloc third-pass counts"; return SW_E_OOM;
+      }
+      // the third pass (16 rows per lane, every query's profile in shared memory) where it fits;
+      // its scratch carries multi-pass rows like the bins'
+      pl.fb_mpad = ((B.maxcol + 32 * kFbK - 1) / (32 * kFbK)) * 32 * kFbK;
+      pl.fb_smem = engine_smem(A, pl.fb_mpad, B.maxcol, kFbK, kKindSw);
+      pl.fb = opt_.third_pass && pl.fb_smem <= 227 * 1024 &&
+              allow_smem_k(kFbK, A, kKindSw, pl.fb_smem) == cudaSuccess;
+      cudaGetLastError();
+      if (pl.fb) {
+        pl.fb_grid = P.sms * std::max(1, occupancy_k(kFbK, A, kKindSw, pl.fb_smem));
+        scr_words = std::max(scr_words, (size_t)pl.fb_grid * warps_of(kFbK) * B.maxcol * kScrWords);
+      }
       const size_t rb = std::max<size_t>(row_words * 4, 16);
       if (rb > B.rowbuf_bytes) {
         retire();
@@ -1557,6 +1637,16 @@ class EngineImpl : public Engine {
         if (cudaMalloc(&B.d_rowbuf, rb) != cudaSuccess) { cudaGetLastError(); *msg = "cudaMalloc row bounds"; return SW_E_OOM; }
         B.rowbuf_bytes = rb;
       }
+    }
+    const size_t scr = std::max<size_t>(scr_words * 4, 16);
+    if (scr > B.scratch_bytes) {
+      cudaFree(B.d_scratch);
+      B.d_scratch = nullptr;
+      B.scratch_bytes = 0;
+      // every plan's graph holds the scratch pointer: growing it retires them
+      for (auto& kv : plans_) if (kv.second->graph) { cudaGraphExecDestroy(kv.second->graph); kv.second->graph = nullptr; }
+      if (cudaMalloc(&B.d_scratch, scr) != cudaSuccess) { cudaGetLastError(); *msg = "cudaMalloc pass scratch"; return SW_E_OOM; }
+      B.scratch_bytes = scr;
     }
     std::vector<int2> rl(big);
     rl.resize((size_t)pl.rerun_cap);
@@ -1579,6 +1669,8 @@ class EngineImpl : public Engine {
       zero_diagonal_kernel<<<(P.nseq + 255) / 256, 256, 0, P.stream>>>(P.out, P.ld, P.nseq);
     set_int_kernel<<<1, 1, 0, P.stream>>>(pl.d_rerun_count, pl.big_count);
     const bool two = !pl.plain_only && pl.kind == kKindScore;
+    EngineJob J3;  // the bins' job, the third pass's template
+    std::memset(&J3, 0, sizeof(J3));
     if (two && (e = cudaMemsetAsync(B.d_counts, 0, sizeof(int) * 8, P.stream)) != cudaSuccess) return e;
     if (!pl.plain_only) {
       if ((e = cudaMemsetAsync(pl.d_counters, 0, sizeof(int) * (pl.bins.size() + 1), P.stream)) != cudaSuccess) return e;
@@ -1619,6 +1711,7 @@ class EngineImpl : public Engine {
         }
       }
       if (bins_t1 && (e = cudaEventRecord(bins_t1, P.stream)) != cudaSuccess) return e;
+      J3 = J;
     }
     if (two) {
       // counters of the first pass's best cells from regions around their traceback paths: the
@@ -1637,6 +1730,7 @@ class EngineImpl : public Engine {
       X.list_cap = B.box_cap;
       X.spill = B.d_spill; X.spill_count = B.d_counts + 1;
       X.spill_cap = (int)std::min<long long>(B.spill_cap, 0x7fffffff);
+      if (pl.fb) { X.fb = B.d_fb; X.fb_count = B.d_counts + 6; X.fb_cap = B.box_cap; }
       BoxJob Y = X;
       if (opt_.box_reg) {
         if ((e = launch_box_scan(X, P.sms, P.stream)) != cudaSuccess) return e;
@@ -1648,6 +1742,30 @@ class EngineImpl : public Engine {
       Y.max_score = kWarpBoxMaxCols * std::max(B.max_s, 0);
       Y.budget = 1 << 16;
       if ((e = launch_box(Y, (int)(B.carry_threads / 128), 128, P.stream)) != cudaSuccess) return e;
+      if (pl.fb) {
+        // third pass: the give-ups bucketed by query, then the one-pass counter kernel on them
+        const int nq = key.row_hi - key.row_lo + 1;
+        int* cnt = B.d_fbq;
+        int* start = cnt + P.nseq;
+        int* fill = start + P.nseq;
+        if ((e = cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)nq, P.stream)) != cudaSuccess) return e;
+        const int g = std::max(1, P.sms * 4);
+        fb_count_kernel<<<g, 256, 0, P.stream>>>(B.d_fb, B.d_counts + 6, B.box_cap, key.row_lo, cnt);
+        fb_scan_kernel<<<1, 1024, 0, P.stream>>>(cnt, start, fill, nq);
+        fb_scatter_kernel<<<g, 256, 0, P.stream>>>(B.d_fb, B.d_counts + 6, B.box_cap, key.row_lo, start, fill,
+                                                   B.d_fbsorted);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        EngineJob F = J3;
+        F.fb_cnt = cnt; F.fb_start = start; F.fb_lo = key.row_lo;
+        F.sorted = B.d_fbsorted;
+        F.items = nullptr; F.nitems = nq;
+        F.counter = B.d_counts + 7;
+        F.mpad = pl.fb_mpad;
+        F.scratch = B.d_scratch;
+        F.rowbuf = nullptr;
+        F.box = nullptr; F.boxwin = nullptr;
+        if ((e = launch_engine_k(kFbK, kKindSw, F, pl.fb_grid, pl.fb_smem, P.stream)) != cudaSuccess) return e;
+      }
     }
     // 32-bit lanes: pairs the static guard routed here, those whose 16-bit lanes tripped, or all
     PlainJob R;

@@ -41,6 +41,7 @@ struct EngineOptions {
   int two_pass = 1;                // SW: score-only pass, then counters from boxes (box step):
                                    // 1 where the gap costs suit it, 2 whenever min(o, e) >= 2, 0 never
   int box_reg = 1;                 // two-pass: register box step first (0: the warp box kernel alone)
+  int third_pass = 1;              // two-pass: the box step's give-ups on 16-bit lanes (0: 32-bit lanes)
   int m_lo = 0, m_hi = 0;          // autotuner: only queries with m_lo < length <= m_hi (0: all)
   int k_weights[7] = {0, 0, 0, 0, 0, 0, 0};  // cost per row at 4, 6, ..., 16 rows per lane
                                              // (0: built-in table; set by autotune)

@@ -93,6 +93,9 @@ struct BoxJob {
   int4* spill;             // box_scan_kernel: pairs for the warp box kernel
   int* spill_count;
   int spill_cap;
+  int2* fb;                // pairs given up on, for the 16-bit counter kernel (nullptr: the 32-bit lanes)
+  int* fb_count;
+  long long fb_cap;
 };
 
 constexpr int kWarpBoxMaxCols = 256;  // box_kernel's largest box (columns and rows)

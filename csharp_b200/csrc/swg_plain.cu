@@ -261,6 +261,23 @@ __device__ __forceinline__ int scan_max_up(int y, int lane) {
 
 constexpr int kBoxMaxA1 = 33;  // letters + padding of the dense codes
 
+// A pair the box step cannot finish: the full DP with counters, on the 16-bit lanes of the
+// one-pass kernel (J.fb) where the engine runs that third pass, else on the 32-bit lanes.
+__device__ __forceinline__ void box_give_up(const BoxJob& J, int q, int d) {
+  atomicAdd(J.stats + 3, 1ull);
+  atomicAdd(J.stats + 1, ~0ull);  // not finished yet (the third pass counts it again)
+  if (J.fb) {
+    const int w = atomicAdd(J.fb_count, 1);
+    if (w < J.fb_cap) {
+      J.fb[w] = make_int2(q, d);
+      atomicAdd(J.stats + 5, 1ull);
+      return;
+    }
+  }
+  const int wr = atomicAdd(J.rerun_count, 1);
+  if (wr < J.rerun_cap) J.rerun[wr] = make_int2(q, d);
+}
+
 __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
   __shared__ int sc[kBoxMaxA1 * kBoxMaxA1];        // S(a, b) of the dense codes
   __shared__ uint32_t fl[kBoxMaxA1 * kBoxMaxA1];
@@ -419,10 +436,7 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
     }
     if (lane == 0) {
       if (!ok) {
-        const int wr = atomicAdd(J.rerun_count, 1);
-        if (wr < J.rerun_cap) J.rerun[wr] = make_int2(q, d);
-        atomicAdd(J.stats + 3, 1ull);
-        atomicAdd(J.stats + 1, ~0ull);  // no longer finished in 16-bit lanes
+        box_give_up(J, q, d);
       } else {
         const int16_t dist = fraction_distance((int)(ccap & 0xFFFFu), (int)(ccap >> 16));
         J.out[(long long)q * J.ld + d] = dist;
@@ -435,14 +449,6 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
 
 // ---- box step, one pair per thread with the DP rows in registers (swg_box_reg.cuh) -------------
 constexpr int kRegThreads = 128;
-
-// The pair goes on to the 32-bit lanes (full DP).
-__device__ __forceinline__ void box_give_up(const BoxJob& J, int q, int d) {
-  const int wr = atomicAdd(J.rerun_count, 1);
-  if (wr < J.rerun_cap) J.rerun[wr] = make_int2(q, d);
-  atomicAdd(J.stats + 3, 1ull);
-  atomicAdd(J.stats + 1, ~0ull);  // no longer finished in 16-bit lanes
-}
 
 // Rows of the box tables: one per residue byte of s1 in query mode, else one per code.
 constexpr int kBoxTabRows = 128;

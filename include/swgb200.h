@@ -184,8 +184,12 @@ int sw_compute_rank_blocks(sw_ctx* ctx, int32_t rank, int32_t world_size, int16_
  * the gap costs with which that neighbourhood stays small; 2: whenever open and extend >= 2; 0:
  * never, the one-pass counter kernels), "box_reg" (two passes: 1, the default, finds each pair's
  * counters with one thread per pair and the DP rows in registers, handing pairs whose alignment
- * region is wider to the warp-per-pair box kernel; 0: the warp-per-pair kernel for every pair).
- * Every knob gives the same distances.  Unknown keys are SW_E_ARG. */
+ * region is wider to the warp-per-pair box kernel; 0: the warp-per-pair kernel for every pair),
+ * "third_pass" (two passes: 1, the default, redoes the pairs the box step cannot finish with the
+ * one-pass 16-bit counter kernel, grouped by query; 0: with the 32-bit lanes), "block_engine"
+ * (block handler: 1, the default, the batched engine for blocks of at least 4,096 pairs and the
+ * one-launch plain kernel below; 2: the engine for every block; 0: the plain kernel for every
+ * block).  Every knob gives the same distances.  Unknown keys are SW_E_ARG. */
 int sw_set_option(sw_ctx* ctx, const char* key, int64_t value);
 
 /* Autotuner (no reference counterpart; the reference has one aligner loop): times every
@@ -202,8 +206,9 @@ int sw_autotune(sw_ctx* ctx, int16_t* d_out, int64_t ld_out, int32_t weights[7])
  * "bins" (rows-per-lane classes used), "alphabet" (distinct residue bytes), "planned_items",
  * and, after waiting for the device, "items" (work items taken), "lane16_pairs" (pairs finished
  * in 16-bit lanes), "tripped" (16-bit lanes handed to 32-bit lanes), "box_spilled" (two-pass pairs
- * the register box step handed to the warp box kernel) and "box_fallbacks" (two-pass pairs handed
- * to 32-bit lanes).  Unknown keys are SW_E_ARG. */
+ * the register box step handed to the warp box kernel), "box_fallbacks" (two-pass pairs the box
+ * step could not finish) and "box_third_pass" (those of them redone by the one-pass 16-bit counter
+ * kernel; the rest go to 32-bit lanes).  Unknown keys are SW_E_ARG. */
 int sw_query(sw_ctx* ctx, const char* key, int64_t* value);
 
 /* ---- block handler without device allocation ------------------------------------------------ */

@@ -486,9 +486,11 @@ def test_two_pass_equals_one_pass_and_oracle(cs, oracle_mod):
     np.testing.assert_array_equal(got3, want3)
 
 
-def test_two_pass_with_most_pairs_falling_back(cs):
-    """Cheap gaps and close relatives: the box kernel gives most pairs to the 32-bit lanes, whose
-    list must hold them all (an overflow would raise in rerun_count)."""
+@pytest.mark.parametrize("third", [1, 0])
+def test_two_pass_with_most_pairs_falling_back(cs, third):
+    """Cheap gaps and close relatives: the box step gives up on most pairs; the third pass (the
+    one-pass 16-bit counter kernel over them, grouped by query) or the 32-bit lanes, whose list
+    must then hold them all (an overflow would raise in rerun_count), redo them."""
     from csharp_b200 import synth
     rng = np.random.default_rng(5)
     seqs = [s.tobytes() for s in synth.dna_family(90, 2, rng.integers(200, 700, 90), seed=6, sub_range=(0.0, 0.03),
@@ -498,10 +500,23 @@ def test_two_pass_with_most_pairs_falling_back(cs):
     want, pairs, _ = one.all_pairs(1)
     two = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 3, 2).upload(seqs)
     two.set_option("two_pass", 2)  # two passes although the default rule keeps 3/2 on one
+    two.set_option("third_pass", third)
     got, _, _ = two.all_pairs(1)
     assert two.query("box_fallbacks") > pairs // 2
+    if third:
+        assert two.query("box_third_pass") == two.query("box_fallbacks")
+        assert two.query("launches") >= 12
+    else:
+        assert two.query("box_third_pass") == 0
     assert two.query("lane16_pairs") + two.rerun_count() == pairs
     np.testing.assert_array_equal(got, want)
+    # a block plan (rows 30..89 against columns 0..29) and a 3-rank checkerboard job
+    two.set_option("block_engine", 2)
+    blk, _ = two.compute_block(30, 89, 0, 29, False)
+    np.testing.assert_array_equal(blk, want[30:90, 0:30])
+    got3, _, _ = two.all_pairs(3)
+    want3, _, _ = one.all_pairs(3)
+    np.testing.assert_array_equal(got3, want3)
 
 
 @pytest.mark.parametrize("o,e", [(16, 4), (10, 3), (20, 8), (4, 2)])
