@@ -58,8 +58,7 @@ __host__ __device__ constexpr int ctas_of(int K, int kind = 0) {
   return kind == kKindScoreShape ? (K <= 10 ? 2 : 1) : (K <= 8 ? 2 : 1);
 }
 constexpr int kMaxChunk = 1024;
-constexpr int kScrWords = 8;    // words of carried state per column in the pass scratch (SW)
-constexpr int kScrWordsNw = 12; // NW: V, G and two counter words per state and lane
+constexpr int kScrWords = 8;    // words of carried state per column in the pass scratch
 
 struct EngineJob {
   const uint8_t* code;      // dense residue codes (pad code = A), same offsets as the residues
@@ -76,7 +75,7 @@ struct EngineJob {
   int16_t* out;
   long long ld;
   int mirror;               // also write (d, q): symmetric jobs and diagonal blocks, never other blocks
-  uint32_t* scratch;        // per (CTA, warp) slot: maxcol * (kScrWords or kScrWordsNw) words
+  uint32_t* scratch;        // per (CTA, warp) slot: maxcol * kScrWords words
   int maxcol;               // longest database sequence
   int2* rerun;              // pairs to redo with 32-bit lanes
   int* rerun_count;
@@ -413,85 +412,88 @@ __device__ __forceinline__ void score_two(const uint32_t* __restrict__ prof, int
 
 // NW (global) counterpart of align_two: V = max(F, G, H) without the 0 floor, boundaries
 // V(i,0) = -o-(i-1)e and V(0,j) = -o-(j-1)e reached through the gap chains, the result taken at
-// (m, n) of each pair.  Every state carries two counter words per lane (NwCnt): w0 = aligned
-// columns << 16 | counted columns, w1 = leading gap run << 16 | signed trailing gap run.
-// Lanes hold value + bias with a bias that covers the all-gap lower bound of every cell a pass
-// touches (padding rows and columns score 0, so they stay inside the same bounds); lanes start
-// at their own column 0, so steps before it change nothing.
+// (m, n) of each pair.  Lanes hold value + bias with a bias that covers the all-gap lower bound of
+// every cell a pass touches (padding rows and columns score 0, so they stay inside the same
+// bounds); lanes start at their own column 0, so steps before it change nothing.
+//
+// One counter word per state and lane: columns << 16 | counted columns.  The trimmed identity of
+// nucleic jobs (Salsa.NeedlemanWunschTPL/Program.cs:547-571) divides by the columns between the
+// first and the last column with no gap in either string: the alignment less its leading gap run
+// and its trailing gap run.  A global path from (0, 0) to (m, n) leaves column 0 (or row 0) for
+// good at its first non-UP (non-LEFT) step, so its leading run is exactly its steps on column 0
+// or row 0; once on column n (row m) it can only go UP (LEFT), so its trailing run is exactly its
+// UP steps within column n or LEFT steps within row m.  Nucleic jobs therefore count no column on
+// the boundary (V(i, 0), V(0, j) carry 0), and the UP / LEFT steps into a cell of column n / row m
+// add no column (ginc / hinc 0 there); every other step adds one.  Protein jobs divide by the
+// whole alignment: every step counts and the boundaries carry i / j columns.
 template <int K, int NP>
 __device__ __forceinline__ void align_two_nw(const uint32_t* __restrict__ prof, int mpad, int passes,
                                              int m, const uint8_t* __restrict__ ca,
                                              const uint8_t* __restrict__ cb, int ncols, int nA, int nB,
                                              const EngineJob& J, uint32_t* __restrict__ scr, int lane,
-                                             uint32_t& capA0, uint32_t& capA1, uint32_t& capB0,
-                                             uint32_t& capB1) {
+                                             uint32_t& capA, uint32_t& capB) {
   const int B = J.bias, o = J.o, e = J.e;
   const uint32_t O2 = (uint32_t)o * 0x10001u, E2 = (uint32_t)e * 0x10001u;
   const uint32_t sent2 = (uint32_t)e * 0x10001u;  // -infinity: loses to any opening, minus e is 0
+  const bool trim = !J.protein;
+  const uint32_t bmul = trim ? 0u : 0x10000u;     // boundary columns counted (protein) or not
   const int plane = NP * mpad;
   // the cell (m, n) of each pair: its pass, lane, row in the lane, and the step that reaches it
   const int pm = (m - 1) / (32 * K), tm = ((m - 1) % (32 * K)) / K, rm = (m - 1) % K;
   const int sA = nA - 1 + tm, sB = nB - 1 + tm;
-  capA0 = capA1 = capB0 = capB1 = 0u;
+  capA = capB = 0u;
   for (int p = 0; p < passes; p++) {
     const int pbase = p * 32 * K;
-    uint32_t VOL[K], H[K], clA0[K], clA1[K], clB0[K], clB1[K], chA0[K], chA1[K], chB0[K], chB1[K];
+    uint32_t VOL[K], H[K], clA[K], clB[K], chA[K], chB[K], hinc[K];
 #pragma unroll
     for (int r = 0; r < K; r++) {
-      const int i = pbase + lane * K + r + 1;  // V(i, 0) = -o - (i-1)e, counters of i UP columns
+      const int i = pbase + lane * K + r + 1;  // V(i, 0) = -o - (i-1)e after i UP steps
       VOL[r] = (uint32_t)(B - 2 * o - (i - 1) * e) * 0x10001u;
       H[r] = sent2;
-      clA0[r] = clB0[r] = (uint32_t)i << 16;
-      clA1[r] = clB1[r] = ((uint32_t)i << 16) | (uint32_t)(i & 0xFFFF);
-      chA0[r] = chA1[r] = chB0[r] = chB1[r] = 0u;
+      clA[r] = clB[r] = (uint32_t)i * bmul;
+      chA[r] = chB[r] = 0u;
+      hinc[r] = (trim && i == m) ? 0u : 0x10000u;  // LEFT steps within row m: the trailing run
     }
     // the row above the lane's first row, at column 0 (the first step's diagonal)
     const int i0 = pbase + lane * K;
     uint32_t dVO = (uint32_t)(i0 == 0 ? B - o : B - 2 * o - (i0 - 1) * e) * 0x10001u;
-    uint32_t dcA0 = (uint32_t)i0 << 16, dcA1 = ((uint32_t)i0 << 16) | (uint32_t)(i0 & 0xFFFF);
-    uint32_t dcB0 = dcA0, dcB1 = dcA1;
-    uint32_t uVO = 0, uG = 0, ucvA0 = 0, ucvA1 = 0, ucvB0 = 0, ucvB1 = 0, ucgA0 = 0, ucgA1 = 0,
-             ucgB0 = 0, ucgB1 = 0;
+    uint32_t dcA = (uint32_t)i0 * bmul, dcB = dcA;
+    uint32_t uVO = 0, uG = 0, ucvA = 0, ucvB = 0, ucgA = 0, ucgB = 0;
     const uint32_t* pl = prof + pbase + lane * 4;
     const int nsteps = ncols + 31;
     for (int s = 0; s < nsteps; s++) {
       const uint32_t bVO = __shfl_up_sync(0xffffffffu, uVO, 1);
       const uint32_t bG = __shfl_up_sync(0xffffffffu, uG, 1);
-      const uint32_t bcvA0 = __shfl_up_sync(0xffffffffu, ucvA0, 1);
-      const uint32_t bcvA1 = __shfl_up_sync(0xffffffffu, ucvA1, 1);
-      const uint32_t bcvB0 = __shfl_up_sync(0xffffffffu, ucvB0, 1);
-      const uint32_t bcvB1 = __shfl_up_sync(0xffffffffu, ucvB1, 1);
-      const uint32_t bcgA0 = __shfl_up_sync(0xffffffffu, ucgA0, 1);
-      const uint32_t bcgA1 = __shfl_up_sync(0xffffffffu, ucgA1, 1);
-      const uint32_t bcgB0 = __shfl_up_sync(0xffffffffu, ucgB0, 1);
-      const uint32_t bcgB1 = __shfl_up_sync(0xffffffffu, ucgB1, 1);
+      const uint32_t bcvA = __shfl_up_sync(0xffffffffu, ucvA, 1);
+      const uint32_t bcvB = __shfl_up_sync(0xffffffffu, ucvB, 1);
+      const uint32_t bcgA = __shfl_up_sync(0xffffffffu, ucgA, 1);
+      const uint32_t bcgB = __shfl_up_sync(0xffffffffu, ucgB, 1);
       if (s >= lane) {  // the lane's columns start at step `lane`
-        uint32_t VOU, GU, cvuA0, cvuA1, cvuB0, cvuB1, cguA0, cguA1, cguB0, cguB1;
+        uint32_t VOU, GU, cvuA, cvuB, cguA, cguB;
         if (lane == 0) {
           if (p == 0) {
             // row 0: V(0, j) = -o - (j-1)e for column j = s + 1 (past the end: clamped)
             const int j = min(s, ncols - 1) + 1;
             VOU = (uint32_t)(B - 2 * o - (j - 1) * e) * 0x10001u;
             GU = sent2;
-            cvuA0 = cvuB0 = (uint32_t)j << 16;
-            cvuA1 = cvuB1 = ((uint32_t)j << 16) | (uint32_t)((-j) & 0xFFFF);
-            cguA0 = cguA1 = cguB0 = cguB1 = 0u;
+            cvuA = cvuB = (uint32_t)j * bmul;
+            cguA = cguB = 0u;
           } else {
             const int js = min(s, ncols - 1);
-            const uint4 x = *reinterpret_cast<const uint4*>(scr + (long)js * kScrWordsNw);
-            const uint4 y = *reinterpret_cast<const uint4*>(scr + (long)js * kScrWordsNw + 4);
-            const uint4 z = *reinterpret_cast<const uint4*>(scr + (long)js * kScrWordsNw + 8);
-            VOU = x.x; GU = x.y; cvuA0 = x.z; cvuA1 = x.w;
-            cvuB0 = y.x; cvuB1 = y.y; cguA0 = y.z; cguA1 = y.w;
-            cguB0 = z.x; cguB1 = z.y;
+            const uint4 x = *reinterpret_cast<const uint4*>(scr + (long)js * kScrWords);
+            const uint2 y = *reinterpret_cast<const uint2*>(scr + (long)js * kScrWords + 4);
+            VOU = x.x; GU = x.y; cvuA = x.z; cvuB = x.w; cguA = y.x; cguB = y.y;
           }
         } else {
-          VOU = bVO; GU = bG; cvuA0 = bcvA0; cvuA1 = bcvA1; cvuB0 = bcvB0; cvuB1 = bcvB1;
-          cguA0 = bcgA0; cguA1 = bcgA1; cguB0 = bcgB0; cguB1 = bcgB1;
+          VOU = bVO; GU = bG; cvuA = bcvA; cvuB = bcvB; cguA = bcgA; cguB = bcgB;
         }
-        uint32_t VOD = dVO, cdA0 = dcA0, cdA1 = dcA1, cdB0 = dcB0, cdB1 = dcB1;
-        dVO = VOU; dcA0 = cvuA0; dcA1 = cvuA1; dcB0 = cvuB0; dcB1 = cvuB1;
-        const int col = 32 + s - lane;
+        uint32_t VOD = dVO, cdA = dcA, cdB = dcB;
+        dVO = VOU; dcA = cvuA; dcB = cvuB;
+        const int jc = s - lane;  // this step's column (0-based)
+        // UP steps within column n: the trailing run
+        const uint32_t gincA = (trim && jc == nA - 1) ? 0u : 0x10000u;
+        const uint32_t gincB = (trim && jc == nB - 1) ? 0u : 0x10000u;
+        const int col = 32 + jc;
         const int xa = ca[col], xb = cb[col];
         const uint32_t* pla = pl + xa * plane;
         const uint32_t* phb = pl + xb * plane + (NP == 3 ? mpad : 0);
@@ -500,34 +502,28 @@ __device__ __forceinline__ void align_two_nw(const uint32_t* __restrict__ prof, 
         auto cell = [&](const int r, const uint32_t pl_r, const uint32_t ph_r, const uint32_t ma_r,
                         const uint32_t mb_r) {
           const uint32_t F = (NP == 3) ? VOD + pl_r + ph_r : mad_hi16(ph_r, VOD + pl_r);
-          const uint32_t cfA0 = cdA0 + ma_r + 0x10000u, cfA1 = cdA1 & 0xFFFF0000u;
-          const uint32_t cfB0 = cdB0 + mb_r + 0x10000u, cfB1 = cdB1 & 0xFFFF0000u;
+          const uint32_t cfA = cdA + ma_r + 0x10000u;
+          const uint32_t cfB = cdB + mb_r + 0x10000u;
           bool hiB, loA;
           // vertical gap: opening wins ties (extend only if strictly better)
           const uint32_t G = vmax2(VOU, GU - E2, hiB, loA);
-          const uint32_t cgA0 = (loA ? cvuA0 : cguA0) + 0x10000u;
-          const uint32_t cgA1 = loA ? ((cvuA1 & 0xFFFF0000u) | 1u) : cguA1 + 1u;
-          const uint32_t cgB0 = (hiB ? cvuB0 : cguB0) + 0x10000u;
-          const uint32_t cgB1 = hiB ? ((cvuB1 & 0xFFFF0000u) | 1u) : cguB1 + 1u;
+          const uint32_t cgA = (loA ? cvuA : cguA) + gincA;
+          const uint32_t cgB = (hiB ? cvuB : cguB) + gincB;
           // horizontal gap
           H[r] = vmax2(VOL[r], H[r] - E2, hiB, loA);
-          chA0[r] = (loA ? clA0[r] : chA0[r]) + 0x10000u;
-          chA1[r] = loA ? ((clA1[r] & 0xFFFF0000u) | 0xFFFFu) : chA1[r] - 1u;
-          chB0[r] = (hiB ? clB0[r] : chB0[r]) + 0x10000u;
-          chB1[r] = hiB ? ((clB1[r] & 0xFFFF0000u) | 0xFFFFu) : chB1[r] - 1u;
+          chA[r] = (loA ? clA[r] : chA[r]) + hinc[r];
+          chB[r] = (hiB ? clB[r] : chB[r]) + hinc[r];
           // V = max(F, G, H) with DIAGONAL > UP > LEFT on ties
           const uint32_t GHv = vmax2(G, H[r], hiB, loA);
-          const uint32_t cghA0 = loA ? cgA0 : chA0[r], cghA1 = loA ? cgA1 : chA1[r];
-          const uint32_t cghB0 = hiB ? cgB0 : chB0[r], cghB1 = hiB ? cgB1 : chB1[r];
+          const uint32_t cghA = loA ? cgA : chA[r];
+          const uint32_t cghB = hiB ? cgB : chB[r];
           const uint32_t V = vmax2(F, GHv, hiB, loA);
-          const uint32_t cvA0 = loA ? cfA0 : cghA0, cvA1 = loA ? cfA1 : cghA1;
-          const uint32_t cvB0 = hiB ? cfB0 : cghB0, cvB1 = hiB ? cfB1 : cghB1;
+          const uint32_t cvA = loA ? cfA : cghA;
+          const uint32_t cvB = hiB ? cfB : cghB;
           const uint32_t VO = V - O2;
-          VOD = VOL[r]; cdA0 = clA0[r]; cdA1 = clA1[r]; cdB0 = clB0[r]; cdB1 = clB1[r];
-          VOL[r] = VO; clA0[r] = cvA0; clA1[r] = cvA1; clB0[r] = cvB0; clB1[r] = cvB1;
-          VOU = VO; GU = G;
-          cvuA0 = cvA0; cvuA1 = cvA1; cvuB0 = cvB0; cvuB1 = cvB1;
-          cguA0 = cgA0; cguA1 = cgA1; cguB0 = cgB0; cguB1 = cgB1;
+          VOD = VOL[r]; cdA = clA[r]; cdB = clB[r];
+          VOL[r] = VO; clA[r] = cvA; clB[r] = cvB;
+          VOU = VO; GU = G; cvuA = cvA; cvuB = cvB; cguA = cgA; cguB = cgB;
         };
 #pragma unroll
         for (int g = 0; g < K / 4; g++) {
@@ -549,24 +545,21 @@ __device__ __forceinline__ void align_two_nw(const uint32_t* __restrict__ prof, 
           cell(K - 2, PL.x, PH.x, MA.x, MB.x);
           cell(K - 1, PL.y, PH.y, MA.y, MB.y);
         }
-        uVO = VOU; uG = GU; ucvA0 = cvuA0; ucvA1 = cvuA1; ucvB0 = cvuB0; ucvB1 = cvuB1;
-        ucgA0 = cguA0; ucgA1 = cguA1; ucgB0 = cguB0; ucgB1 = cguB1;
+        uVO = VOU; uG = GU; ucvA = cvuA; ucvB = cvuB; ucgA = cguA; ucgB = cguB;
         // the (m, n) cells: lane tm of pass pm holds them after steps sA / sB
         if (p == pm && lane == tm && (s == sA || s == sB)) {
 #pragma unroll
           for (int r = 0; r < K; r++)
             if (r == rm) {
-              if (s == sA) { capA0 = clA0[r]; capA1 = clA1[r]; }
-              if (s == sB) { capB0 = clB0[r]; capB1 = clB1[r]; }
+              if (s == sA) capA = clA[r];
+              if (s == sB) capB = clB[r];
             }
         }
         if (lane == 31 && p + 1 < passes) {
           const int j = s - 31;
           if (j >= 0 && j < ncols) {
-            uint32_t* w = scr + (long)j * kScrWordsNw;
-            *reinterpret_cast<uint4*>(w) = make_uint4(uVO, uG, ucvA0, ucvA1);
-            *reinterpret_cast<uint4*>(w + 4) = make_uint4(ucvB0, ucvB1, ucgA0, ucgA1);
-            *reinterpret_cast<uint4*>(w + 8) = make_uint4(ucgB0, ucgB1, 0u, 0u);
+            *reinterpret_cast<uint4*>(scr + (long)j * kScrWords) = make_uint4(uVO, uG, ucvA, ucvB);
+            *reinterpret_cast<uint2*>(scr + (long)j * kScrWords + 4) = make_uint2(ucgA, ucgB);
           }
         }
       }
@@ -574,28 +567,20 @@ __device__ __forceinline__ void align_two_nw(const uint32_t* __restrict__ prof, 
     __syncwarp();
   }
   // the holder of (m, n) is lane tm: everyone gets its counters
-  capA0 = __shfl_sync(0xffffffffu, capA0, tm);
-  capA1 = __shfl_sync(0xffffffffu, capA1, tm);
-  capB0 = __shfl_sync(0xffffffffu, capB0, tm);
-  capB1 = __shfl_sync(0xffffffffu, capB1, tm);
+  capA = __shfl_sync(0xffffffffu, capA, tm);
+  capB = __shfl_sync(0xffffffffu, capB, tm);
 }
 
-// NW distance (Salsa.NeedlemanWunschTPL/Program.cs:547-571, :583-604) from the counters of (m, n).
-__device__ __forceinline__ int16_t engine_nw_distance(uint32_t w0, uint32_t w1, int m, int n, int protein) {
-  const int count = (int)(w0 & 0xFFFFu), len = (int)(w0 >> 16);
-  if (protein) return fraction_distance(count, len);
-  const int lead = (int)(w1 >> 16);
-  const int run = (int)(int16_t)(w1 & 0xFFFFu);
-  int trimmed = len - lead - (run < 0 ? -run : run);
-  if (m == 0 || n == 0) trimmed = 0;
-  return fraction_distance(count, trimmed);
+// NW distance (Salsa.NeedlemanWunschTPL/Program.cs:547-571, :583-604) from the counter word of
+// (m, n): counted columns over the trimmed (nucleic) or whole (protein) alignment.
+__device__ __forceinline__ int16_t engine_nw_distance(uint32_t w) {
+  return fraction_distance((int)(w & 0xFFFFu), (int)(w >> 16));
 }
 
-// Counters of a pair with an empty side: all of it one gap run along the boundary.
-__device__ __forceinline__ void nw_boundary(int m, int n, uint32_t& w0, uint32_t& w1) {
-  if (m == 0 && n == 0) { w0 = 0u; w1 = 0u; }
-  else if (m == 0) { w0 = (uint32_t)n << 16; w1 = ((uint32_t)n << 16) | (uint32_t)((-n) & 0xFFFF); }
-  else { w0 = (uint32_t)m << 16; w1 = ((uint32_t)m << 16) | (uint32_t)(m & 0xFFFF); }
+// Counter word of a pair with an empty side: all of it one gap run along the boundary (nucleic:
+// all of it trimmed away).
+__device__ __forceinline__ uint32_t nw_boundary(int m, int n, int protein) {
+  return protein ? (uint32_t)(m + n) << 16 : 0u;
 }
 
 // Lexicographic (max score, min row) over the warp; lane 0 ends with the winner.
@@ -626,7 +611,7 @@ __global__ void __launch_bounds__(warps_of(K, KIND) * 32, ctas_of(K, KIND)) engi
   static_assert(kKindScore == kKindScoreShape, "score kind");
   constexpr bool NW = KIND == kKindNw;
   constexpr int kEngWarps = warps_of(K, KIND);
-  constexpr int kScr = NW ? kScrWordsNw : kScrWords;
+  constexpr int kScr = kScrWords;
   extern __shared__ __align__(16) uint8_t smem[];
   uint32_t* prof = reinterpret_cast<uint32_t*>(smem);
   const int A1 = J.A + 1;
@@ -805,15 +790,15 @@ __global__ void __launch_bounds__(warps_of(K, KIND) * 32, ctas_of(K, KIND)) engi
         continue;
       }
       if constexpr (NW) {
-        uint32_t a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+        uint32_t wa = 0, wb = 0;
         if (m > 0 && ncols > 0)
-          align_two_nw<K, NP>(prof, J.mpad, passes, m, ca, cb, ncols, nA, nB, J, scr, lane, a0, a1, b0, b1);
+          align_two_nw<K, NP>(prof, J.mpad, passes, m, ca, cb, ncols, nA, nB, J, scr, lane, wa, wb);
         if (lane == 0) {
-          if (m == 0 || nA == 0) nw_boundary(m, nA, a0, a1);
-          emit(J, q, dA, engine_nw_distance(a0, a1, m, nA, J.protein));
+          if (m == 0 || nA == 0) wa = nw_boundary(m, nA, J.protein);
+          emit(J, q, dA, engine_nw_distance(wa));
           if (dB >= 0) {
-            if (m == 0 || nB == 0) nw_boundary(m, nB, b0, b1);
-            emit(J, q, dB, engine_nw_distance(b0, b1, m, nB, J.protein));
+            if (m == 0 || nB == 0) wb = nw_boundary(m, nB, J.protein);
+            emit(J, q, dB, engine_nw_distance(wb));
           }
           atomicAdd(J.stats + 1, (unsigned long long)(1 + (dB >= 0)));
         }
@@ -1010,11 +995,10 @@ long k_weight(int k) {
 
 // Rows per lane and passes for a query of m rows: fewest padded rows, then fewest passes.
 void choose_k(int m, int kov, int* K, int* passes, bool nw = false, const int* tuned = nullptr) {
-  if (nw && kov > 14) kov = 14;  // NW kernels stop at 14 rows per lane
+  (void)nw;  // NW takes the same tile shapes
   if (kov) { *K = kov; *passes = std::max(1, (m + 32 * kov - 1) / (32 * kov)); return; }
   long best = -1;
   for (int k : kKs) {
-    if (nw && k > 14) continue;
     const int p = std::max(1, (m + 32 * k - 1) / (32 * k));
     // rows computed (padding included) times the per-row cost of that K (few rows per lane do
     // not amortise the per-step shuffles, loads and column bookkeeping); ties go to fewer passes
@@ -1311,7 +1295,6 @@ class EngineImpl : public Engine {
     cudaEventCreate(&t1);
     double rate[kNumK] = {0};
     for (int x = 0; x < kNumK; x++) {
-      if (nw && kKs[x] > 14) continue;
       opt_.k_override = kKs[x];
       opt_.m_lo = 32 * (kKs[x] - 2);
       opt_.m_hi = 32 * kKs[x];
@@ -1571,7 +1554,7 @@ class EngineImpl : public Engine {
       const int occ = std::max(1, occupancy_k(bn.K, A, pl.kind, bn.smem));
       bn.grid = (int)std::min<long>((long)P.sms * occ, (long)bn.items.size());
       bn.scratch_off = scr_words;
-      if (bn.max_passes > 1) scr_words += (size_t)bn.grid * warps_of(bn.K, pl.kind) * B.maxcol * (nw ? kScrWordsNw : kScrWords);
+      if (bn.max_passes > 1) scr_words += (size_t)bn.grid * warps_of(bn.K, pl.kind) * B.maxcol * kScrWords;
       bn.rowbuf_off = row_words;
       if (pl.kind == kKindScore) row_words += (size_t)bn.grid * warps_of(bn.K, pl.kind) * bn.mpad;
     }
