@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/swgb200.h"
+#include "swg_log.cuh"
 #include "swg_device.cuh"
 #include "swg_engine.h"
 #include "swg_serve.h"
@@ -474,7 +475,7 @@ int sw_align_pair(sw_ctx* ctx, const uint8_t* s1, int32_t m, const uint8_t* s2, 
       if (t1 <= eps || t2 <= eps) v = 10.0;
       else {
         volatile double a = 1.0 - 2.0 * P - Q;
-        volatile double l1 = -0.5 * std::log(a), l2 = 0.25 * std::log(t2);
+        volatile double l1 = -0.5 * swg::cr_log(a), l2 = 0.25 * swg::cr_log(t2);
         v = l1 - l2;
       }
       if (ms && v > 10.0) v = 10.0;
@@ -488,7 +489,7 @@ int sw_align_pair(sw_ctx* ctx, const uint8_t* s1, int32_t m, const uint8_t* s2, 
         }
         v = 10.0;
       } else {
-        v = -0.75 * std::log(d);
+        v = -0.75 * swg::cr_log(d);
       }
     }
     volatile double x = v * 32767.0;
@@ -538,7 +539,7 @@ static int16_t traced_distance(const sw_ctx* ctx, const char* a, const char* b, 
       volatile double t1 = 1.0 - (2.0 * P + Q), t2 = 1.0 - 2.0 * Q;
       if (t1 <= eps || t2 <= eps) v = 10.0;
       else {
-        volatile double l1 = -0.5 * std::log(1.0 - 2.0 * P - Q), l2 = 0.25 * std::log(t2);
+        volatile double l1 = -0.5 * swg::cr_log(1.0 - 2.0 * P - Q), l2 = 0.25 * swg::cr_log(t2);
         v = l1 - l2;
       }
       if (capped && v > 10.0) v = 10.0;
@@ -548,7 +549,7 @@ static int16_t traced_distance(const sw_ctx* ctx, const char* a, const char* b, 
         if (!capped) { *throws = 1; return 0; }
         v = 10.0;
       } else {
-        v = -0.75 * std::log(d);
+        v = -0.75 * swg::cr_log(d);
       }
     }
     volatile double x = v * 32767.0;

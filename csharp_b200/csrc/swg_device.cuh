@@ -19,6 +19,8 @@
 #pragma once
 #include <cstdint>
 
+#include "swg_log.cuh"
+
 namespace swg {
 
 constexpr int kNegInf = -(1 << 28);  // -infinity of the float DP (only ever loses a max)
@@ -159,8 +161,8 @@ __device__ __forceinline__ double kimura2_value(int len, int diag, int ts, int t
   const double Q = __ddiv_rn((double)tv, __dsub_rn(length, gapc));
   if (__dsub_rn(1.0, __dadd_rn(__dmul_rn(2.0, P), Q)) <= kDoubleEpsilon) return 10.0;
   if (__dsub_rn(1.0, __dmul_rn(2.0, Q)) <= kDoubleEpsilon) return 10.0;
-  return __dsub_rn(__dmul_rn(-0.5, log(__dsub_rn(__dsub_rn(1.0, __dmul_rn(2.0, P)), Q))),
-                   __dmul_rn(0.25, log(__dsub_rn(1.0, __dmul_rn(2.0, Q)))));
+  return __dsub_rn(__dmul_rn(-0.5, cr_log(__dsub_rn(__dsub_rn(1.0, __dmul_rn(2.0, P)), Q))),
+                   __dmul_rn(0.25, cr_log(__dsub_rn(1.0, __dmul_rn(2.0, Q)))));
 }
 
 // JukesCantor (Alignment.cs:314-348): 1 - (4/3)(diff / non-gap columns); false where the
@@ -169,7 +171,7 @@ __device__ __forceinline__ bool jukes_cantor_value(int len, int diag, int identi
   const double length = (double)len, gapc = (double)(len - diag);
   const double d = __dsub_rn(1.0, __dmul_rn(4.0 / 3.0, __ddiv_rn((double)(diag - identical), __dsub_rn(length, gapc))));
   if (d <= kDoubleEpsilon) return false;
-  *out = __dmul_rn(-0.75, log(d));
+  *out = __dmul_rn(-0.75, cr_log(d));
   return true;
 }
 
