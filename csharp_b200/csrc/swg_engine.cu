@@ -1827,8 +1827,8 @@ class QueryRunnerImpl : public QueryRunner {
     int rc = build_base(B_, P, msg);
     if (rc) return rc;
     N_ = P.nseq;
-    lanes16_ = !(B_.alpha > kMaxAlpha16 || P.mode == kModeNw || P.lanes == SW_LANES_32 || B_.alpha == 0 ||
-                 (P.dist_fn != 0 && !P.protein));
+    nw_ = P.mode == kModeNw;
+    lanes16_ = !(B_.alpha > kMaxAlpha16 || P.lanes == SW_LANES_32 || B_.alpha == 0 || (P.dist_fn != 0 && !P.protein));
     // database chunks in length order
     for (int c0 = 0; c0 < N_; c0 += kQueryChunk) {
       const int c1 = std::min(N_, c0 + kQueryChunk);
@@ -1859,14 +1859,26 @@ class QueryRunnerImpl : public QueryRunner {
         maxS = std::max(maxS, v);
         minS = std::min(minS, v);
       }
-    bias_ = std::max(std::max(P.o + 2 * P.e, -minS), 1);
+    if (nw_) {
+      // NW lanes hold value + bias with the bias above the all-gap bound of every cell a pass
+      // touches: query rows padded by up to 32 x 16 - 1, database columns by up to 63.  The
+      // largest bias that still holds the highest score of any pair leaves the most room for long
+      // queries; a query beyond that length (nw_qmax_) goes to 32-bit lanes.
+      const long bias = 32767L - (long)maxS * (B_.maxcol + 1);
+      const long fixed = 3L * P.o + 2L * P.e + (512L + B_.maxcol + 64) * P.e - minS;
+      nw_qmax_ = bias > fixed && P.e > 0 ? (int)std::min<long>((bias - fixed) / P.e, 32767) : 0;
+      if (nw_qmax_ < 1) { lanes16_ = false; return SW_OK; }
+      bias_ = (int)bias;
+    } else {
+      bias_ = std::max(std::max(P.o + 2 * P.e, -minS), 1);
+    }
     max_s_ = maxS;
     thresh_ = 32767 - bias_ - max_s_;
     std::vector<int32_t> qtab((size_t)128 * A1);
     std::vector<uint32_t> qflag((size_t)128 * A1, 0u);
     for (int x = 0; x < 128; x++)
       for (int c = 0; c < A1; c++) {
-        int v = -bias_;
+        int v = nw_ ? 0 : -bias_;  // padding (NW: 0 keeps its values inside the bias's bound)
         uint32_t f = 0;
         if (x != kPadCode && c != A) {
           v = P.h_scores[x * 128 + B_.letters[c]];
@@ -1879,7 +1891,7 @@ class QueryRunnerImpl : public QueryRunner {
     if ((rc = upload_vec(&d_qflag_, qflag, msg, "query flag table"))) return rc;
     // two passes where the engine uses them (the same rule): the score-only kernels, then the box
     // step with a table row per query residue byte
-    two_ = P.mode != kModeNw && std::min(P.o, P.e) >= 2 && P.o >= 3 * max_s_ && P.e >= 3;
+    two_ = !nw_ && std::min(P.o, P.e) >= 2 && P.o >= 3 * max_s_ && P.e >= 3;
     if (two_) {
       std::vector<int32_t> qsc((size_t)128 * A1), qscf((size_t)128 * A1);
       for (int x = 0; x < 128; x++)
@@ -1902,11 +1914,12 @@ class QueryRunnerImpl : public QueryRunner {
 
   void plan_query(int slot, int m, std::vector<QueryItem>* items) const override {
     int K = 0, passes = 0;
-    bool fits = lanes16_;
+    bool fits = lanes16_ && (!nw_ || m <= nw_qmax_);
     if (fits) {
       choose_k(m, 0, &K, &passes);
       // a profile beyond shared memory (queries of several thousand residues): 32-bit lanes
-      fits = engine_smem(B_.alpha, passes * 32 * K, B_.maxcol, K) <= 227 * 1024;
+      fits = engine_smem(B_.alpha, passes * 32 * K, B_.maxcol, K, nw_ ? kKindNw : two_ ? kKindScore : kKindSw) <=
+             227 * 1024;
     }
     for (size_t c = 0; c < chunk_lo_.size(); c++) {
       QueryItem it;
@@ -1970,7 +1983,7 @@ class QueryRunnerImpl : public QueryRunner {
     // per-bin launch shape and scratch (bins run concurrently, each multi-pass bin has its own;
     // two passes: each bin its own rows' bounds too)
     const int A = B_.alpha;
-    const int kind = two_ ? kKindScore : kKindSw;
+    const int kind = nw_ ? kKindNw : two_ ? kKindScore : kKindSw;
     std::vector<size_t> smem(ls.size()), scr_off(ls.size()), row_off(ls.size());
     std::vector<int> grid(ls.size());
     size_t scr_words = 0, row_words = 0;
@@ -2006,7 +2019,7 @@ class QueryRunnerImpl : public QueryRunner {
       std::memset(&J, 0, sizeof(J));
       J.code = B_.d_code; J.off = P_.off; J.sorted = B_.d_sorted;
       J.A = A; J.o = P_.o; J.e = P_.e; J.bias = bias_; J.thresh = thresh_;
-      J.mode = P_.mode; J.ranks = 1; J.nseq = N_;
+      J.mode = P_.mode; J.ranks = 1; J.nseq = N_; J.protein = P_.protein;
       J.maxcol = B_.maxcol;
       J.rerun = W.d_rerun; J.rerun_count = W.d_rerun_count; J.rerun_cap = (int)rerun_cap;
       J.stats = W.d_stats;
@@ -2176,6 +2189,8 @@ class QueryRunnerImpl : public QueryRunner {
   int32_t* d_qtab_ = nullptr;
   uint32_t* d_qflag_ = nullptr;
   bool two_ = false;          // SW-Gotoh with gap costs that suit the box step: two passes
+  bool nw_ = false;           // global alignment (the NW kernels)
+  int nw_qmax_ = 0;           // NW: longest query the 16-bit lanes' bias covers
   int32_t* d_qbsc_ = nullptr;   // [128 * (A+1)] box step tables (query residue byte x database code)
   int32_t* d_qbscf_ = nullptr;
   WaveBuf wb_[2];

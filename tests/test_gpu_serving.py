@@ -106,6 +106,31 @@ def test_protein_database_matches_oracle(cs, oracle_mod):
     np.testing.assert_array_equal(r["out"], _expected(cs, oracle_mod, queries, db, "BLOSUM62", 10, 1, atype=0))
 
 
+@pytest.mark.parametrize("matrix,atype,o,e", [("EDNAFULL", 1, 16, 4), ("BLOSUM62", 0, 10, 1)])
+def test_nw_database_matches_oracle(cs, oracle_mod, matrix, atype, o, e):
+    """NW (global) serving on 16-bit lanes, with a query longer than the lanes' bias covers (it
+    goes to 32-bit lanes) and empty / one-residue queries."""
+    from csharp_b200 import synth
+    rng = np.random.default_rng(73 + atype)
+    sc = cs.ScoringMatrix.Load(matrix).Scores
+    if atype:
+        db = _dna(150, 74, 1, 500)
+        queries = _dna(6, 75, 20, 400) + [b"", b"G", _dna(1, 76, 6000, 6000)[0]]
+    else:
+        db = [s.tobytes() for s in synth.protein_family(120, 5, rng.integers(5, 300, 120), 77, sc)]
+        queries = [s.tobytes() for s in synth.protein_family(5, 2, rng.integers(5, 300, 5), 78, sc)] + [b"W"]
+    eng = cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=cs.NW, alignment_type=atype)
+    eng.upload(db)
+    r = eng.wait(eng.submit(queries))
+    concat, off = cs.pack_sequences(list(queries) + list(db))
+    nq, nd = len(queries), len(db)
+    ii = np.repeat(np.arange(nq), nd)
+    jj = np.tile(np.arange(nq, nq + nd), nq)
+    want = oracle_mod.nw_pairs(concat, off, ii, jj, sc[:127, :127].astype(np.float32), float(o), float(e),
+                               protein=not atype, threads=os.cpu_count()).reshape(nq, nd)
+    np.testing.assert_array_equal(r["out"], want)
+
+
 def test_submit_errors(cs):
     eng = cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4)
     with pytest.raises(cs.SwError):  # no database yet
