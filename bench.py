@@ -327,11 +327,12 @@ def _timed(stream, fn):
     return b.elapsed_time(e)
 
 
-def config_sets(cs):
-    """Configurations 1, 2 and 4: (name, description, sequences, matrix, open, extend, mode, type)."""
+def config_sets(cs, only=None, n=None):
+    """Configurations 1, 2 and 4: (name, description, sequences, matrix, open, extend, mode, type).
+    only: the names to keep; n: the first n sequences of each (a smaller case, for profiling)."""
     from csharp_b200 import synth
     bl = cs.ScoringMatrix.Load("BLOSUM62").Scores
-    return [
+    sets = [
         ("cfg1", "plain SW-Gotoh: 1,000 DNA, 20 roots of 500 nt, lengths 200-600, EDNAFULL 16/4",
          synth.config1(), "EDNAFULL", 16, 4, cs.SWG_MPI, cs.NUCLEIC),
         ("cfg2", "NW global: 10,000 DNA, lengths uniform 300-500, 100 roots, EDNAFULL 16/4",
@@ -339,6 +340,11 @@ def config_sets(cs):
         ("cfg4", "protein SW-Gotoh: 20,000 sequences (20 amino acids, lengths 100-1000, 500 roots), BLOSUM62 10/1",
          synth.config4(bl), "BLOSUM62", 10, 1, cs.SWG_MPI, cs.PROTEIN),
     ]
+    if only:
+        sets = [s for s in sets if s[0] in only]
+    if n:
+        sets = [(s[0], s[1] + f" (first {n} sequences)", s[2][:n]) + tuple(s[3:]) for s in sets]
+    return sets
 
 
 def config_parity_pairs(n, name, rng):
@@ -403,6 +409,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="built-in rows-per-lane costs instead of measured ones")
     ap.add_argument("--serving-only", action="store_true", help="only the serving workload (one JSON line)")
     ap.add_argument("--configs-only", action="store_true", help="only configurations 1, 2 and 4 (one JSON line)")
+    ap.add_argument("--only", default="", help="with --configs-only: comma-separated names (cfg1,cfg2,cfg4)")
+    ap.add_argument("--config-n", type=int, default=0, help="with --configs-only: first N sequences of each")
     ap.add_argument("--serve-jobs", type=int, default=SERVE["jobs"])
     ap.add_argument("--box-reg", type=int, default=-1, choices=[-1, 0, 1],
                     help="two-pass box step: 1 register box step first, 0 warp box kernel only (-1: engine default)")
@@ -423,7 +431,7 @@ def main():
     if a.configs_only:
         import torch
         import csharp_b200 as cs
-        sets = config_sets(cs)
+        sets = config_sets(cs, [x for x in a.only.split(",") if x], a.config_n)
         picks = {s[0]: config_parity_pairs(len(s[2]), s[0], np.random.default_rng(21)) for s in sets}
         parity = start_parity(cs, sets, picks, threads)
         st = torch.cuda.Stream()
