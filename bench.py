@@ -416,7 +416,12 @@ def main():
                     help="two-pass box step: 1 register box step first, 0 warp box kernel only (-1: engine default)")
     ap.add_argument("--third-pass", type=int, default=-1, choices=[-1, 0, 1],
                     help="two-pass give-ups: 1 one-pass 16-bit counter kernel, 0 32-bit lanes (-1: engine default)")
+    ap.add_argument("--engine-option", action="append", default=[], metavar="KEY=VALUE",
+                    help="any sw_set_option knob for every engine of the run (repeatable)")
     a = ap.parse_args()
+    for kv in a.engine_option:
+        k, v = kv.split("=", 1)
+        ENGINE_OPTIONS[k] = int(v)
     if a.box_reg >= 0:
         ENGINE_OPTIONS["box_reg"] = a.box_reg
     if a.third_pass >= 0:

@@ -1891,7 +1891,8 @@ class QueryRunnerImpl : public QueryRunner {
     if ((rc = upload_vec(&d_qflag_, qflag, msg, "query flag table"))) return rc;
     // two passes where the engine uses them (the same rule): the score-only kernels, then the box
     // step with a table row per query residue byte
-    two_ = !nw_ && std::min(P.o, P.e) >= 2 && P.o >= 3 * max_s_ && P.e >= 3;
+    two_ = !nw_ && std::min(P.o, P.e) >= 2 &&
+           (P.two_pass == 2 || (P.two_pass == 1 && P.o >= 3 * max_s_ && P.e >= 3));
     if (two_) {
       std::vector<int32_t> qsc((size_t)128 * A1), qscf((size_t)128 * A1);
       for (int x = 0; x < 128; x++)

@@ -21,6 +21,7 @@ struct EngineParams {
   int o, e;
   int mode, protein, lanes;
   int dist_fn = 0;         // SW_DIST_*: Kimura2 / JukesCantor run on 32-bit lanes
+  int two_pass = 1;        // serving: the engine's two_pass option (0 never, 1 where it suits, 2 always)
   int* throws = nullptr;   // device flag: SWG-MPI JukesCantor met log(0)
   int ranks;
   int row_lo = 0, row_hi = -1;  // queries (s1 indices) aligned; row_hi < 0: all
