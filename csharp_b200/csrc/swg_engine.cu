@@ -645,7 +645,7 @@ __global__ void __launch_bounds__(warps_of(K, KIND) * 32, ctas_of(K, KIND)) engi
       const int4 item = J.items[it];
       q = item.x; c0 = item.y; c1 = item.z; passes = item.w;
     }
-    if (threadIdx.x == 0) atomicAdd(J.stats, 1ull);
+    if (threadIdx.x == 0 && !J.fb_cnt) atomicAdd(J.stats, 1ull);  // planned items only
     const int m = J.qmode ? J.qlen[q] : (int)(J.off[q + 1] - J.off[q]);
     const int mrows = passes * 32 * K;
     // query profile (rows beyond m and the pad column score -bias, count nothing)
