@@ -291,6 +291,18 @@ static int check_throws(sw_ctx* ctx) {
 
 static swg::EngineParams db_params(sw_ctx* ctx);
 
+// After the context's stream is idle: SW_E_CUDA if the last engine launch recorded a violation of
+// its kernels' self-checks (a work item or pair outside the plan's bounds; it was skipped).
+static int check_kernel(sw_ctx* ctx) {
+  if (!ctx->engine) return SW_OK;
+  const int64_t v = ctx->engine->stat("kernel_error");
+  if (v <= 0) return SW_OK;
+  char buf[112];
+  std::snprintf(buf, sizeof buf, "engine self-check %lld failed at index %lld", (long long)(v >> 48),
+                (long long)(v & 0xFFFFFFFFLL));
+  return fail(ctx, SW_E_CUDA, buf);
+}
+
 // One engine job: the queries row_lo..row_hi of a `ranks`-rank run, or (block 1 / 2) the diagonal /
 // off-diagonal block of those rows by the columns col_lo..col_hi, with d_out pointing at the
 // block's element (0, 0).
@@ -410,6 +422,7 @@ int sw_compute_block(sw_ctx* ctx, int32_t rs, int32_t re, int32_t cs, int32_t ce
   CK(cudaStreamSynchronize(ctx->stream), "compute block");
   for (size_t k = 0; k < keep.size(); k++) out[k * (size_t)ld + k] = keep[k];
   if (pairs) *pairs = J.npairs;
+  if ((rc = check_kernel(ctx))) return rc;
   return check_throws(ctx);
 }
 
@@ -744,7 +757,7 @@ int sw_query(sw_ctx* ctx, const char* key, int64_t* value) {
   }
   if (k != "launches" && k != "bins" && k != "alphabet" && k != "items" && k != "lane16_pairs" &&
       k != "tripped" && k != "planned_items" && k != "box_fallbacks" && k != "box_spilled" &&
-      k != "box_third_pass")
+      k != "box_third_pass" && k != "kernel_error")
     return fail(ctx, SW_E_ARG, "unknown counter " + k);
   *value = ctx->engine ? ctx->engine->stat(key) : 0;
   return SW_OK;
@@ -815,6 +828,7 @@ int sw_all_pairs(sw_ctx* ctx, int32_t ranks, int16_t* out, int64_t ld, int64_t* 
   if ((rc = sw_all_pairs_device(ctx, ranks, ctx->d_stage, (int64_t)N, pairs, cells))) return rc;
   if (N) CK(cudaMemcpy2DAsync(out, (size_t)ld * 2, ctx->d_stage, N * 2, N * 2, N, cudaMemcpyDeviceToHost, ctx->stream), "copy result");
   CK(cudaStreamSynchronize(ctx->stream), "all pairs");
+  if ((rc = check_kernel(ctx))) return rc;
   return check_throws(ctx);
 }
 

@@ -81,6 +81,8 @@ struct EngineJob {
   int* rerun_count;
   int rerun_cap;
   int mpad;                 // profile rows staged (passes * 32 * K of the bin)
+  long long scratch_words;  // pass scratch from `scratch` on, and rows' bounds from `rowbuf` on
+  long long rowbuf_words;   // (the kernel checks its slots against them)
   int protein;              // NW distance rule: similarity over the full length
   unsigned long long* stats; // [0] items taken, [1] pairs finished in 16-bit lanes, [2] tripped
   // third pass (fb_cnt != nullptr): item it is query fb_lo + it with the fb_cnt[it] partners at
@@ -603,6 +605,11 @@ __device__ __forceinline__ void emit(const EngineJob& J, int q, int d, int16_t d
   if (J.mirror) J.out[(long long)d * J.ld + q] = dist;
 }
 
+// The first self-check violation of a launch: stats[7] = site << 48 | index (0: none).
+__device__ __forceinline__ void record_error(const EngineJob& J, int site, int index) {
+  atomicCAS(J.stats + 7, 0ull, ((unsigned long long)site << 48) | (unsigned long long)(unsigned)index);
+}
+
 // What a kernel instantiation computes per pair.
 enum { kKindSw = 0, kKindNw = 1, kKindScore = 2 };
 
@@ -646,8 +653,15 @@ __global__ void __launch_bounds__(warps_of(K, KIND) * 32, ctas_of(K, KIND)) engi
       q = item.x; c0 = item.y; c1 = item.z; passes = item.w;
     }
     if (threadIdx.x == 0 && !J.fb_cnt) atomicAdd(J.stats, 1ull);  // planned items only
-    const int m = J.qmode ? J.qlen[q] : (int)(J.off[q + 1] - J.off[q]);
     const int mrows = passes * 32 * K;
+    // self-checks (CTA-uniform): a work item outside the plan's bounds is recorded and skipped
+    if ((!J.qmode && (q < 0 || q >= J.nseq)) || c1 < c0 || mrows > J.mpad ||
+        (passes > 1 && ((long long)blockIdx.x + 1) * kEngWarps * J.maxcol * kScr > J.scratch_words) ||
+        (rowb && ((long long)blockIdx.x + 1) * kEngWarps * J.mpad > J.rowbuf_words)) {
+      if (threadIdx.x == 0) record_error(J, 1, it);
+      continue;  // every thread has read s_item
+    }
+    const int m = J.qmode ? J.qlen[q] : (int)(J.off[q + 1] - J.off[q]);
     // query profile (rows beyond m and the pad column score -bias, count nothing)
     const bool rebuild = (q != s_q);
     __syncthreads();
@@ -703,9 +717,17 @@ __global__ void __launch_bounds__(warps_of(K, KIND) * 32, ctas_of(K, KIND)) engi
       if (pi >= cnt) break;
       const int dA = list[pi];
       const int dB = (pi + 1 < cnt) ? list[pi + 1] : -1;
+      if (dA < 0 || dA >= J.nseq || dB >= J.nseq) {  // self-check (warp-uniform)
+        if (lane == 0) record_error(J, 2, dA);
+        continue;
+      }
       const int nA = (int)(J.off[dA + 1] - J.off[dA]);
       const int nB = dB >= 0 ? (int)(J.off[dB + 1] - J.off[dB]) : 0;
       const int ncols = max(nA, nB);
+      if (ncols > J.maxcol) {
+        if (lane == 0) record_error(J, 3, dA);
+        continue;
+      }
       const uint8_t* sa = J.code + J.off[dA];
       const uint8_t* sb = dB >= 0 ? J.code + J.off[dB] : sa;
       for (int k = lane; k < 32 + ncols; k += 32) {
@@ -1247,13 +1269,14 @@ class EngineImpl : public Engine {
     }
     if (k == "alphabet") return base_ ? base_->alpha : 0;
     if (k == "items" || k == "lane16_pairs" || k == "tripped" || k == "box_fallbacks" || k == "box_spilled" ||
-        k == "box_third_pass") {
+        k == "box_third_pass" || k == "kernel_error") {
       if (!last_->d_stats) return 0;
       unsigned long long h[kNumStats] = {};
       cudaDeviceSynchronize();
       cudaMemcpy(h, last_->d_stats, sizeof(h), cudaMemcpyDeviceToHost);
       return (int64_t)(k == "items" ? h[0] : k == "lane16_pairs" ? h[1] : k == "tripped" ? h[2]
-                       : k == "box_fallbacks" ? h[3] : k == "box_spilled" ? h[4] : h[5]);
+                       : k == "box_fallbacks" ? h[3] : k == "box_spilled" ? h[4]
+                       : k == "box_third_pass" ? h[5] : h[7]);
     }
     if (k == "planned_items") {
       int64_t n = 0;
@@ -1686,7 +1709,9 @@ class EngineImpl : public Engine {
         J.counter = pl.d_counters + b;
         J.mpad = bn.mpad;
         J.scratch = B.d_scratch + bn.scratch_off;
+        J.scratch_words = (long long)(B.scratch_bytes / 4) - (long long)bn.scratch_off;
         J.rowbuf = two ? B.d_rowbuf + bn.rowbuf_off : nullptr;
+        J.rowbuf_words = two ? (long long)(B.rowbuf_bytes / 4) - (long long)bn.rowbuf_off : 0;
         if ((e = launch_engine_k(bn.K, pl.kind, J, bn.grid, bn.smem, st)) != cudaSuccess) return e;
         if (fork) {
           if ((e = cudaEventRecord(join_[x], st)) != cudaSuccess) return e;
@@ -1745,6 +1770,8 @@ class EngineImpl : public Engine {
         F.counter = B.d_counts + 7;
         F.mpad = pl.fb_mpad;
         F.scratch = B.d_scratch;
+        F.scratch_words = (long long)(B.scratch_bytes / 4);
+        F.rowbuf_words = 0;
         F.rowbuf = nullptr;
         F.box = nullptr; F.boxwin = nullptr;
         if ((e = launch_engine_k(kFbK, kKindSw, F, pl.fb_grid, pl.fb_smem, P.stream)) != cudaSuccess) return e;
@@ -2040,7 +2067,9 @@ class QueryRunnerImpl : public QueryRunner {
         J.counter = W.d_counters + ls[x].b;
         J.mpad = ls[x].mpad;
         J.scratch = W.d_scratch + scr_off[x];
+        J.scratch_words = (long long)(W.scratch_bytes / 4) - (long long)scr_off[x];
         J.rowbuf = two_ ? W.d_rowbuf + row_off[x] : nullptr;
+        J.rowbuf_words = two_ ? (long long)(W.rowbuf_bytes / 4) - (long long)row_off[x] : 0;
         if ((e = launch_engine_k(ls[x].K, kind, J, grid[x], smem[x], s2)) != cudaSuccess) return cuda_err(e, msg);
         if (fork) {
           if ((e = cudaEventRecord(W.join[x], s2)) != cudaSuccess) return cuda_err(e, msg);

@@ -208,7 +208,9 @@ int sw_autotune(sw_ctx* ctx, int16_t* d_out, int64_t ld_out, int32_t weights[7])
  * in 16-bit lanes), "tripped" (16-bit lanes handed to 32-bit lanes), "box_spilled" (two-pass pairs
  * the register box step handed to the warp box kernel), "box_fallbacks" (two-pass pairs the box
  * step could not finish) and "box_third_pass" (those of them redone by the one-pass 16-bit counter
- * kernel; the rest go to 32-bit lanes).  Unknown keys are SW_E_ARG. */
+ * kernel; the rest go to 32-bit lanes) and "kernel_error" (0, or the first work item or pair the
+ * engine kernels' bounds self-checks rejected and skipped: site << 48 | index; the host-output
+ * calls return SW_E_CUDA when it is set).  Unknown keys are SW_E_ARG. */
 int sw_query(sw_ctx* ctx, const char* key, int64_t* value);
 
 /* ---- block handler without device allocation ------------------------------------------------ */
