@@ -846,7 +846,8 @@ static swg::EngineParams db_params(sw_ctx* ctx) {
   P.lanes = ctx->cfg.lanes;
   P.dist_fn = ctx->cfg.distance_fn;
   P.throws = ctx->d_throws;
-  P.two_pass = ctx->engine ? ctx->engine->options().two_pass : 1;
+  P.two_pass = ctx->engine ? ctx->engine->current_options().two_pass : 1;
+  P.third_pass = ctx->engine ? ctx->engine->current_options().third_pass : 1;
   P.ranks = 1;
   P.out = nullptr; P.ld = 0;
   P.sms = ctx->sms;

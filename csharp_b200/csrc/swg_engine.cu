@@ -26,6 +26,7 @@
 #include <cmath>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <numeric>
@@ -647,7 +648,8 @@ __global__ void __launch_bounds__(warps_of(K, KIND) * 32, ctas_of(K, KIND)) engi
         __syncthreads();  // every thread has read s_item
         continue;
       }
-      passes = max(1, (int)((J.off[q + 1] - J.off[q] + 32 * K - 1) / (32 * K)));
+      const int mq = J.qmode ? J.qlen[q] : (int)(J.off[q + 1] - J.off[q]);
+      passes = max(1, (mq + 32 * K - 1) / (32 * K));
     } else {
       const int4 item = J.items[it];
       q = item.x; c0 = item.y; c1 = item.z; passes = item.w;
@@ -968,10 +970,22 @@ auto with_kp(int K, int A, int kind, Fn fn) {
   });
 }
 
+// Raises an instantiation's dynamic shared-memory allowance to at least smem.  The attribute is
+// per function and process-wide (every context and thread launches the same kernels), so it only
+// ever grows: lowering it would fail launches of plans built earlier with a larger profile.
 cudaError_t allow_smem_k(int K, int A, int kind, size_t smem) {
-  return with_kp(K, A, kind, [&](auto kern, int) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int, int>, size_t> granted;  // (device, K, planes, kind)
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& g = granted[std::make_tuple(dev, K, planes_of(A), kind)];
+  if (smem <= g) return cudaSuccess;
+  const cudaError_t e = with_kp(K, A, kind, [&](auto kern, int) {
     return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   });
+  if (e == cudaSuccess) g = smem;
+  return e;
 }
 
 cudaError_t launch_engine_k(int K, int kind, const EngineJob& J, int grid, size_t smem, cudaStream_t st) {
@@ -994,11 +1008,12 @@ int occupancy_k(int K, int A, int kind, size_t smem) {
 // 3,000-sequence uniform 300-500 DNA job.
 long k_weight_nw(int k) {
   switch (k) {
-    case 4: return 120;
-    case 6: return 103;
-    case 8: return 105;
-    case 10: return 106;
-    case 12: return 106;
+    case 4: return 160;
+    case 6: return 127;
+    case 8: return 106;
+    case 10: return 107;
+    case 12: return 100;
+    case 14: return 105;
     default: return 100;
   }
 }
@@ -1250,6 +1265,7 @@ class EngineImpl : public Engine {
     last_ = nullptr;
     return opt_;
   }
+  const EngineOptions& current_options() const override { return opt_; }
   void set_plan_only(int v) override { opt_.plan_only = v; }
 
   int64_t stat(const char* key) const override {
@@ -1837,6 +1853,7 @@ class QueryRunnerImpl : public QueryRunner {
     cudaFree(d_qtab_); cudaFree(d_qflag_); cudaFree(d_qbsc_); cudaFree(d_qbscf_);
     for (auto& w : wb_) {
       cudaFree(w.d_box); cudaFree(w.d_win); cudaFree(w.d_cls[0]); cudaFree(w.d_cls[1]); cudaFree(w.d_counts);
+      cudaFree(w.d_fb); cudaFree(w.d_fbsorted); cudaFree(w.d_fbq);
       cudaFree(w.d_rowbuf);
       cudaFree(w.d_items); cudaFree(w.d_counters); cudaFree(w.d_stats); cudaFree(w.d_rerun);
       cudaFree(w.d_rerun_count); cudaFreeHost(w.h_items); cudaFreeHost(w.h_rerun); cudaFree(w.d_scratch);
@@ -1855,6 +1872,7 @@ class QueryRunnerImpl : public QueryRunner {
     if (rc) return rc;
     N_ = P.nseq;
     nw_ = P.mode == kModeNw;
+    third_ = P.third_pass != 0;
     lanes16_ = !(B_.alpha > kMaxAlpha16 || P.lanes == SW_LANES_32 || B_.alpha == 0 || (P.dist_fn != 0 && !P.protein));
     // database chunks in length order
     for (int c0 = 0; c0 < N_; c0 += kQueryChunk) {
@@ -2026,7 +2044,26 @@ class QueryRunnerImpl : public QueryRunner {
       row_off[x] = row_words;
       if (two_) row_words += (size_t)grid[x] * warps_of(ls[x].K, kind) * ls[x].mpad;
     }
+    // third pass (two passes): the box step's give-ups on the one-pass 16-bit counter kernel, the
+    // wave's longest query in passes of 512 rows, where its profile fits shared memory
+    int fb_nq = 0, fb_mpad = 0, fb_grid = 0;
+    size_t fb_smem = 0;
+    bool fb = false;
+    if (two_ && !ls.empty() && third_) {
+      int mrows = 0;
+      for (const QueryItem& it : items)
+        if (it.K) { fb_nq = std::max(fb_nq, it.slot + 1); mrows = std::max(mrows, it.passes * 32 * it.K); }
+      fb_mpad = ((mrows + 32 * kFbK - 1) / (32 * kFbK)) * 32 * kFbK;
+      fb_smem = engine_smem(A, fb_mpad, B_.maxcol, kFbK, kKindSw);
+      fb = fb_nq > 0 && fb_smem <= 227 * 1024 && allow_smem_k(kFbK, A, kKindSw, fb_smem) == cudaSuccess;
+      cudaGetLastError();
+      if (fb) {
+        fb_grid = P_.sms * std::max(1, occupancy_k(kFbK, A, kKindSw, fb_smem));
+        scr_words = std::max(scr_words, (size_t)fb_grid * warps_of(kFbK) * B_.maxcol * kScrWords);
+      }
+    }
     if (two_ && (rc = grow_box(W, std::max<size_t>((size_t)pairs16, 1), std::max<size_t>(row_words * 4, 16), msg))) return rc;
+    if (fb && (rc = grow_fbq(W, (size_t)fb_nq, msg))) return rc;
     if (scr_words * 4 > W.scratch_bytes) {
       // the earlier wave of this buffer is done; the other buffer's wave may run (own scratch)
       cudaFree(W.d_scratch);
@@ -2042,9 +2079,9 @@ class QueryRunnerImpl : public QueryRunner {
     if ((e = cudaMemsetAsync(W.d_stats, 0, sizeof(unsigned long long) * kNumStats, st)) != cudaSuccess) return cuda_err(e, msg);
     if (two_ && (e = cudaMemsetAsync(W.d_counts, 0, sizeof(int) * 8, st)) != cudaSuccess) return cuda_err(e, msg);
     set_int_kernel<<<1, 1, 0, st>>>(W.d_rerun_count, (int)big);
+    EngineJob J;
+    std::memset(&J, 0, sizeof(J));
     if (!ls.empty()) {
-      EngineJob J;
-      std::memset(&J, 0, sizeof(J));
       J.code = B_.d_code; J.off = P_.off; J.sorted = B_.d_sorted;
       J.A = A; J.o = P_.o; J.e = P_.e; J.bias = bias_; J.thresh = thresh_;
       J.mode = P_.mode; J.ranks = 1; J.nseq = N_; J.protein = P_.protein;
@@ -2091,9 +2128,34 @@ class QueryRunnerImpl : public QueryRunner {
       X.stats = W.d_stats;
       X.list_cap = (long long)W.box_cap;
       X.spill_count = W.d_counts + 1;  // no warp box kernel here: spill_cap 0 sends them on
+      if (fb) { X.fb = W.d_fb; X.fb_count = W.d_counts + 6; X.fb_cap = (long long)W.box_cap; }
       if ((e = launch_box_scan(X, P_.sms, st)) != cudaSuccess) return cuda_err(e, msg);
       for (int c = 0; c < 4; c++)
         if ((e = launch_box_band(X, c, P_.sms, st)) != cudaSuccess) return cuda_err(e, msg);
+      if (fb) {
+        // the give-ups bucketed by query slot, then the one-pass counter kernel on them
+        int* cnt = W.d_fbq;
+        int* start = cnt + W.fbq_cap;
+        int* fill = start + W.fbq_cap;
+        if ((e = cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)fb_nq, st)) != cudaSuccess) return cuda_err(e, msg);
+        const int g4 = std::max(1, P_.sms * 4);
+        fb_count_kernel<<<g4, 256, 0, st>>>(W.d_fb, W.d_counts + 6, (long long)W.box_cap, 0, cnt);
+        fb_scan_kernel<<<1, 1024, 0, st>>>(cnt, start, fill, fb_nq);
+        fb_scatter_kernel<<<g4, 256, 0, st>>>(W.d_fb, W.d_counts + 6, (long long)W.box_cap, 0, start, fill,
+                                              W.d_fbsorted);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(e, msg);
+        EngineJob F = J;
+        F.fb_cnt = cnt; F.fb_start = start; F.fb_lo = 0;
+        F.sorted = W.d_fbsorted;
+        F.items = nullptr; F.nitems = fb_nq;
+        F.counter = W.d_counts + 7;
+        F.mpad = fb_mpad;
+        F.scratch = W.d_scratch;
+        F.scratch_words = (long long)(W.scratch_bytes / 4);
+        F.rowbuf = nullptr; F.rowbuf_words = 0;
+        F.box = nullptr; F.boxwin = nullptr;
+        if ((e = launch_engine_k(kFbK, kKindSw, F, fb_grid, fb_smem, st)) != cudaSuccess) return cuda_err(e, msg);
+      }
     }
     // 32-bit lanes: pairs routed there by the static guard and 16-bit lanes that tripped
     PlainJob R;
@@ -2106,7 +2168,7 @@ class QueryRunnerImpl : public QueryRunner {
     R.dist_fn = P_.dist_fn; R.throws = P_.throws;
     R.carry = B_.d_carry;
     R.qseq = T.qseq; R.qoff = T.qoff; R.qlen = T.qlen; R.qout = T.qout;
-    const int g = big > 0 ? (int)(B_.carry_threads / 128) : P_.sms;
+    const int g = (big > 0 || two_) ? (int)(B_.carry_threads / 128) : P_.sms;
     // the 32-bit lanes' scratch is shared: after the other buffer's 32-bit kernel
     WaveBuf& other = wb_[(buf & 1) ^ 1];
     if (other.plain_used && (e = cudaStreamWaitEvent(st, other.plain_done, 0)) != cudaSuccess) return cuda_err(e, msg);
@@ -2143,7 +2205,26 @@ class QueryRunnerImpl : public QueryRunner {
     size_t box_cap = 0;
     uint32_t* d_rowbuf = nullptr;
     size_t rowbuf_bytes = 0;
+    // third pass: the give-ups (box_cap entries), their partners bucketed by query slot, and per
+    // slot counts / offsets / fill (fbq_cap each)
+    int2* d_fb = nullptr;
+    int* d_fbsorted = nullptr;
+    int* d_fbq = nullptr;
+    size_t fbq_cap = 0;
   };
+
+  int grow_fbq(WaveBuf& W, size_t nq, std::string* msg) {
+    if (nq <= W.fbq_cap) return SW_OK;
+    const size_t cap = std::max(nq, W.fbq_cap * 2);
+    cudaFree(W.d_fbq);
+    W.d_fbq = nullptr;
+    W.fbq_cap = 0;
+    if (cudaMalloc(&W.d_fbq, sizeof(int) * 3 * cap) != cudaSuccess) {
+      cudaGetLastError(); *msg = "cudaMalloc wave third-pass counts"; return SW_E_OOM;
+    }
+    W.fbq_cap = cap;
+    return SW_OK;
+  }
 
   // Two-pass buffers of a wave buffer for `pairs` box records and `rowbuf` bytes of rows' bounds.
   int grow_box(WaveBuf& W, size_t pairs, size_t rowbuf, std::string* msg) {
@@ -2153,8 +2234,12 @@ class QueryRunnerImpl : public QueryRunner {
     if (pairs > W.box_cap) {
       const size_t cap = std::max(pairs, W.box_cap * 2);
       cudaFree(W.d_box); cudaFree(W.d_win); cudaFree(W.d_cls[0]); cudaFree(W.d_cls[1]);
+      cudaFree(W.d_fb); cudaFree(W.d_fbsorted);
       W.d_box = nullptr; W.d_win = nullptr; W.d_cls[0] = W.d_cls[1] = nullptr; W.box_cap = 0;
+      W.d_fb = nullptr; W.d_fbsorted = nullptr;
       if (cudaMalloc(&W.d_box, sizeof(int4) * cap) != cudaSuccess ||
+          cudaMalloc(&W.d_fb, sizeof(int2) * cap) != cudaSuccess ||
+          cudaMalloc(&W.d_fbsorted, sizeof(int) * cap) != cudaSuccess ||
           cudaMalloc(&W.d_win, sizeof(uint32_t) * kRegWinWords * cap) != cudaSuccess ||
           cudaMalloc(&W.d_cls[0], sizeof(int) * cap) != cudaSuccess ||
           cudaMalloc(&W.d_cls[1], sizeof(int) * cap) != cudaSuccess) {
@@ -2220,6 +2305,7 @@ class QueryRunnerImpl : public QueryRunner {
   uint32_t* d_qflag_ = nullptr;
   bool two_ = false;          // SW-Gotoh with gap costs that suit the box step: two passes
   bool nw_ = false;           // global alignment (the NW kernels)
+  bool third_ = true;         // two passes: the box step's give-ups on 16-bit lanes (third pass)
   int nw_qmax_ = 0;           // NW: longest query the 16-bit lanes' bias covers
   int32_t* d_qbsc_ = nullptr;   // [128 * (A+1)] box step tables (query residue byte x database code)
   int32_t* d_qbscf_ = nullptr;

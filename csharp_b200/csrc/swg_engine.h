@@ -22,6 +22,7 @@ struct EngineParams {
   int mode, protein, lanes;
   int dist_fn = 0;         // SW_DIST_*: Kimura2 / JukesCantor run on 32-bit lanes
   int two_pass = 1;        // serving: the engine's two_pass option (0 never, 1 where it suits, 2 always)
+  int third_pass = 1;      // serving: the engine's third_pass option
   int* throws = nullptr;   // device flag: SWG-MPI JukesCantor met log(0)
   int ranks;
   int row_lo = 0, row_hi = -1;  // queries (s1 indices) aligned; row_hi < 0: all
@@ -56,7 +57,8 @@ class Engine {
   // The set's residues changed but not its lengths or letters: the plans and graphs stay valid;
   // the dense residue codes are rebuilt on the device from d_seq (ordered on st).
   virtual int refresh_codes(const uint8_t* d_seq, int64_t total, cudaStream_t st, std::string* msg) = 0;
-  virtual EngineOptions& options() = 0;
+  virtual EngineOptions& options() = 0;                 // for changing them: drops the plans
+  virtual const EngineOptions& current_options() const = 0;  // reading them keeps the plans
   virtual void set_plan_only(int v) = 0;  // keeps the plans (options() drops them)
   // Returns an SW_* status.
   virtual int run(const EngineParams& p, int64_t* pairs, int64_t* cells, int64_t* reruns,

@@ -48,14 +48,18 @@ def _engine(cs, db, matrix="EDNAFULL", o=16, e=4, atype=1, **opts):
     return eng
 
 
-def test_query_batch_matches_oracle(cs, oracle_mod):
+@pytest.mark.parametrize("opts", [{}, {"third_pass": 0}, {"two_pass": 0}, {"two_pass": 2}])
+def test_query_batch_matches_oracle(cs, oracle_mod, opts):
+    """Two passes with the third pass (the default at 16/4), without it, one pass, and two passes
+    forced at 3/2 gap costs (most pairs given up by the box step)."""
     db = _dna(300, 11, 1, 700)
     queries = _dna(9, 12, 30, 600) + [b"", b"A", _dna(1, 13, 1500, 1500)[0]]
-    eng = _engine(cs, db)
+    o, e = (3, 2) if opts.get("two_pass") == 2 else (16, 4)
+    eng = _engine(cs, db, o=o, e=e, **opts)
     t = eng.submit(queries)
     r = eng.wait(t)
     assert r["status"] == 0 and r["queries"] == len(queries) and r["pairs"] == len(queries) * len(db)
-    np.testing.assert_array_equal(r["out"], _expected(cs, oracle_mod, queries, db, "EDNAFULL", 16, 4))
+    np.testing.assert_array_equal(r["out"], _expected(cs, oracle_mod, queries, db, "EDNAFULL", o, e))
     assert r["submit_s"] <= r["admit_s"] <= r["done_s"]
 
 
