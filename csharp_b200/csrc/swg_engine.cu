@@ -59,6 +59,7 @@ __host__ __device__ constexpr int ctas_of(int K, int kind = 0) {
   return kind == kKindScoreShape ? (K <= 10 ? 2 : 1) : (K <= 8 ? 2 : 1);
 }
 constexpr int kMaxChunk = 1024;
+constexpr int kFbChunk = 64;  // third-pass partners per work item
 constexpr int kScrWords = 8;    // words of carried state per column in the pass scratch
 
 struct EngineJob {
@@ -86,11 +87,14 @@ struct EngineJob {
   long long rowbuf_words;   // (the kernel checks its slots against them)
   int protein;              // NW distance rule: similarity over the full length
   unsigned long long* stats; // [0] items taken, [1] pairs finished in 16-bit lanes, [2] tripped
-  // third pass (fb_cnt != nullptr): item it is query fb_lo + it with the fb_cnt[it] partners at
-  // sorted[fb_start[it] ..] (the box step's give-ups, bucketed by query)
+  // third pass (fb_cnt != nullptr): the box step's give-ups bucketed by query, query k (k < fb_nq)
+  // holding fb_cnt[k] partners at sorted[fb_start[k] ..] in chunks of kFbChunk; item it is chunk
+  // it - fb_cstart[k] of the query k with fb_cstart[k] <= it < fb_cstart[k + 1], *fb_total items
   const int* fb_cnt;
   const int* fb_start;
-  int fb_lo;
+  const int* fb_cstart;
+  const int* fb_total;
+  int fb_nq, fb_lo;
   int4* box;                // two-pass: pairs whose counters the box step finds
   uint32_t* boxwin;         // two-pass: per box record, the threshold codes of the 128 rows above ie
   int* box_count;
@@ -634,16 +638,23 @@ __global__ void __launch_bounds__(warps_of(K, KIND) * 32, ctas_of(K, KIND)) engi
   uint32_t* scr = J.scratch + ((long)blockIdx.x * kEngWarps + warp) * (long)J.maxcol * kScr;
   uint32_t* rowb = J.rowbuf ? J.rowbuf + ((long)blockIdx.x * kEngWarps + warp) * (long)J.mpad : nullptr;
   if (threadIdx.x == 0) s_q = -1;
+  const int nitems = J.fb_cnt ? *J.fb_total : J.nitems;
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(J.counter, 1);
     __syncthreads();
     const int it = s_item;
-    if (it >= J.nitems) break;
+    if (it >= nitems) break;
     int q, c0, c1, passes;
-    if (J.fb_cnt) {  // third pass: a query's pairs the box step gave up on
-      q = J.fb_lo + it;
-      c0 = J.fb_start[it];
-      c1 = c0 + J.fb_cnt[it];
+    if (J.fb_cnt) {  // third pass: a chunk of a query's pairs the box step gave up on
+      int lo = 0, hi = J.fb_nq;  // fb_cstart[lo] <= it < fb_cstart[hi]
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (J.fb_cstart[mid] <= it) lo = mid;
+        else hi = mid;
+      }
+      q = J.fb_lo + lo;
+      c0 = J.fb_start[lo] + (it - J.fb_cstart[lo]) * kFbChunk;
+      c1 = min(J.fb_start[lo] + J.fb_cnt[lo], c0 + kFbChunk);
       if (c1 == c0) {
         __syncthreads();  // every thread has read s_item
         continue;
@@ -874,26 +885,40 @@ __global__ void fb_count_kernel(const int2* fb, const int* n, long long cap, int
     atomicAdd(cnt + (fb[p].x - lo), 1);
 }
 
-// Exclusive prefix sums of cnt[0..nq) into start (one CTA of 1024 threads), fill reset to 0.
-__global__ void __launch_bounds__(1024) fb_scan_kernel(const int* cnt, int* start, int* fill, int nq) {
-  __shared__ int part[1024];
+// Exclusive prefix sums over the nq queries (one CTA of 1024 threads): start[] of the partner
+// counts and cstart[] of their kFbChunk-pair chunks (cstart[nq] = *total = all chunks); fill
+// reset to 0.
+__global__ void __launch_bounds__(1024) fb_scan_kernel(const int* cnt, int* start, int* fill, int* cstart,
+                                                       int* total, int nq) {
+  __shared__ int part[1024], cpart[1024];
   const int t = threadIdx.x;
   const int per = (nq + 1023) / 1024, lo = min(nq, t * per), hi = min(nq, lo + per);
-  int sum = 0;
-  for (int k = lo; k < hi; k++) sum += cnt[k];
+  int sum = 0, csum = 0;
+  for (int k = lo; k < hi; k++) {
+    sum += cnt[k];
+    csum += (cnt[k] + kFbChunk - 1) / kFbChunk;
+  }
   part[t] = sum;
+  cpart[t] = csum;
   __syncthreads();
-  for (int d = 1; d < 1024; d <<= 1) {  // inclusive scan of the per-thread sums
-    const int v = t >= d ? part[t - d] : 0;
+  for (int d = 1; d < 1024; d <<= 1) {  // inclusive scans of the per-thread sums
+    const int v = t >= d ? part[t - d] : 0, cv = t >= d ? cpart[t - d] : 0;
     __syncthreads();
     part[t] += v;
+    cpart[t] += cv;
     __syncthreads();
   }
-  int run = part[t] - sum;
+  int run = part[t] - sum, crun = cpart[t] - csum;
   for (int k = lo; k < hi; k++) {
     start[k] = run;
+    cstart[k] = crun;
     run += cnt[k];
+    crun += (cnt[k] + kFbChunk - 1) / kFbChunk;
     fill[k] = 0;
+  }
+  if (t == 1023) {
+    cstart[nq] = cpart[1023];
+    *total = cpart[1023];
   }
 }
 
@@ -1107,7 +1132,7 @@ struct Base {
   // third pass: the give-ups (pair list, bucketed partners) and per-query counts / offsets / fill
   int2* d_fb = nullptr;
   int* d_fbsorted = nullptr;
-  int* d_fbq = nullptr;         // [3 * nseq]: counts, offsets, fill
+  int* d_fbq = nullptr;         // [4 * nseq + 2]: counts, offsets, fill, chunk offsets (+1), chunks
   void free_box() {
     cudaFree(d_box); cudaFree(d_boxwin); cudaFree(d_cls[0]); cudaFree(d_cls[1]); cudaFree(d_spill);
     cudaFree(d_fb); cudaFree(d_fbsorted);
@@ -1636,7 +1661,7 @@ class EngineImpl : public Engine {
       if (!B.d_counts && cudaMalloc(&B.d_counts, sizeof(int) * 8) != cudaSuccess) {
         cudaGetLastError(); B.d_counts = nullptr; *msg = "cudaMalloc two-pass counts"; return SW_E_OOM;
       }
-      if (!B.d_fbq && cudaMalloc(&B.d_fbq, sizeof(int) * 3 * (size_t)std::max(N, 1)) != cudaSuccess) {
+      if (!B.d_fbq && cudaMalloc(&B.d_fbq, sizeof(int) * (4 * (size_t)std::max(N, 1) + 2)) != cudaSuccess) {
         cudaGetLastError(); B.d_fbq = nullptr; *msg = "cudaMalloc third-pass counts"; return SW_E_OOM;
       }
       // the third pass (16 rows per lane, every query's profile in shared memory) where it fits;
@@ -1772,17 +1797,20 @@ class EngineImpl : public Engine {
         int* cnt = B.d_fbq;
         int* start = cnt + P.nseq;
         int* fill = start + P.nseq;
+        int* cstart = fill + P.nseq;
+        int* total = cstart + P.nseq + 1;
         if ((e = cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)nq, P.stream)) != cudaSuccess) return e;
         const int g = std::max(1, P.sms * 4);
         fb_count_kernel<<<g, 256, 0, P.stream>>>(B.d_fb, B.d_counts + 6, B.box_cap, key.row_lo, cnt);
-        fb_scan_kernel<<<1, 1024, 0, P.stream>>>(cnt, start, fill, nq);
+        fb_scan_kernel<<<1, 1024, 0, P.stream>>>(cnt, start, fill, cstart, total, nq);
         fb_scatter_kernel<<<g, 256, 0, P.stream>>>(B.d_fb, B.d_counts + 6, B.box_cap, key.row_lo, start, fill,
                                                    B.d_fbsorted);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         EngineJob F = J3;
-        F.fb_cnt = cnt; F.fb_start = start; F.fb_lo = key.row_lo;
+        F.fb_cnt = cnt; F.fb_start = start; F.fb_cstart = cstart; F.fb_total = total;
+        F.fb_nq = nq; F.fb_lo = key.row_lo;
         F.sorted = B.d_fbsorted;
-        F.items = nullptr; F.nitems = nq;
+        F.items = nullptr; F.nitems = 0;
         F.counter = B.d_counts + 7;
         F.mpad = pl.fb_mpad;
         F.scratch = B.d_scratch;
@@ -2137,17 +2165,20 @@ class QueryRunnerImpl : public QueryRunner {
         int* cnt = W.d_fbq;
         int* start = cnt + W.fbq_cap;
         int* fill = start + W.fbq_cap;
+        int* cstart = fill + W.fbq_cap;
+        int* total = cstart + W.fbq_cap + 1;
         if ((e = cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)fb_nq, st)) != cudaSuccess) return cuda_err(e, msg);
         const int g4 = std::max(1, P_.sms * 4);
         fb_count_kernel<<<g4, 256, 0, st>>>(W.d_fb, W.d_counts + 6, (long long)W.box_cap, 0, cnt);
-        fb_scan_kernel<<<1, 1024, 0, st>>>(cnt, start, fill, fb_nq);
+        fb_scan_kernel<<<1, 1024, 0, st>>>(cnt, start, fill, cstart, total, fb_nq);
         fb_scatter_kernel<<<g4, 256, 0, st>>>(W.d_fb, W.d_counts + 6, (long long)W.box_cap, 0, start, fill,
                                               W.d_fbsorted);
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(e, msg);
         EngineJob F = J;
-        F.fb_cnt = cnt; F.fb_start = start; F.fb_lo = 0;
+        F.fb_cnt = cnt; F.fb_start = start; F.fb_cstart = cstart; F.fb_total = total;
+        F.fb_nq = fb_nq; F.fb_lo = 0;
         F.sorted = W.d_fbsorted;
-        F.items = nullptr; F.nitems = fb_nq;
+        F.items = nullptr; F.nitems = 0;
         F.counter = W.d_counts + 7;
         F.mpad = fb_mpad;
         F.scratch = W.d_scratch;
@@ -2206,7 +2237,7 @@ class QueryRunnerImpl : public QueryRunner {
     uint32_t* d_rowbuf = nullptr;
     size_t rowbuf_bytes = 0;
     // third pass: the give-ups (box_cap entries), their partners bucketed by query slot, and per
-    // slot counts / offsets / fill (fbq_cap each)
+    // slot counts / offsets / fill (fbq_cap each), chunk offsets (fbq_cap + 1) and the chunk count
     int2* d_fb = nullptr;
     int* d_fbsorted = nullptr;
     int* d_fbq = nullptr;
@@ -2219,7 +2250,7 @@ class QueryRunnerImpl : public QueryRunner {
     cudaFree(W.d_fbq);
     W.d_fbq = nullptr;
     W.fbq_cap = 0;
-    if (cudaMalloc(&W.d_fbq, sizeof(int) * 3 * cap) != cudaSuccess) {
+    if (cudaMalloc(&W.d_fbq, sizeof(int) * (4 * cap + 2)) != cudaSuccess) {
       cudaGetLastError(); *msg = "cudaMalloc wave third-pass counts"; return SW_E_OOM;
     }
     W.fbq_cap = cap;
