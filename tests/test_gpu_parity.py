@@ -313,6 +313,14 @@ def test_engine_accounts_for_every_pair(cs):
     _, pairs, _ = eng.all_pairs(1)
     assert eng.query("items") == eng.query("planned_items") > 0
     assert eng.query("lane16_pairs") + eng.rerun_count() == pairs
+    assert eng.query("kernel_error") == 0  # no work item or pair outside the plan's bounds
+    # the self-check word is per launch: a device-output job leaves it readable too
+    import torch
+    out = torch.zeros((len(seqs), len(seqs)), dtype=torch.int16, device="cuda")
+    eng.set_option("two_pass", 0)
+    eng.all_pairs_device(out.data_ptr(), len(seqs), 3)
+    eng.synchronize()
+    assert eng.query("kernel_error") == 0 and eng.query("lane16_pairs") + eng.rerun_count() == pairs
 
 
 def test_protein_engine_uses_16bit_lanes_and_matches_oracle(cs, oracle_mod):
