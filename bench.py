@@ -42,7 +42,7 @@ sys.path.insert(0, str(ROOT))
 WORKLOAD = dict(n=20000, median=400, sigma=0.6, lo=50, hi=1500, roots=200, seed=3)
 OPS_PER_CELL = 11      # algorithmic integer ops of one SW-Gotoh cell (E, F, H, running best)
 LANES_PER_OP = 2       # the engine's score registers hold two 16-bit lanes
-SHARES = 8             # steps per whole job: the shares of an 8-rank run
+SHARES = 8             # steps per whole job: 8 shares of equal DP cells (and an 8-rank run's blocks)
 SERVE = dict(db=100000, qmin=1, qmax=512, load=0.7, jobs=100, seed=6)
 PARITY_SAMPLE = 100000  # pairs of configurations 2 and 4 checked against the oracle
 ENGINE_OPTIONS = {}    # engine knobs from the command line (sw_set_option), applied to every engine
@@ -78,6 +78,16 @@ def ranges(n, parts):
 def block_computed(r, c):
     """Rank r computes block (r, c) (the SWG-MPI checkerboard)."""
     return (r > c and (r + c) % 2 == 0) or (r < c and (r + c) % 2 == 1)
+
+
+def checkerboard_share_cells(lens, share, parts=SHARES):
+    """DP cells (sum of m * n) of the pairs rank `share` of a `parts`-rank run aligns."""
+    lens = np.asarray(lens, dtype=np.float64)
+    tot = 0.0
+    for rs, re_, cs_, ce, diag in share_blocks(len(lens), share, parts):
+        r = lens[rs:re_ + 1]
+        tot += (r.sum() ** 2 - (r * r).sum()) / 2 if diag else r.sum() * lens[cs_:ce + 1].sum()
+    return tot
 
 
 def share_blocks(n, share, parts=SHARES):
@@ -473,20 +483,24 @@ def main():
     def share_of(step):
         return (step * world + rank) % SHARES
 
+    # the job's shares: contiguous rows of equal DP cells (the cost-balanced partition of the
+    # one-process-per-GPU path), each aligned as a one-rank run orients its pairs
+    from csharp_b200.driver import balanced_row_ranges
+    bal = balanced_row_ranges(lens, SHARES)
     # the autotuner times each rows-per-lane choice on a sample of this job (before any timing)
     tuned = None if (a.no_autotune or a.rows_per_lane) else eng.autotune(out.data_ptr(), N)
     share_cells = {}
     t_plan = time.perf_counter()
     eng.set_option("plan_only", 1)  # plan and capture every share before timing; launch nothing
     for s in range(SHARES):
-        eng.rank_blocks_device(s, SHARES, out.data_ptr(), N)
+        eng.rows_device(*bal[s], out.data_ptr(), N)
         share_cells[s] = eng.query("cells")
     eng.set_option("plan_only", 0)
     plan_s = time.perf_counter() - t_plan
     torch.cuda.synchronize()
 
     for w in range(a.warmup):
-        eng.rank_blocks_device(share_of(w), SHARES, out.data_ptr(), N)
+        eng.rows_device(*bal[share_of(w)], out.data_ptr(), N)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -502,7 +516,7 @@ def main():
             flush.zero_()
             s = share_of(a.warmup + k)
             ev[k][0].record(stream)
-            eng.rank_blocks_device(s, SHARES, out.data_ptr(), N)
+            eng.rows_device(*bal[s], out.data_ptr(), N)
             ev[k][1].record(stream)
             cells += share_cells[s]
             launches += eng.query("launches")
@@ -527,7 +541,9 @@ def main():
               "data": "synthetic (seeded family generator; no dataset in the reference)",
               "config": {"workload": f"cfg3 batched uneven SW-Gotoh all-pairs: {N} DNA, lognormal(median 400, sigma 0.6) "
                                      f"clipped 50-1500, 200 roots, EDNAFULL, open 16 / extend 4, PercentIdentity Int16",
-                         "step": f"one rank's share of an {SHARES}-rank MPI run of the job (whole job = {SHARES} steps)",
+                         "step": f"one of {SHARES} contiguous row shares of equal DP cells, pairs oriented as a "
+                                 f"one-rank run (whole job = {SHARES} steps)",
+                         "share_cells_max_over_mean": round(max(share_cells.values()) * SHARES / sum(share_cells.values()), 4),
                          "l2": "flushed (256 MB write) before every timed step",
                          "cells_per_job": int(sum(share_cells.values())), "pairs_per_job": N * (N - 1) // 2,
                          "plan_s": round(plan_s, 2),
@@ -552,7 +568,7 @@ def main():
                               "kernel_ms": round(kernel_ms, 2)}
     if not a.skip_extras and rank == 0:
         covered = {share_of(k) for k in range(a.warmup + a.steps)}
-        extras(a, cs, eng, stream, flush, out, concat, off, lens, N, share_cells, threads, result, covered)
+        extras(a, cs, eng, stream, flush, out, concat, off, lens, N, bal, threads, result, covered)
     if rank == 0:
         print(json.dumps(result))
     if world > 1:
@@ -576,13 +592,16 @@ def start_parity(cs, sets, picks, threads):
     return parity
 
 
-def extras(a, cs, eng, stream, flush, out, concat, off, lens, N, share_cells, threads, result, covered):
+def extras(a, cs, eng, stream, flush, out, concat, off, lens, N, bal, threads, result, covered):
     import torch
-    # ---- CPU baseline: the reference's aligner on a uniform sample of the job's pairs, oriented
-    # as the 8-rank run orients them (s1 = the row of the share that aligns the pair), alone on the
-    # host cores; its distances against the GPU matrix of the shares the timed run computed
-    ii, jj, blk = sample_pairs(N, 200000, np.random.default_rng(5))
-    keep = np.isin(blk[ii], list(covered))
+    # ---- CPU baseline: the reference's aligner on a uniform sample of the job's pairs (s1 = the
+    # larger index, as the timed shares orient them), alone on the host cores; its distances
+    # against the GPU matrix of the shares the timed run computed
+    rng = np.random.default_rng(5)
+    ii = rng.integers(1, N, 200000)
+    jj = (rng.random(200000) * ii).astype(np.int64)
+    share_of_row = np.searchsorted(np.array([lo for lo, _ in bal]), ii, side="right") - 1
+    keep = np.isin(share_of_row, list(covered))
     ii, jj = ii[keep], jj[keep]
     per_pair = float(np.mean(lens[ii] * lens[jj]))
     npairs = int(max(threads * 4, min(len(ii), a.cpu_seconds * threads * 0.12e9 / per_pair)))
@@ -631,7 +650,7 @@ def extras(a, cs, eng, stream, flush, out, concat, off, lens, N, share_cells, th
         dt = time.perf_counter() - t
         if k >= 0:
             e_s += dt
-            e_cells += share_cells[s]
+            e_cells += checkerboard_share_cells(lens, s)
             h2d += concat.nbytes + off.nbytes
             d2h += sum((re_ - rs + 1) * (ce - cs_ + 1) * 2 for rs, re_, cs_, ce, _ in share_blocks(N, s))
     result["e2e"] = {"value": round(e_cells / e_s / 1e9, 3), "unit": "GCUPS",
@@ -667,7 +686,7 @@ def extras(a, cs, eng, stream, flush, out, concat, off, lens, N, share_cells, th
         flush.zero_()
         times[name] = _timed(stream, lambda: handler_calls(dst))
     eng.set_option("block_engine", 1)
-    sc = float(share_cells[share])
+    sc = float(checkerboard_share_cells(lens, share))
     result["plain_vs_batched"] = {"share": f"rank {share} of an {SHARES}-rank run: {len(blocks)} blocks, "
                                            f"{sc:.3g} cells, one block-handler call per block",
                                   "plain_gcups": round(sc / (times["plain"] * 1e-3) / 1e9, 2),

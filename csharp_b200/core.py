@@ -213,18 +213,17 @@ class Engine:
 
     def rows_device(self, row_start, row_end, d_out_ptr, ld):
         """Rows row_start..row_end of a one-rank run -- every pair (i, j) with j < i, s1 = sequence
-        i -- into the N x N device matrix at d_out_ptr (leading dimension ld): the rows' diagonal
-        block (mirrored entries written too) and the block left of it (rows only).  SWG-MPI and NW
-        modes; returns the pairs aligned."""
+        i, written at (i, j) and (j, i) -- into the N x N device matrix at d_out_ptr (leading
+        dimension ld), one engine job (sw_compute_rows).  SWG-MPI and NW modes; returns the pairs
+        aligned."""
         if self.mode == SWG_MS:
             raise ValueError("rows_device: SWG-MS aligns both orientations; use its blocks")
         lo, hi = int(row_start), int(row_end)
         if hi < lo:
             return 0
-        n = self.compute_block_device(lo, hi, lo, hi, True, d_out_ptr + 2 * (lo * ld + lo), ld)
-        if lo > 0:
-            n += self.compute_block_device(lo, hi, 0, lo - 1, False, d_out_ptr + 2 * lo * ld, ld)
-        return n
+        p = C.c_int64()
+        self._ck(L.load().sw_compute_rows(self._h, lo, hi, C.c_void_p(d_out_ptr), ld, C.byref(p)))
+        return p.value
 
     def align(self, s1, s2) -> PairwiseAlignment:
         a = np.frombuffer(s1.encode() if isinstance(s1, str) else bytes(s1), dtype=np.uint8)

@@ -728,6 +728,21 @@ int sw_compute_rank_blocks(sw_ctx* ctx, int32_t rank, int32_t world, int16_t* d_
   return run_engine(ctx, world, st[rank], en[rank], d_out, ld, pairs, &cells);
 }
 
+int sw_compute_rows(sw_ctx* ctx, int32_t row_start, int32_t row_end, int16_t* d_out, int64_t ld,
+                    int64_t* pairs) {
+  if (!ctx) return SW_E_ARG;
+  if (ctx->cfg.mode == SW_MODE_SWG_MS)
+    return fail(ctx, SW_E_UNSUPPORTED, "SWG-MS aligns both orientations of a pair: use its rank blocks");
+  if (row_start < 0 || row_end >= ctx->nseq || row_start > row_end + 1)
+    return fail(ctx, SW_E_ARG, "rows outside the uploaded sequences");
+  if (row_start > row_end) {  // no rows: no pairs
+    if (pairs) *pairs = 0;
+    return SW_OK;
+  }
+  int64_t cells = 0;
+  return run_engine(ctx, 1, row_start, row_end, d_out, ld, pairs, &cells);
+}
+
 int sw_autotune(sw_ctx* ctx, int16_t* d_out, int64_t ld, int32_t weights[7]) {
   if (!ctx) return SW_E_ARG;
   if (!ctx->d_seq) return fail(ctx, SW_E_STATE, "no sequences uploaded");

@@ -28,7 +28,7 @@ EXPORTS = [
     "sw_all_pairs", "sw_last_rerun_count", "sw_synchronize", "sw_parse_scoring_matrix",
     "sw_builtin_scoring_matrix", "sw_parse_fasta", "sw_partition_ranges", "sw_block_is_computed",
     "sw_write_full_matrix", "sw_write_ms_block", "sw_read_ms_block_dims", "sw_read_ms_block_values",
-    "sw_measure_int_peak", "sw_set_option", "sw_compute_rank_blocks", "sw_query",
+    "sw_measure_int_peak", "sw_set_option", "sw_compute_rank_blocks", "sw_compute_rows", "sw_query",
     "sw_compute_block_static", "sw_submit_job", "sw_poll", "sw_serve_stats", "sw_serve_drain",
     "sw_autotune", "sw_align_strings",
 ]
@@ -110,6 +110,7 @@ def load():
         "sw_measure_int_peak": ([I32, C.POINTER(C.c_double), C.POINTER(C.c_double)], I32),
         "sw_set_option": ([P, C.c_char_p, I64], I32),
         "sw_compute_rank_blocks": ([P, I32, I32, P, I64, C.POINTER(I64)], I32),
+        "sw_compute_rows": ([P, I32, I32, P, I64, C.POINTER(I64)], I32),
         "sw_query": ([P, C.c_char_p, C.POINTER(I64)], I32),
         "sw_compute_block_static": ([C.POINTER(sw_config), P, P, I32, I32, I32, I32, I32, I32, P, I64,
                                      C.POINTER(I64), P], I32),

@@ -174,6 +174,16 @@ int sw_synchronize(sw_ctx* ctx);
 int sw_compute_rank_blocks(sw_ctx* ctx, int32_t rank, int32_t world_size, int16_t* d_out,
                            int64_t ld_out, int64_t* pairs);
 
+/* Rows row_start..row_end of a one-rank run: every pair (i, j) with j < i and i in the rows,
+ * s1 = sequence i, written at (i, j) and at the mirrored (j, i) of the device N x N matrix d_out
+ * (the distances of sw_all_pairs_device with ranks = 1, whatever the rows).  A process's share of a
+ * partition of the job into contiguous rows of about equal DP cells; no reference counterpart (the
+ * reference partitions by count, sw_compute_rank_blocks).  SWG-MPI and NW; SWG-MS, which aligns
+ * both orientations of a pair, is SW_E_UNSUPPORTED.  row_start = row_end + 1: no rows.  Ordered on
+ * the context's stream; does not wait. */
+int sw_compute_rows(sw_ctx* ctx, int32_t row_start, int32_t row_end, int16_t* d_out, int64_t ld_out,
+                    int64_t* pairs);
+
 /* Engine knobs: "stream" (a caller's cudaStream_t as an integer, 0 = the context's own; later
  * calls are ordered on it), "int16_threshold" (best score above which a 16-bit lane is redone in 32-bit
  * lanes; -1 restores the value derived from the lane range), "use_graph" (0/1), "chunk"

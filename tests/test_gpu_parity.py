@@ -255,15 +255,13 @@ def test_rank_blocks_partition_the_job(cs):
 
 
 @pytest.mark.parametrize("name", ["mpi_p1.npz", "protein_mpi.npz", "nw_restated.npz"])
-@pytest.mark.parametrize("block_engine", [0, 2])
-def test_balanced_row_shares_give_the_one_rank_matrix(cs, name, block_engine):
-    """The balanced scheme's shares (rows cut at equal DP cells, rows_device) for 1-4 ranks,
+def test_balanced_row_shares_give_the_one_rank_matrix(cs, name):
+    """The balanced scheme's shares (rows cut at equal DP cells, sw_compute_rows) for 1-4 ranks,
     merged as merge_row_slabs does, give the reference's one-rank matrix."""
     import torch
     from csharp_b200.driver import balanced_row_ranges, merge_row_slabs
     z = load_npz(name)
     eng = _golden_engine(cs, z, mode=int(z["mode"]) if "mode" in z else 0)
-    eng.set_option("block_engine", block_engine)
     N = len(z["offsets"]) - 1
     want = z["distances"].copy()
     np.fill_diagonal(want, 0)  # the full matrix's diagonal (NW's restatement holds self-distances)
@@ -275,6 +273,21 @@ def test_balanced_row_shares_give_the_one_rank_matrix(cs, name, block_engine):
         assert npairs == N * (N - 1) // 2
         merge_row_slabs(out, 0, 1, [(0, N - 1)], "balanced")
         np.testing.assert_array_equal(out.cpu().numpy(), want)
+    assert eng.rows_device(5, 4, out.data_ptr(), N) == 0  # no rows
+
+
+def test_rows_reject_ms_and_bad_ranges(cs):
+    from csharp_b200.lib import SwError
+    import torch
+    z = load_npz("ms_restated.npz")
+    N = len(z["offsets"]) - 1
+    out = torch.zeros((N, N), dtype=torch.int16, device="cuda")
+    ms = _golden_engine(cs, z, mode=1)
+    with pytest.raises(ValueError):
+        ms.rows_device(0, N - 1, out.data_ptr(), N)
+    mpi = _golden_engine(cs, load_npz("mpi_p1.npz"))
+    with pytest.raises(SwError):
+        mpi.rows_device(0, 10 ** 6, out.data_ptr(), N)
 
 
 def test_sequence_validation(cs):
