@@ -1881,7 +1881,7 @@ class QueryRunnerImpl : public QueryRunner {
     cudaFree(d_qtab_); cudaFree(d_qflag_); cudaFree(d_qbsc_); cudaFree(d_qbscf_);
     for (auto& w : wb_) {
       cudaFree(w.d_box); cudaFree(w.d_win); cudaFree(w.d_cls[0]); cudaFree(w.d_cls[1]); cudaFree(w.d_counts);
-      cudaFree(w.d_fb); cudaFree(w.d_fbsorted); cudaFree(w.d_fbq);
+      cudaFree(w.d_fb); cudaFree(w.d_fbsorted); cudaFree(w.d_fbq); cudaFree(w.d_spill);
       cudaFree(w.d_rowbuf);
       cudaFree(w.d_items); cudaFree(w.d_counters); cudaFree(w.d_stats); cudaFree(w.d_rerun);
       cudaFree(w.d_rerun_count); cudaFreeHost(w.h_items); cudaFreeHost(w.h_rerun); cudaFree(w.d_scratch);
@@ -2155,11 +2155,18 @@ class QueryRunnerImpl : public QueryRunner {
       X.rerun = W.d_rerun; X.rerun_count = W.d_rerun_count; X.rerun_cap = (int)rerun_cap;
       X.stats = W.d_stats;
       X.list_cap = (long long)W.box_cap;
-      X.spill_count = W.d_counts + 1;  // no warp box kernel here: spill_cap 0 sends them on
+      // pairs whose region is wider than the register step's go to the warp box kernel
+      X.spill = W.d_spill; X.spill_count = W.d_counts + 1;
+      X.spill_cap = (int)std::min<size_t>(W.spill_cap, 0x7fffffff);
       if (fb) { X.fb = W.d_fb; X.fb_count = W.d_counts + 6; X.fb_cap = (long long)W.box_cap; }
       if ((e = launch_box_scan(X, P_.sms, st)) != cudaSuccess) return cuda_err(e, msg);
       for (int c = 0; c < 4; c++)
         if ((e = launch_box_band(X, c, P_.sms, st)) != cudaSuccess) return cuda_err(e, msg);
+      BoxJob Y = X;
+      Y.list = W.d_spill; Y.count = W.d_counts + 1; Y.list_cap = (long long)W.spill_cap;
+      Y.max_score = kWarpBoxMaxCols * std::max(max_s_, 0);
+      Y.budget = 1 << 16;
+      if ((e = launch_box(Y, (int)(B_.carry_threads / 128), 128, st)) != cudaSuccess) return cuda_err(e, msg);
       if (fb) {
         // the give-ups bucketed by query slot, then the one-pass counter kernel on them
         int* cnt = W.d_fbq;
@@ -2242,6 +2249,9 @@ class QueryRunnerImpl : public QueryRunner {
     int* d_fbsorted = nullptr;
     int* d_fbq = nullptr;
     size_t fbq_cap = 0;
+    // the register step's spills for the warp box kernel
+    int4* d_spill = nullptr;
+    size_t spill_cap = 0;
   };
 
   int grow_fbq(WaveBuf& W, size_t nq, std::string* msg) {
@@ -2265,10 +2275,12 @@ class QueryRunnerImpl : public QueryRunner {
     if (pairs > W.box_cap) {
       const size_t cap = std::max(pairs, W.box_cap * 2);
       cudaFree(W.d_box); cudaFree(W.d_win); cudaFree(W.d_cls[0]); cudaFree(W.d_cls[1]);
-      cudaFree(W.d_fb); cudaFree(W.d_fbsorted);
+      cudaFree(W.d_fb); cudaFree(W.d_fbsorted); cudaFree(W.d_spill);
       W.d_box = nullptr; W.d_win = nullptr; W.d_cls[0] = W.d_cls[1] = nullptr; W.box_cap = 0;
-      W.d_fb = nullptr; W.d_fbsorted = nullptr;
-      if (cudaMalloc(&W.d_box, sizeof(int4) * cap) != cudaSuccess ||
+      W.d_fb = nullptr; W.d_fbsorted = nullptr; W.d_spill = nullptr; W.spill_cap = 0;
+      const size_t nspill = std::max<size_t>(cap / 16, 1 << 16);
+      if (cudaMalloc(&W.d_spill, sizeof(int4) * nspill) != cudaSuccess ||
+          cudaMalloc(&W.d_box, sizeof(int4) * cap) != cudaSuccess ||
           cudaMalloc(&W.d_fb, sizeof(int2) * cap) != cudaSuccess ||
           cudaMalloc(&W.d_fbsorted, sizeof(int) * cap) != cudaSuccess ||
           cudaMalloc(&W.d_win, sizeof(uint32_t) * kRegWinWords * cap) != cudaSuccess ||
@@ -2277,6 +2289,7 @@ class QueryRunnerImpl : public QueryRunner {
         cudaGetLastError(); *msg = "cudaMalloc wave box lists"; return SW_E_OOM;
       }
       W.box_cap = cap;
+      W.spill_cap = nspill;
     }
     if (rowbuf > W.rowbuf_bytes) {
       cudaFree(W.d_rowbuf);

@@ -260,6 +260,8 @@ __device__ __forceinline__ int scan_max_up(int y, int lane) {
 }
 
 constexpr int kBoxMaxA1 = 33;  // letters + padding of the dense codes
+// Rows of the box tables: one per residue byte of s1 in query mode, else one per code.
+constexpr int kBoxTabRows = 128;
 
 // A pair the box step cannot finish: the full DP with counters, on the 16-bit lanes of the
 // one-pass kernel (J.fb) where the engine runs that third pass, else on the 32-bit lanes.
@@ -279,14 +281,13 @@ __device__ __forceinline__ void box_give_up(const BoxJob& J, int q, int d) {
 }
 
 __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
-  __shared__ int sc[kBoxMaxA1 * kBoxMaxA1];        // S(a, b) of the dense codes
-  __shared__ uint32_t fl[kBoxMaxA1 * kBoxMaxA1];
+  // S(a, b) << 8 | counted flag; rows: s1's dense codes, or its residue bytes in query mode
+  __shared__ int scf[kBoxTabRows * kBoxMaxA1];
   __shared__ int4 rowbuf[kBoxWarps * kBoxMaxW];
   const int A1 = J.A + 1;
-  for (int k = threadIdx.x; k < A1 * A1; k += blockDim.x) {
-    sc[k] = J.lettab[k] - J.o;
-    fl[k] = J.flagtab[k];
-  }
+  for (int k = threadIdx.x; k < (J.qseq ? kBoxTabRows : A1) * A1; k += blockDim.x)
+    scf[k] = J.qseq ? J.qscf[k]
+                    : (int)(((uint32_t)(J.lettab[k] - J.o) << 8) | (J.flagtab[k] & kFlagCount));
   __syncthreads();
   constexpr int NEG = kNegInf;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -299,7 +300,7 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
     const int4 rec = J.list[p];
     const int q = rec.x, d = rec.y, S = rec.z & 0xFFFF;
     const int ie = (int)((uint32_t)rec.w >> 16), je = rec.w & 0xFFFF;
-    const uint8_t* a = J.seq + J.off[q];
+    const uint8_t* a = J.qseq ? J.qseq + J.qoff[q] : J.seq + J.off[q];
     const uint8_t* b = J.seq + J.off[d];
     // ---- reverse scan: positions (i, j) = residues consumed ----
     int hi = je, lo = je;
@@ -316,7 +317,7 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
       if (lane == 0) rwn0 = NEG;
       int pair0 = NEG;
       if (rwn0 > NEG && j0 >= 0 && j0 < je) {
-        pair0 = (int)sc[arow + b[j0]] + rwn0;
+        pair0 = (scf[arow + b[j0]] >> 8) + rwn0;
         if (pair0 == S) { cand_i = min(cand_i, i + 1); cand_j = min(cand_j, j0 + 1); }
       }
       const int x0 = max(pair0, rgb0 > NEG ? rgb0 - o : NEG);
@@ -340,7 +341,7 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
         if (lane == 0) rwn1 = last0;
         int pair1 = NEG;
         if (rwn1 > NEG && j1 >= 0 && j1 < je) {
-          pair1 = (int)sc[arow + b[j1]] + rwn1;
+          pair1 = (scf[arow + b[j1]] >> 8) + rwn1;
           if (pair1 == S) { cand_i = min(cand_i, i + 1); cand_j = min(cand_j, j1 + 1); }
         }
         const int x1 = max(pair1, rgb1 > NEG ? rgb1 - o : NEG);
@@ -416,7 +417,8 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
             const int col = (int)b[jlo - 1 + c];
             int v, g;
             uint32_t cv, cg;
-            gotoh_cell<true, SwCnt>(sc[arow + col], fl[arow + col], vd, cd, vu, gu, cvu, cgu,
+            const int sf = scf[arow + col];
+            gotoh_cell<true, SwCnt>(sf >> 8, (uint32_t)sf & 0xFFu, vd, cd, vu, gu, cvu, cgu,
                                     vl, cl, hh, ch, o, e, 0, 0, v, g, cv, cg);
             vl = v;
             cl = cv;
@@ -439,8 +441,12 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
         box_give_up(J, q, d);
       } else {
         const int16_t dist = fraction_distance((int)(ccap & 0xFFFFu), (int)(ccap >> 16));
-        J.out[(long long)q * J.ld + d] = dist;
-        if (J.mirror) J.out[(long long)d * J.ld + q] = dist;
+        if (J.qout) {
+          J.qout[q][d] = dist;
+        } else {
+          J.out[(long long)q * J.ld + d] = dist;
+          if (J.mirror) J.out[(long long)d * J.ld + q] = dist;
+        }
       }
     }
     __syncwarp();
@@ -449,9 +455,6 @@ __global__ void __launch_bounds__(kBoxWarps * 32) box_kernel(BoxJob J) {
 
 // ---- box step, one pair per thread with the DP rows in registers (swg_box_reg.cuh) -------------
 constexpr int kRegThreads = 128;
-
-// Rows of the box tables: one per residue byte of s1 in query mode, else one per code.
-constexpr int kBoxTabRows = 128;
 
 __global__ void __launch_bounds__(kRegThreads) box_scan_kernel(BoxJob J) {
   __shared__ int sc[kBoxTabRows * kBoxMaxA1];
