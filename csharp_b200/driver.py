@@ -163,9 +163,12 @@ def merge_row_slabs(out, rank, world, row_ranges, scheme, group=None, dst=None):
     rows = [max(0, hi - lo + 1) for lo, hi in row_ranges]
     maxrows = max(max(rows), 1)
     lo, hi = row_ranges[rank]
-    buf = torch.zeros((maxrows, N), dtype=torch.int16, device=out.device)
+    dev = out.device
+    if world > 1 and out.is_cuda and dist.get_backend(group) == "gloo":
+        dev = torch.device("cpu")  # gloo's collectives take host tensors
+    buf = torch.zeros((maxrows, N), dtype=torch.int16, device=dev)
     if rows[rank]:
-        buf[:rows[rank]] = out[lo:hi + 1]
+        buf[:rows[rank]] = out[lo:hi + 1].to(dev)
     if world > 1:
         if dst is None:
             parts = [torch.empty_like(buf) for _ in range(world)]
@@ -178,7 +181,7 @@ def merge_row_slabs(out, rank, world, row_ranges, scheme, group=None, dst=None):
                 return False
     else:
         parts = [buf]
-    full = torch.zeros((N, N), dtype=torch.int16, device=out.device)
+    full = torch.zeros((N, N), dtype=torch.int16, device=dev)
     for r, (a, b) in enumerate(row_ranges):
         if rows[r]:
             full[a:b + 1] = parts[r][:rows[r]]
