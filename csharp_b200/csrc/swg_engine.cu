@@ -448,9 +448,14 @@ __device__ __forceinline__ void align_two_nw(const uint32_t* __restrict__ prof, 
   // the cell (m, n) of each pair: its pass, lane, row in the lane, and the step that reaches it
   const int pm = (m - 1) / (32 * K), tm = ((m - 1) % (32 * K)) / K, rm = (m - 1) % K;
   const int sA = nA - 1 + tm, sB = nB - 1 + tm;
+  // the step at which this lane is at column n of pair A / B (-1: never counts as trailing)
+  const int gsA = trim ? nA - 1 + lane : -1, gsB = trim ? nB - 1 + lane : -1;
   capA = capB = 0u;
   for (int p = 0; p < passes; p++) {
     const int pbase = p * 32 * K;
+    // the steps at which this lane holds (m, n) of pair A / B in this pass (-1: none)
+    const bool holder = p == pm && lane == tm;
+    const int cA = holder ? sA : -1, cB = holder ? sB : -1;
     uint32_t VOL[K], H[K], clA[K], clB[K], chA[K], chB[K], hinc[K];
 #pragma unroll
     for (int r = 0; r < K; r++) {
@@ -498,8 +503,8 @@ __device__ __forceinline__ void align_two_nw(const uint32_t* __restrict__ prof, 
         dVO = VOU; dcA = cvuA; dcB = cvuB;
         const int jc = s - lane;  // this step's column (0-based)
         // UP steps within column n: the trailing run
-        const uint32_t gincA = (trim && jc == nA - 1) ? 0u : 0x10000u;
-        const uint32_t gincB = (trim && jc == nB - 1) ? 0u : 0x10000u;
+        const uint32_t gincA = s == gsA ? 0u : 0x10000u;
+        const uint32_t gincB = s == gsB ? 0u : 0x10000u;
         const int col = 32 + jc;
         const int xa = ca[col], xb = cb[col];
         const uint32_t* pla = pl + xa * plane;
@@ -554,12 +559,12 @@ __device__ __forceinline__ void align_two_nw(const uint32_t* __restrict__ prof, 
         }
         uVO = VOU; uG = GU; ucvA = cvuA; ucvB = cvuB; ucgA = cguA; ucgB = cguB;
         // the (m, n) cells: lane tm of pass pm holds them after steps sA / sB
-        if (p == pm && lane == tm && (s == sA || s == sB)) {
+        if (s == cA || s == cB) {
 #pragma unroll
           for (int r = 0; r < K; r++)
             if (r == rm) {
-              if (s == sA) capA = clA[r];
-              if (s == sB) capB = clB[r];
+              if (s == cA) capA = clA[r];
+              if (s == cB) capB = clB[r];
             }
         }
         if (lane == 31 && p + 1 < passes) {
