@@ -821,7 +821,7 @@ int sw_set_option(sw_ctx* ctx, const char* key, int64_t value) {
   else if (k == "box_reg") o.box_reg = value ? 1 : 0;
   else if (k == "third_pass") o.third_pass = value ? 1 : 0;
   else if (k == "chunk") {
-    if (value < 32 || value > 1024) return fail(ctx, SW_E_ARG, "chunk must be in [32, 1024]");
+    if (value != 0 && (value < 32 || value > 1024)) return fail(ctx, SW_E_ARG, "chunk must be 0 or in [32, 1024]");
     o.chunk = (int)value;
   } else if (k == "rows_per_lane") {
     if (value != 0 && (value < 4 || value > 16 || (value & 1))) return fail(ctx, SW_E_ARG, "rows_per_lane must be 0 or an even number from 4 to 16");

@@ -1528,7 +1528,9 @@ class EngineImpl : public Engine {
     }
     const int A = B.alpha;
     pl.thresh = (opt_.int16_threshold >= 0) ? (int)opt_.int16_threshold : 32767 - B.bias - B.max_s;
-    const int chunk = std::min(std::max(opt_.chunk, 32), kMaxChunk);
+    // large jobs: fewer, longer items (1 % faster on the 20,000-sequence job); small ones keep
+    // enough items to fill the GPU (the 1,000-sequence job is 5 % slower with 1,024)
+    const int chunk = opt_.chunk ? std::min(std::max(opt_.chunk, 32), kMaxChunk) : (N >= 8192 ? 1024 : 512);
     const int nchunks = (N + chunk - 1) / chunk;
     std::vector<std::vector<int>> cidx(nchunks);
     std::vector<std::vector<double>> csum(nchunks);

@@ -37,7 +37,7 @@ struct EngineParams {
 struct EngineOptions {
   long long int16_threshold = -1;  // < 0: derived from the lane range; else forced trip level
   int use_graph = 1;
-  int chunk = 1024;                // database entries per work item (1024 measured 1 % faster than 512 on cfg3)
+  int chunk = 0;                   // database entries per work item (0: 1024 for 8,192 sequences or more, else 512)
   int k_override = 0;              // 0: per-query choice; else rows per lane
   int plan_only = 0;               // build plans and graphs, launch nothing
   int two_pass = 1;                // SW: score-only pass, then counters from boxes (box step):

@@ -187,7 +187,8 @@ int sw_compute_rows(sw_ctx* ctx, int32_t row_start, int32_t row_end, int16_t* d_
 /* Engine knobs: "stream" (a caller's cudaStream_t as an integer, 0 = the context's own; later
  * calls are ordered on it), "int16_threshold" (best score above which a 16-bit lane is redone in 32-bit
  * lanes; -1 restores the value derived from the lane range), "use_graph" (0/1), "chunk"
- * (database entries per work item, 32..1024, default 1024), "rows_per_lane" (0 = chosen per query, else an even number 4..16),
+ * (database entries per work item, 32..1024; 0, the default: 1024 for 8,192 sequences or more, else
+ * 512), "rows_per_lane" (0 = chosen per query, else an even number 4..16),
  * "plan_only" (1: engine calls build their work plans and graphs but launch nothing; 0: run),
  * "two_pass" (SW-Gotoh: a score-only pass, then each pair's counters from the neighbourhood of
  * its best cell; 1, the default: where open >= 3 x the largest substitution score and extend >= 3,
