@@ -52,15 +52,20 @@ namespace swg {
 // of 8 warps), 12-16 rows fit 168 (1 CTA of 12 warps).
 constexpr int kMaxWarps = 12;
 constexpr int kKindScoreShape = 2;  // the kind value of the score-only kernels (see kKindScore)
+constexpr int kKindKimShape = 3;    // the kind value of the Kimura2 / JukesCantor kernels (kKindKim)
+// The Kimura2 / JukesCantor kernels keep 15 registers per row (two counter words per state and
+// lane): at most 8 rows per lane, one CTA of 8 warps per SM (two at 4 rows).
 __host__ __device__ constexpr int warps_of(int K, int kind = 0) {
-  return kind == kKindScoreShape ? (K <= 10 ? 8 : 12) : (K <= 8 ? 8 : K <= 12 ? 12 : 8);
+  return kind == kKindScoreShape ? (K <= 10 ? 8 : 12) : kind == kKindKimShape ? 8 : (K <= 8 ? 8 : K <= 12 ? 12 : 8);
 }
 __host__ __device__ constexpr int ctas_of(int K, int kind = 0) {
-  return kind == kKindScoreShape ? (K <= 10 ? 2 : 1) : (K <= 8 ? 2 : 1);
+  return kind == kKindScoreShape ? (K <= 10 ? 2 : 1) : kind == kKindKimShape ? (K <= 4 ? 2 : 1) : (K <= 8 ? 2 : 1);
 }
+constexpr int kKimMaxK = 8;  // rows per lane of the Kimura2 / JukesCantor kernels
 constexpr int kMaxChunk = 1024;
 constexpr int kFbChunk = 64;  // third-pass partners per work item
 constexpr int kScrWords = 8;    // words of carried state per column in the pass scratch
+constexpr int kScrWordsKim = 12;  // Kimura2 / JukesCantor: V, G and two counter words per state and lane
 
 struct EngineJob {
   const uint8_t* code;      // dense residue codes (pad code = A), same offsets as the residues
@@ -86,6 +91,8 @@ struct EngineJob {
   long long scratch_words;  // pass scratch from `scratch` on, and rows' bounds from `rowbuf` on
   long long rowbuf_words;   // (the kernel checks its slots against them)
   int protein;              // NW distance rule: similarity over the full length
+  int dist_fn;              // Kimura2 / JukesCantor kernels: SW_DIST_KIMURA2 or SW_DIST_JUKES_CANTOR
+  int* throws;              // set by a SWG-MPI JukesCantor pair whose log argument is <= 0
   unsigned long long* stats; // [0] items taken, [1] pairs finished in 16-bit lanes, [2] tripped
   // third pass (fb_cnt != nullptr): the box step's give-ups bucketed by query, query k (k < fb_nq)
   // holding fb_cnt[k] partners at sorted[fb_start[k] ..] in chunks of kFbChunk; item it is chunk
@@ -306,6 +313,165 @@ __device__ __forceinline__ void align_two(const uint32_t* __restrict__ prof, int
       const int sB = (int)(int16_t)(BEST[r] >> 16) - J.bias;
       if (sA > bestA) { bestA = sA; rowA = row; cntA = bcA[r]; }
       if (sB > bestB) { bestB = sB; rowB = row; cntB = bcB[r]; }
+    }
+  }
+}
+
+// Kimura2 / JukesCantor counterpart of align_two (nucleic jobs whose letters fit three profile
+// planes): each state and lane carries the two KimCnt words of Alignment.cs:254-348 -- aligned
+// columns << 16 | A-flagged columns, non-gap columns << 16 | B-flagged columns -- and the flag
+// plane holds the residue pair's A | B << 16 (transition / transversion, or identical / none).
+// Gap steps add an aligned column; a diagonal step adds an aligned and a non-gap column and the
+// pair's flags; STOP clears both words.  The best cell is tracked as in align_two.
+template <int K>
+__device__ __forceinline__ void align_two_kim(const uint32_t* __restrict__ prof, int mpad, int passes,
+                                              const uint8_t* __restrict__ ca,
+                                              const uint8_t* __restrict__ cb, int ncols,
+                                              const EngineJob& J, uint32_t* __restrict__ scr,
+                                              int lane, int& bestA, int& rowA, uint2& cntA,
+                                              int& bestB, int& rowB, uint2& cntB) {
+  const uint32_t bias2 = (uint32_t)J.bias * 0x10001u;
+  const uint32_t O2 = (uint32_t)J.o * 0x10001u, E2 = (uint32_t)J.e * 0x10001u;
+  const uint32_t sent2 = (uint32_t)(J.bias - J.o - J.e) * 0x10001u;  // -infinity + bias
+  const uint32_t best0 = (uint32_t)(J.bias - 1) * 0x10001u;          // below any V
+  const uint32_t vo_top = (uint32_t)(J.bias - J.o) * 0x10001u;        // V(0,j) - o + bias
+  const int plane = 3 * mpad;
+  bestA = bestB = -1;
+  rowA = rowB = 0;
+  cntA = cntB = make_uint2(0u, 0u);
+  for (int p = 0; p < passes; p++) {
+    uint32_t VOL[K], H[K], BEST[K];
+    uint32_t clA0[K], clA1[K], clB0[K], clB1[K], chA0[K], chA1[K], chB0[K], chB1[K];
+    uint32_t bcA0[K], bcA1[K], bcB0[K], bcB1[K];
+#pragma unroll
+    for (int r = 0; r < K; r++) {
+      VOL[r] = vo_top; H[r] = sent2; BEST[r] = best0;
+      clA0[r] = clA1[r] = clB0[r] = clB1[r] = 0u;
+      chA0[r] = chA1[r] = chB0[r] = chB1[r] = 0u;
+      bcA0[r] = bcA1[r] = bcB0[r] = bcB1[r] = 0u;
+    }
+    uint32_t uVO = vo_top, uG = sent2;
+    uint32_t ucvA0 = 0, ucvA1 = 0, ucvB0 = 0, ucvB1 = 0, ucgA0 = 0, ucgA1 = 0, ucgB0 = 0, ucgB1 = 0;
+    uint32_t dVO = vo_top, dcA0 = 0, dcA1 = 0, dcB0 = 0, dcB1 = 0;
+    const int pbase = p * 32 * K;
+    const uint32_t* pl = prof + pbase + lane * 4;
+    const int nsteps = ncols + 31;
+    for (int s = 0; s < nsteps; s++) {
+      const uint32_t bVO = __shfl_up_sync(0xffffffffu, uVO, 1);
+      const uint32_t bG = __shfl_up_sync(0xffffffffu, uG, 1);
+      const uint32_t bcvA0 = __shfl_up_sync(0xffffffffu, ucvA0, 1);
+      const uint32_t bcvA1 = __shfl_up_sync(0xffffffffu, ucvA1, 1);
+      const uint32_t bcvB0 = __shfl_up_sync(0xffffffffu, ucvB0, 1);
+      const uint32_t bcvB1 = __shfl_up_sync(0xffffffffu, ucvB1, 1);
+      const uint32_t bcgA0 = __shfl_up_sync(0xffffffffu, ucgA0, 1);
+      const uint32_t bcgA1 = __shfl_up_sync(0xffffffffu, ucgA1, 1);
+      const uint32_t bcgB0 = __shfl_up_sync(0xffffffffu, ucgB0, 1);
+      const uint32_t bcgB1 = __shfl_up_sync(0xffffffffu, ucgB1, 1);
+      uint32_t VOU, GU, cvuA0, cvuA1, cvuB0, cvuB1, cguA0, cguA1, cguB0, cguB1;
+      if (lane == 0) {
+        if (p == 0 || s >= ncols) {
+          VOU = vo_top; GU = sent2;
+          cvuA0 = cvuA1 = cvuB0 = cvuB1 = cguA0 = cguA1 = cguB0 = cguB1 = 0u;
+        } else {
+          const uint4 x = *reinterpret_cast<const uint4*>(scr + (long)s * kScrWordsKim);
+          const uint4 y = *reinterpret_cast<const uint4*>(scr + (long)s * kScrWordsKim + 4);
+          const uint2 z = *reinterpret_cast<const uint2*>(scr + (long)s * kScrWordsKim + 8);
+          VOU = x.x; GU = x.y; cvuA0 = x.z; cvuA1 = x.w;
+          cvuB0 = y.x; cvuB1 = y.y; cguA0 = y.z; cguA1 = y.w;
+          cguB0 = z.x; cguB1 = z.y;
+        }
+      } else {
+        VOU = bVO; GU = bG; cvuA0 = bcvA0; cvuA1 = bcvA1; cvuB0 = bcvB0; cvuB1 = bcvB1;
+        cguA0 = bcgA0; cguA1 = bcgA1; cguB0 = bcgB0; cguB1 = bcgB1;
+      }
+      uint32_t VOD = dVO, cdA0 = dcA0, cdA1 = dcA1, cdB0 = dcB0, cdB1 = dcB1;
+      dVO = VOU; dcA0 = cvuA0; dcA1 = cvuA1; dcB0 = cvuB0; dcB1 = cvuB1;
+      const int col = 32 + s - lane;
+      const int xa = ca[col], xb = cb[col];
+      const uint32_t* pla = pl + xa * plane;
+      const uint32_t* phb = pl + xb * plane + mpad;
+      const uint32_t* pma = pl + xa * plane + 2 * mpad;
+      const uint32_t* pmb = pl + xb * plane + 2 * mpad;
+      auto cell = [&](const int r, const uint32_t pl_r, const uint32_t ph_r, const uint32_t ma_r,
+                      const uint32_t mb_r) {
+        const uint32_t F = VOD + pl_r + ph_r;
+        const uint32_t cfA0 = cdA0 + (ma_r & 0xFFFFu) + 0x10000u, cfA1 = cdA1 + (ma_r >> 16) + 0x10000u;
+        const uint32_t cfB0 = cdB0 + (mb_r & 0xFFFFu) + 0x10000u, cfB1 = cdB1 + (mb_r >> 16) + 0x10000u;
+        bool hiB, loA;
+        // vertical gap: reopen from V above unless extending is strictly better
+        const uint32_t G = vmax2(VOU, GU - E2, hiB, loA);
+        const uint32_t cgA0 = (loA ? cvuA0 : cguA0) + 0x10000u, cgA1 = loA ? cvuA1 : cguA1;
+        const uint32_t cgB0 = (hiB ? cvuB0 : cguB0) + 0x10000u, cgB1 = hiB ? cvuB1 : cguB1;
+        // horizontal gap
+        H[r] = vmax2(VOL[r], H[r] - E2, hiB, loA);
+        chA0[r] = (loA ? clA0[r] : chA0[r]) + 0x10000u;
+        chA1[r] = loA ? clA1[r] : chA1[r];
+        chB0[r] = (hiB ? clB0[r] : chB0[r]) + 0x10000u;
+        chB1[r] = hiB ? clB1[r] : chB1[r];
+        // V = max(F, G, H, 0) with STOP > DIAGONAL > UP > LEFT on ties
+        const uint32_t GHv = vmax2(G, H[r], hiB, loA);
+        const uint32_t cghA0 = loA ? cgA0 : chA0[r], cghA1 = loA ? cgA1 : chA1[r];
+        const uint32_t cghB0 = hiB ? cgB0 : chB0[r], cghB1 = hiB ? cgB1 : chB1[r];
+        const uint32_t FGH = vmax2(F, GHv, hiB, loA);
+        const uint32_t cfgA0 = loA ? cfA0 : cghA0, cfgA1 = loA ? cfA1 : cghA1;
+        const uint32_t cfgB0 = hiB ? cfB0 : cghB0, cfgB1 = hiB ? cfB1 : cghB1;
+        const uint32_t V = vmax2(bias2, FGH, hiB, loA);
+        const uint32_t cvA0 = loA ? 0u : cfgA0, cvA1 = loA ? 0u : cfgA1;
+        const uint32_t cvB0 = hiB ? 0u : cfgB0, cvB1 = hiB ? 0u : cfgB1;
+        // first strictly greater V of this row (columns ascend within a lane)
+        BEST[r] = vmax2(BEST[r], V, hiB, loA);
+        bcA0[r] = loA ? bcA0[r] : cvA0;
+        bcA1[r] = loA ? bcA1[r] : cvA1;
+        bcB0[r] = hiB ? bcB0[r] : cvB0;
+        bcB1[r] = hiB ? bcB1[r] : cvB1;
+        const uint32_t VO = V - O2;
+        VOD = VOL[r]; cdA0 = clA0[r]; cdA1 = clA1[r]; cdB0 = clB0[r]; cdB1 = clB1[r];
+        VOL[r] = VO; clA0[r] = cvA0; clA1[r] = cvA1; clB0[r] = cvB0; clB1[r] = cvB1;
+        VOU = VO; GU = G;
+        cvuA0 = cvA0; cvuA1 = cvA1; cvuB0 = cvB0; cvuB1 = cvB1;
+        cguA0 = cgA0; cguA1 = cgA1; cguB0 = cgB0; cguB1 = cgB1;
+      };
+#pragma unroll
+      for (int g = 0; g < K / 4; g++) {
+        const uint4 PL = *reinterpret_cast<const uint4*>(pla + g * 128);
+        const uint4 PH = *reinterpret_cast<const uint4*>(phb + g * 128);
+        const uint4 MA = *reinterpret_cast<const uint4*>(pma + g * 128);
+        const uint4 MB = *reinterpret_cast<const uint4*>(pmb + g * 128);
+        cell(g * 4 + 0, PL.x, PH.x, MA.x, MB.x);
+        cell(g * 4 + 1, PL.y, PH.y, MA.y, MB.y);
+        cell(g * 4 + 2, PL.z, PH.z, MA.z, MB.z);
+        cell(g * 4 + 3, PL.w, PH.w, MA.w, MB.w);
+      }
+      if (K % 4 == 2) {
+        const int t2 = (K / 4) * 128 - lane * 2;
+        const uint2 PL = *reinterpret_cast<const uint2*>(pla + t2);
+        const uint2 PH = *reinterpret_cast<const uint2*>(phb + t2);
+        const uint2 MA = *reinterpret_cast<const uint2*>(pma + t2);
+        const uint2 MB = *reinterpret_cast<const uint2*>(pmb + t2);
+        cell(K - 2, PL.x, PH.x, MA.x, MB.x);
+        cell(K - 1, PL.y, PH.y, MA.y, MB.y);
+      }
+      uVO = VOU; uG = GU;
+      ucvA0 = cvuA0; ucvA1 = cvuA1; ucvB0 = cvuB0; ucvB1 = cvuB1;
+      ucgA0 = cguA0; ucgA1 = cguA1; ucgB0 = cguB0; ucgB1 = cguB1;
+      if (lane == 31 && p + 1 < passes) {
+        const int j = s - 31;
+        if (j >= 0 && j < ncols) {
+          *reinterpret_cast<uint4*>(scr + (long)j * kScrWordsKim) = make_uint4(uVO, uG, ucvA0, ucvA1);
+          *reinterpret_cast<uint4*>(scr + (long)j * kScrWordsKim + 4) = make_uint4(ucvB0, ucvB1, ucgA0, ucgA1);
+          *reinterpret_cast<uint2*>(scr + (long)j * kScrWordsKim + 8) = make_uint2(ucgB0, ucgB1);
+        }
+      }
+    }
+    __syncwarp();
+    // rows ascend within a lane and across passes: keep the first strictly greater
+#pragma unroll
+    for (int r = 0; r < K; r++) {
+      const int row = pbase + lane * K + r;
+      const int sA = (int)(int16_t)(BEST[r] & 0xFFFFu) - J.bias;
+      const int sB = (int)(int16_t)(BEST[r] >> 16) - J.bias;
+      if (sA > bestA) { bestA = sA; rowA = row; cntA = make_uint2(bcA0[r], bcA1[r]); }
+      if (sB > bestB) { bestB = sB; rowB = row; cntB = make_uint2(bcB0[r], bcB1[r]); }
     }
   }
 }
@@ -606,6 +772,18 @@ __device__ __forceinline__ void warp_best(int& best, int& row, uint32_t& cnt) {
   }
 }
 
+// warp_best with the two KimCnt words.
+__device__ __forceinline__ void warp_best2(int& best, int& row, uint2& cnt) {
+#pragma unroll
+  for (int d = 16; d >= 1; d >>= 1) {
+    const int ob = __shfl_down_sync(0xffffffffu, best, d);
+    const int orow = __shfl_down_sync(0xffffffffu, row, d);
+    const uint32_t ox = __shfl_down_sync(0xffffffffu, cnt.x, d);
+    const uint32_t oy = __shfl_down_sync(0xffffffffu, cnt.y, d);
+    if (ob > best || (ob == best && orow < row)) { best = ob; row = orow; cnt = make_uint2(ox, oy); }
+  }
+}
+
 __device__ __forceinline__ void emit(const EngineJob& J, int q, int d, int16_t dist) {
   if (J.qmode) {
     J.qout[q][d] = dist;
@@ -621,14 +799,14 @@ __device__ __forceinline__ void record_error(const EngineJob& J, int site, int i
 }
 
 // What a kernel instantiation computes per pair.
-enum { kKindSw = 0, kKindNw = 1, kKindScore = 2 };
+enum { kKindSw = 0, kKindNw = 1, kKindScore = 2, kKindKim = 3 };
 
 template <int K, int NP, int KIND>
 __global__ void __launch_bounds__(warps_of(K, KIND) * 32, ctas_of(K, KIND)) engine_kernel(EngineJob J) {
-  static_assert(kKindScore == kKindScoreShape, "score kind");
+  static_assert(kKindScore == kKindScoreShape && kKindKim == kKindKimShape, "kernel kinds");
   constexpr bool NW = KIND == kKindNw;
   constexpr int kEngWarps = warps_of(K, KIND);
-  constexpr int kScr = kScrWords;
+  constexpr int kScr = KIND == kKindKim ? kScrWordsKim : kScrWords;
   extern __shared__ __align__(16) uint8_t smem[];
   uint32_t* prof = reinterpret_cast<uint32_t*>(smem);
   const int A1 = J.A + 1;
@@ -829,6 +1007,42 @@ __global__ void __launch_bounds__(warps_of(K, KIND) * 32, ctas_of(K, KIND)) engi
         __syncwarp();
         continue;
       }
+      if constexpr (KIND == kKindKim) {
+        int bA, rA, bB, rB;
+        uint2 cA, cB;
+        if (m > 0 && ncols > 0) {
+          align_two_kim<K>(prof, J.mpad, passes, ca, cb, ncols, J, scr, lane, bA, rA, cA, bB, rB, cB);
+        } else {
+          bA = bB = 0; rA = rB = 0; cA = cB = make_uint2(0u, 0u);
+        }
+        warp_best2(bA, rA, cA);
+        warp_best2(bB, rB, cB);
+        if (lane == 0) {
+          const bool tA = bA > J.thresh && m > 0 && nA > 0, tB = dB >= 0 && bB > J.thresh && m > 0 && nB > 0;
+          atomicAdd(J.stats + 1, (unsigned long long)(1 + (dB >= 0)) - (unsigned long long)(tA + tB));
+          if (tA + tB) atomicAdd(J.stats + 2, (unsigned long long)(tA + tB));
+          // Int16 distance from the counters (SWG-MS caps Kimura2 and maps Log(Zero) to 10)
+          const bool ms = J.mode == kModeSwgMs;
+          if (tA) {
+            const int w = atomicAdd(J.rerun_count, 1);
+            if (w < J.rerun_cap) J.rerun[w] = make_int2(q, dA);
+          } else {
+            const uint2 c = (m > 0 && nA > 0) ? cA : make_uint2(0u, 0u);
+            emit(J, q, dA, kim_distance(KimCnt::T{c.x, c.y}, J.dist_fn, ms, J.throws));
+          }
+          if (dB >= 0) {
+            if (tB) {
+              const int w = atomicAdd(J.rerun_count, 1);
+              if (w < J.rerun_cap) J.rerun[w] = make_int2(q, dB);
+            } else {
+              const uint2 c = (m > 0 && nB > 0) ? cB : make_uint2(0u, 0u);
+              emit(J, q, dB, kim_distance(KimCnt::T{c.x, c.y}, J.dist_fn, ms, J.throws));
+            }
+          }
+        }
+        __syncwarp();
+        continue;
+      }
       if constexpr (NW) {
         uint32_t wa = 0, wb = 0;
         if (m > 0 && ncols > 0)
@@ -996,6 +1210,10 @@ auto with_kp(int K, int A, int kind, Fn fn) {
     const bool p3 = planes_of(A) == 3;
     if (kind == kKindNw) return p3 ? fn(engine_kernel<kk, 3, kKindNw>, threads) : fn(engine_kernel<kk, 2, kKindNw>, threads);
     if (kind == kKindScore) return p3 ? fn(engine_kernel<kk, 3, kKindScore>, threads) : fn(engine_kernel<kk, 2, kKindScore>, threads);
+    if (kind == kKindKim) {  // three planes and at most kKimMaxK rows per lane (the planner's rule)
+      constexpr int kq = kk > kKimMaxK ? kKimMaxK : kk;
+      return fn(engine_kernel<kq, 3, kKindKim>, warps_of(kq, kKindKim) * 32);
+    }
     return p3 ? fn(engine_kernel<kk, 3, kKindSw>, threads) : fn(engine_kernel<kk, 2, kKindSw>, threads);
   });
 }
@@ -1061,11 +1279,17 @@ long k_weight(int k) {
 }
 
 // Rows per lane and passes for a query of m rows: fewest padded rows, then fewest passes.
-void choose_k(int m, int kov, int* K, int* passes, bool nw = false, const int* tuned = nullptr) {
-  (void)nw;  // NW takes the same tile shapes
-  if (kov) { *K = kov; *passes = std::max(1, (m + 32 * kov - 1) / (32 * kov)); return; }
+// kmax: the largest rows per lane the kernel kind has (Kimura2 / JukesCantor: kKimMaxK).
+void choose_k(int m, int kov, int* K, int* passes, bool nw = false, const int* tuned = nullptr, int kmax = 16) {
+  if (kov) {
+    kov = std::min(kov, kmax);
+    *K = kov;
+    *passes = std::max(1, (m + 32 * kov - 1) / (32 * kov));
+    return;
+  }
   long best = -1;
   for (int k : kKs) {
+    if (k > kmax) continue;
     const int p = std::max(1, (m + 32 * k - 1) / (32 * k));
     // rows computed (padding included) times the per-row cost of that K (few rows per lane do
     // not amortise the per-step shuffles, loads and column bookkeeping); ties go to fewer passes
@@ -1117,6 +1341,7 @@ struct Base {
   int32_t* d_sorted = nullptr;
   int32_t* d_lettab = nullptr;
   uint32_t* d_flagtab = nullptr;
+  uint32_t* d_kimtab = nullptr;  // Kimura2 / JukesCantor: A-flag | B-flag << 16 per letter pair
   uint32_t* d_scratch = nullptr;
   size_t scratch_bytes = 0;
   void* d_carry = nullptr;
@@ -1146,7 +1371,7 @@ struct Base {
     box_cap = spill_cap = 0;
   }
   ~Base() {
-    cudaFree(d_code); cudaFree(d_sorted); cudaFree(d_lettab); cudaFree(d_flagtab);
+    cudaFree(d_code); cudaFree(d_sorted); cudaFree(d_lettab); cudaFree(d_flagtab); cudaFree(d_kimtab);
     cudaFree(d_scratch); cudaFree(d_carry);
     free_box();
     cudaFree(d_counts); cudaFree(d_rowbuf); cudaFree(d_fbq);
@@ -1205,18 +1430,21 @@ int build_base(Base& B, const EngineParams& P, std::string* msg) {
   }
   B.max_s = maxS;
   std::vector<int32_t> lettab((size_t)A1 * A1);
-  std::vector<uint32_t> flagtab((size_t)A1 * A1, 0u);
+  std::vector<uint32_t> flagtab((size_t)A1 * A1, 0u), kimtab((size_t)A1 * A1, 0u);
   for (int a = 0; a < A1; a++)
     for (int c = 0; c < A1; c++) {
       int s;
-      uint32_t f = 0;
+      uint32_t f = 0, fk = 0;
       if (a == A || c == A) s = nw ? 0 : -B.bias;  // padding: NW keeps its values bounded
       else {
         s = P.h_scores[letters[a] * 128 + letters[c]];
-        f = P.h_flags[letters[a] * 128 + letters[c]] & kFlagCount;
+        const uint32_t fl = P.h_flags[letters[a] * 128 + letters[c]];
+        f = fl & kFlagCount;
+        fk = ((fl & kFlagCntA) ? 1u : 0u) | ((fl & kFlagCntB) ? 0x10000u : 0u);
       }
       lettab[(size_t)a * A1 + c] = s + P.o;
       flagtab[(size_t)a * A1 + c] = f;
+      kimtab[(size_t)a * A1 + c] = fk;
     }
   for (int x = 0; x < 128; x++) B.lut.v[x] = (uint8_t)(code_of[x] < 0 ? A : code_of[x]);
   std::vector<uint8_t> code((size_t)total + 64, (uint8_t)A);
@@ -1225,6 +1453,8 @@ int build_base(Base& B, const EngineParams& P, std::string* msg) {
   if ((rc = upload_vec(&B.d_sorted, B.sorted_h, msg, "order"))) return rc;
   if ((rc = upload_vec(&B.d_lettab, lettab, msg, "score table"))) return rc;
   if ((rc = upload_vec(&B.d_flagtab, flagtab, msg, "flag table"))) return rc;
+  if (P.dist_fn != 0 && !P.protein && (rc = upload_vec(&B.d_kimtab, kimtab, msg, "Kimura flag table")))
+    return rc;
   return SW_OK;
 }
 
@@ -1497,8 +1727,11 @@ class EngineImpl : public Engine {
     };
     const int dlo = key.block ? key.col_lo : 0, dhi = key.block ? key.col_hi : N - 1;
     const bool nw = P.mode == kModeNw;
-    const bool kim = P.dist_fn != 0 && !P.protein;  // Kimura2 / JukesCantor: 32-bit lanes
-    pl.plain_only = B.alpha > kMaxAlpha16 || (nw && !B.nw16) || kim || P.lanes == SW_LANES_32;
+    // Kimura2 / JukesCantor of SWG-MPI / SWG-MS on nucleic letters that fit three profile planes:
+    // the 16-bit kernels with two counter words; NW's and the MinMaxNormScore rule: 32-bit lanes
+    const bool kim = P.dist_fn != 0 && !P.protein;
+    const bool kim16 = kim && (P.dist_fn == 1 || P.dist_fn == 2) && !nw && planes_of(B.alpha) == 3;
+    pl.plain_only = B.alpha > kMaxAlpha16 || (nw && !B.nw16) || (kim && !kim16) || P.lanes == SW_LANES_32;
     // Two passes pay off only where the box step finishes nearly every pair: a pair it gives up
     // on costs the int32 full DP, about nine times a score-pass cell, so a few per cent of them
     // eat the gain.  The box step needs short local alignments and short gap chains (they decay by
@@ -1510,7 +1743,7 @@ class EngineImpl : public Engine {
     // rule, 2 uses two passes whenever min(o, e) >= 2, 0 never.
     const bool two_pass_ok = std::min(P.o, P.e) >= 2 &&
                              (opt_.two_pass == 2 || (opt_.two_pass == 1 && P.o >= 3 * B.max_s && P.e >= 3));
-    pl.kind = nw ? kKindNw : two_pass_ok ? kKindScore : kKindSw;
+    pl.kind = nw ? kKindNw : kim16 ? kKindKim : two_pass_ok ? kKindScore : kKindSw;
     std::vector<int2> big;
     if (pl.plain_only) {
       for (int q = key.row_lo; q <= key.row_hi; q++)
@@ -1550,7 +1783,7 @@ class EngineImpl : public Engine {
       const int m = B.len[q];
       if (opt_.m_hi > 0 && (m <= opt_.m_lo || m > opt_.m_hi)) continue;  // autotuner sample
       int K, passes;
-      choose_k(m, opt_.k_override, &K, &passes, nw, opt_.k_weights);
+      choose_k(m, opt_.k_override, &K, &passes, nw, opt_.k_weights, pl.kind == kKindKim ? kKimMaxK : 16);
       // a profile beyond shared memory (long queries, large alphabets): 32-bit lanes
       const bool fits = engine_smem(A, passes * 32 * K, B.maxcol, K, pl.kind) <= 227 * 1024;
       const int bi = (int)(std::find(std::begin(kKs), std::end(kKs), K) - std::begin(kKs));
@@ -1625,7 +1858,8 @@ class EngineImpl : public Engine {
       const int occ = std::max(1, occupancy_k(bn.K, A, pl.kind, bn.smem));
       bn.grid = (int)std::min<long>((long)P.sms * occ, (long)bn.items.size());
       bn.scratch_off = scr_words;
-      if (bn.max_passes > 1) scr_words += (size_t)bn.grid * warps_of(bn.K, pl.kind) * B.maxcol * kScrWords;
+      if (bn.max_passes > 1)
+        scr_words += (size_t)bn.grid * warps_of(bn.K, pl.kind) * B.maxcol * (pl.kind == kKindKim ? kScrWordsKim : kScrWords);
       bn.rowbuf_off = row_words;
       if (pl.kind == kKindScore) row_words += (size_t)bn.grid * warps_of(bn.K, pl.kind) * bn.mpad;
     }
@@ -1732,9 +1966,10 @@ class EngineImpl : public Engine {
       EngineJob J;
       std::memset(&J, 0, sizeof(J));
       J.code = B.d_code; J.off = P.off; J.sorted = B.d_sorted;
-      J.lettab = B.d_lettab; J.flagtab = B.d_flagtab;
+      J.lettab = B.d_lettab; J.flagtab = pl.kind == kKindKim ? B.d_kimtab : B.d_flagtab;
       J.A = B.alpha; J.o = P.o; J.e = P.e; J.bias = B.bias; J.thresh = pl.thresh;
       J.mode = P.mode; J.ranks = P.ranks; J.nseq = P.nseq; J.protein = P.protein;
+      J.dist_fn = P.dist_fn; J.throws = P.throws;
       J.rb_a = P.nseq / P.ranks; J.rb_b = P.nseq % P.ranks;
       J.blk_mode = key.block; J.col_lo = key.col_lo; J.col_hi = key.col_hi;
       J.out = P.out; J.ld = P.ld; J.mirror = mirror;

@@ -440,6 +440,39 @@ def test_kimura_and_jukes_cantor_against_oracle(cs, oracle_mod, dist_fn, mode):
         np.testing.assert_array_equal(full, want)
 
 
+@pytest.mark.parametrize("dist_fn,mode", [(1, 0), (2, 1)])
+def test_kimura_and_jukes_cantor_16bit_lanes(cs, oracle_mod, dist_fn, mode):
+    """Kimura2 / JukesCantor run on the 16-bit kernel with two counter words per state (at most 8
+    rows per lane, so queries over 256 residues take several passes): every pair equals the 32-bit
+    lanes and the oracle, and the pairs ran on 16-bit lanes."""
+    from csharp_b200 import synth
+    rng = np.random.default_rng(700 + dist_fn)
+    lens = np.concatenate([rng.integers(200, 1400, 44), [0, 1, 255, 256, 257, 513]])
+    seqs = [s.tobytes() for s in synth.dna_family(len(lens), 4, lens, seed=701)]
+    sm = cs.ScoringMatrix.Load("EDNAFULL")
+    eng = cs.Engine(sm, 16, 4, mode=mode, distance_fn=dist_fn).upload(seqs)
+    full, pairs, _ = eng.all_pairs(1)
+    assert eng.query("kernel_error") == 0
+    assert eng.query("lane16_pairs") + eng.rerun_count() == pairs
+    assert eng.query("lane16_pairs") >= pairs - len(seqs)
+    wide = cs.Engine(sm, 16, 4, mode=mode, distance_fn=dist_fn, lanes=32).upload(seqs)
+    full32, pairs32, _ = wide.all_pairs(1)
+    assert pairs32 == pairs
+    np.testing.assert_array_equal(full, full32)
+    for k in (4, 6):  # forced rows per lane
+        eng.set_option("rows_per_lane", k)
+        got, _, _ = eng.all_pairs(1)
+        np.testing.assert_array_equal(got, full32)
+    concat, off = cs.pack_sequences(seqs)
+    N = len(seqs)
+    r0 = N - 16  # the oracle on the last rows (the edge lengths among them)
+    want, _ = oracle_mod.block(concat, off, r0, N - 1, 0, N - 1, False, mode,
+                               sm.Scores[:127, :127].astype(np.float32), 16.0, 4.0, 1, dist_fn)
+    for q in range(r0, N):
+        cols = [d for d in range(N) if mode == 1 or d < q]
+        np.testing.assert_array_equal(full[q, cols], want[q - r0, cols])
+
+
 def test_jukes_cantor_log_zero_is_reported(cs, oracle_mod):
     """A matrix whose mismatches score above zero aligns AAAA with CCCC: 1 - 4/3 < 0, where
     SWG-MPI's JukesCantor throws (SW_E_THROWS) and SWG-MS gives 10."""
