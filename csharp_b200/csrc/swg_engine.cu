@@ -63,7 +63,8 @@ __host__ __device__ constexpr int ctas_of(int K, int kind = 0) {
 }
 constexpr int kKimMaxK = 8;  // rows per lane of the Kimura2 / JukesCantor kernels
 constexpr int kMaxChunk = 1024;
-constexpr int kFbChunk = 64;  // third-pass partners per work item
+constexpr int kFbChunk = 64;     // third-pass partners per work item, at most
+constexpr int kFbChunkMin = 2;   // ... and at least (one warp's two lanes A / B)
 constexpr int kScrWords = 8;    // words of carried state per column in the pass scratch
 constexpr int kScrWordsKim = 12;  // Kimura2 / JukesCantor: V, G and two counter words per state and lane
 
@@ -95,8 +96,9 @@ struct EngineJob {
   int* throws;              // set by a SWG-MPI JukesCantor pair whose log argument is <= 0
   unsigned long long* stats; // [0] items taken, [1] pairs finished in 16-bit lanes, [2] tripped
   // third pass (fb_cnt != nullptr): the box step's give-ups bucketed by query, query k (k < fb_nq)
-  // holding fb_cnt[k] partners at sorted[fb_start[k] ..] in chunks of kFbChunk; item it is chunk
-  // it - fb_cstart[k] of the query k with fb_cstart[k] <= it < fb_cstart[k + 1], *fb_total items
+  // holding fb_cnt[k] partners at sorted[fb_start[k] ..] in chunks of fb_total[1] partners; item
+  // it is chunk it - fb_cstart[k] of the query k with fb_cstart[k] <= it < fb_cstart[k + 1],
+  // fb_total[0] items
   const int* fb_cnt;
   const int* fb_start;
   const int* fb_cstart;
@@ -836,8 +838,9 @@ __global__ void __launch_bounds__(warps_of(K, KIND) * 32, ctas_of(K, KIND)) engi
         else hi = mid;
       }
       q = J.fb_lo + lo;
-      c0 = J.fb_start[lo] + (it - J.fb_cstart[lo]) * kFbChunk;
-      c1 = min(J.fb_start[lo] + J.fb_cnt[lo], c0 + kFbChunk);
+      const int chunk = J.fb_total[1];
+      c0 = J.fb_start[lo] + (it - J.fb_cstart[lo]) * chunk;
+      c1 = min(J.fb_start[lo] + J.fb_cnt[lo], c0 + chunk);
       if (c1 == c0) {
         __syncthreads();  // every thread has read s_item
         continue;
@@ -1104,40 +1107,56 @@ __global__ void fb_count_kernel(const int2* fb, const int* n, long long cap, int
     atomicAdd(cnt + (fb[p].x - lo), 1);
 }
 
+// Inclusive scan of v over the 1024 threads of the CTA (buf: 1024 ints of shared memory); all =
+// the sum over the CTA.  buf is free again when it returns.
+__device__ __forceinline__ int cta_scan_1024(int* buf, int v, int& all) {
+  const int t = threadIdx.x;
+  buf[t] = v;
+  __syncthreads();
+  for (int d = 1; d < 1024; d <<= 1) {
+    const int x = t >= d ? buf[t - d] : 0;
+    __syncthreads();
+    buf[t] += x;
+    __syncthreads();
+  }
+  const int r = buf[t];
+  all = buf[1023];
+  __syncthreads();
+  return r;
+}
+
 // Exclusive prefix sums over the nq queries (one CTA of 1024 threads): start[] of the partner
-// counts and cstart[] of their kFbChunk-pair chunks (cstart[nq] = *total = all chunks); fill
-// reset to 0.
+// counts and cstart[] of their chunks (cstart[nq] = total[0] = all chunks); fill reset to 0.
+// The chunk size (total[1], even, kFbChunkMin..kFbChunk partners) spreads the give-ups over
+// about `target` work items (the launch's CTAs): a few hundred give-ups of long pairs -- a
+// serving wave's -- then run on many SMs at once instead of a few CTAs working through 64
+// partners each, which left the rest of the GPU idle for the whole launch.
 __global__ void __launch_bounds__(1024) fb_scan_kernel(const int* cnt, int* start, int* fill, int* cstart,
-                                                       int* total, int nq) {
-  __shared__ int part[1024], cpart[1024];
+                                                       int* total, int nq, int target) {
+  __shared__ int part[1024];
   const int t = threadIdx.x;
   const int per = (nq + 1023) / 1024, lo = min(nq, t * per), hi = min(nq, lo + per);
-  int sum = 0, csum = 0;
-  for (int k = lo; k < hi; k++) {
-    sum += cnt[k];
-    csum += (cnt[k] + kFbChunk - 1) / kFbChunk;
-  }
-  part[t] = sum;
-  cpart[t] = csum;
-  __syncthreads();
-  for (int d = 1; d < 1024; d <<= 1) {  // inclusive scans of the per-thread sums
-    const int v = t >= d ? part[t - d] : 0, cv = t >= d ? cpart[t - d] : 0;
-    __syncthreads();
-    part[t] += v;
-    cpart[t] += cv;
-    __syncthreads();
-  }
-  int run = part[t] - sum, crun = cpart[t] - csum;
+  int sum = 0;
+  for (int k = lo; k < hi; k++) sum += cnt[k];
+  int all, call;
+  const int incl = cta_scan_1024(part, sum, all);
+  const int want = (all + max(target, 1) - 1) / max(target, 1);
+  const int chunk = min(kFbChunk, max(kFbChunkMin, (want + 1) & ~1));
+  int csum = 0;
+  for (int k = lo; k < hi; k++) csum += (cnt[k] + chunk - 1) / chunk;
+  const int cincl = cta_scan_1024(part, csum, call);
+  int run = incl - sum, crun = cincl - csum;
   for (int k = lo; k < hi; k++) {
     start[k] = run;
     cstart[k] = crun;
     run += cnt[k];
-    crun += (cnt[k] + kFbChunk - 1) / kFbChunk;
+    crun += (cnt[k] + chunk - 1) / chunk;
     fill[k] = 0;
   }
-  if (t == 1023) {
-    cstart[nq] = cpart[1023];
-    *total = cpart[1023];
+  if (t == 0) {
+    cstart[nq] = call;
+    total[0] = call;
+    total[1] = chunk;
   }
 }
 
@@ -1362,7 +1381,7 @@ struct Base {
   // third pass: the give-ups (pair list, bucketed partners) and per-query counts / offsets / fill
   int2* d_fb = nullptr;
   int* d_fbsorted = nullptr;
-  int* d_fbq = nullptr;         // [4 * nseq + 2]: counts, offsets, fill, chunk offsets (+1), chunks
+  int* d_fbq = nullptr;         // [4 * nseq + 3]: counts, offsets, fill, chunk offsets (+1), chunks, chunk size
   void free_box() {
     cudaFree(d_box); cudaFree(d_boxwin); cudaFree(d_cls[0]); cudaFree(d_cls[1]); cudaFree(d_spill);
     cudaFree(d_fb); cudaFree(d_fbsorted);
@@ -1902,7 +1921,7 @@ class EngineImpl : public Engine {
       if (!B.d_counts && cudaMalloc(&B.d_counts, sizeof(int) * 8) != cudaSuccess) {
         cudaGetLastError(); B.d_counts = nullptr; *msg = "cudaMalloc two-pass counts"; return SW_E_OOM;
       }
-      if (!B.d_fbq && cudaMalloc(&B.d_fbq, sizeof(int) * (4 * (size_t)std::max(N, 1) + 2)) != cudaSuccess) {
+      if (!B.d_fbq && cudaMalloc(&B.d_fbq, sizeof(int) * (4 * (size_t)std::max(N, 1) + 3)) != cudaSuccess) {
         cudaGetLastError(); B.d_fbq = nullptr; *msg = "cudaMalloc third-pass counts"; return SW_E_OOM;
       }
       // the third pass (16 rows per lane, every query's profile in shared memory) where it fits;
@@ -2044,7 +2063,7 @@ class EngineImpl : public Engine {
         if ((e = cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)nq, P.stream)) != cudaSuccess) return e;
         const int g = std::max(1, P.sms * 4);
         fb_count_kernel<<<g, 256, 0, P.stream>>>(B.d_fb, B.d_counts + 6, B.box_cap, key.row_lo, cnt);
-        fb_scan_kernel<<<1, 1024, 0, P.stream>>>(cnt, start, fill, cstart, total, nq);
+        fb_scan_kernel<<<1, 1024, 0, P.stream>>>(cnt, start, fill, cstart, total, nq, pl.fb_grid);
         fb_scatter_kernel<<<g, 256, 0, P.stream>>>(B.d_fb, B.d_counts + 6, B.box_cap, key.row_lo, start, fill,
                                                    B.d_fbsorted);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -2419,7 +2438,7 @@ class QueryRunnerImpl : public QueryRunner {
         if ((e = cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)fb_nq, st)) != cudaSuccess) return cuda_err(e, msg);
         const int g4 = std::max(1, P_.sms * 4);
         fb_count_kernel<<<g4, 256, 0, st>>>(W.d_fb, W.d_counts + 6, (long long)W.box_cap, 0, cnt);
-        fb_scan_kernel<<<1, 1024, 0, st>>>(cnt, start, fill, cstart, total, fb_nq);
+        fb_scan_kernel<<<1, 1024, 0, st>>>(cnt, start, fill, cstart, total, fb_nq, fb_grid);
         fb_scatter_kernel<<<g4, 256, 0, st>>>(W.d_fb, W.d_counts + 6, (long long)W.box_cap, 0, start, fill,
                                               W.d_fbsorted);
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(e, msg);
@@ -2486,7 +2505,8 @@ class QueryRunnerImpl : public QueryRunner {
     uint32_t* d_rowbuf = nullptr;
     size_t rowbuf_bytes = 0;
     // third pass: the give-ups (box_cap entries), their partners bucketed by query slot, and per
-    // slot counts / offsets / fill (fbq_cap each), chunk offsets (fbq_cap + 1) and the chunk count
+    // slot counts / offsets / fill (fbq_cap each), chunk offsets (fbq_cap + 1), the chunk count
+    // and the chunk size
     int2* d_fb = nullptr;
     int* d_fbsorted = nullptr;
     int* d_fbq = nullptr;
@@ -2502,7 +2522,7 @@ class QueryRunnerImpl : public QueryRunner {
     cudaFree(W.d_fbq);
     W.d_fbq = nullptr;
     W.fbq_cap = 0;
-    if (cudaMalloc(&W.d_fbq, sizeof(int) * (4 * cap + 2)) != cudaSuccess) {
+    if (cudaMalloc(&W.d_fbq, sizeof(int) * (4 * cap + 3)) != cudaSuccess) {
       cudaGetLastError(); *msg = "cudaMalloc wave third-pass counts"; return SW_E_OOM;
     }
     W.fbq_cap = cap;
