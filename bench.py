@@ -272,8 +272,11 @@ def serving(cs, device, jobs, load):
     """Serving workload: a device-resident database of 100,000 DNA sequences (lognormal median
     500, sigma 0.6, clipped 50-2,000), a Poisson stream of `jobs` query batches (sizes log-uniform
     in 1-512, query lengths from the same distribution) aligned SW-Gotoh against the whole
-    database.  The arrival rate is set from a calibration job so that the offered load is `load`
-    of the GPU.  Latency of a job = its completion (results in host memory) minus its submission."""
+    database.  The arrival rate is set from the measured capacity (a burst of 8 jobs of 64 queries
+    submitted at once: their cells over first submission to last completion) so that the offered
+    load is `load` of the GPU; `gcups` is then the cells of the stream over its span, about `load`
+    times the capacity.  Latency of a job = its completion (results in host memory) minus its
+    submission."""
     from csharp_b200 import pack_sequences, synth
     db = synth.config5_db(SERVE["db"])
     concat, off = pack_sequences(db)
@@ -282,10 +285,12 @@ def serving(cs, device, jobs, load):
     pool = synth.dna_family(4000, 40, synth.lognormal_lengths(4000, 500, 0.6, 50, 2000, rng), SERVE["seed"])
     eng = with_options(cs.Engine(cs.ScoringMatrix.Load("EDNAFULL"), 16, 4, device=device))
     eng.upload(concat=concat, offsets=off)
-    # calibration (also builds the database state): 64 queries alone
-    cal = [pool[k].tobytes() for k in range(64)]
-    r = eng.wait(eng.submit(cal))
-    cal_rate = r["cells"] / max(r["done_s"] - r["admit_s"], 1e-9)
+    # warm-up (builds the database state), then the capacity: a burst of 8 jobs of 64 queries
+    # submitted at once, their cells over first submission to last completion
+    eng.wait(eng.submit([pool[k].tobytes() for k in range(16)]))
+    burst = [eng.submit([pool[k].tobytes() for k in rng.integers(0, len(pool), 64)]) for _ in range(8)]
+    rs = [eng.wait(t) for t in burst]
+    cal_rate = sum(x["cells"] for x in rs) / max(max(x["done_s"] for x in rs) - min(x["submit_s"] for x in rs), 1e-9)
     mean_q = (SERVE["qmax"] - SERVE["qmin"]) / np.log(SERVE["qmax"] / SERVE["qmin"])
     mean_cells = mean_q * float(np.mean([len(p) for p in pool])) * dblen
     lam = load * cal_rate / mean_cells           # batches per second
@@ -321,7 +326,7 @@ def serving(cs, device, jobs, load):
             "arrival_rate_per_s": round(lam, 3), "span_s": round(span, 1),
             "p50_ms": round(float(np.percentile(lat, 50)), 1), "p99_ms": round(float(np.percentile(lat, 99)), 1),
             "mean_ms": round(float(lat.mean()), 1), "gcups": round(cells / span / 1e9, 1),
-            "calibration_gcups": round(cal_rate / 1e9, 1), "max_admitted": st["max_active"], "waves": st["waves"],
+            "capacity_gcups": round(cal_rate / 1e9, 1), "max_admitted": st["max_active"], "waves": st["waves"],
             "all_ok": ok}
 
 
