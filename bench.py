@@ -18,9 +18,9 @@ Besides the headline value (inputs resident in HBM, one engine call per share), 
                    on the host cores, over a uniform sample of the job's pairs, with its parity
   plain_vs_batched one 8-rank share block by block: the plain one-thread-per-pair kernel against
                    the engine behind the same block handler, identical results required
-  configs          configurations 1, 2 and 4 on the engine, each checked against the oracle
-                   (cfg1 every pair, cfg2 and cfg4 uniform samples) by CPU workers that run while
-                   the GPU legs run
+  configs          configurations 1, 2 and 4, and configuration 1 with the Kimura2 distance, on
+                   the engine, each checked against the oracle (cfg1 every pair, the others
+                   uniform samples) by CPU workers that run while the GPU legs run
   serving          configuration 5: Poisson query batches against a 100,000-sequence database
   clocks           the SM clocks sampled while timing
 """
@@ -193,13 +193,13 @@ def _parity_task(args):
     """One chunk of a parity check: (set name, checker, pairs) -> the oracle's distances."""
     name, kind, rows, cols = args
     import oracle
-    concat, off, scores, o, e, atype = _PARITY_SETS[name]
+    concat, off, scores, o, e, atype, dist_fn = _PARITY_SETS[name]
     if kind == "count":    # the in-DP integer checker, one counter word (pinned by the tests)
         return oracle.indp_pairs(concat, off, rows, cols, scores.astype(np.int32), o, e, atype, threads=1, fast=True)
     if kind == "nw":       # the NW traceback restatement
         return oracle.nw_pairs(concat, off, rows, cols, scores.astype(np.float32), float(o), float(e),
                                protein=atype == 0, threads=1)
-    return oracle.ref_distances("BLOSUM62" if atype == 0 else "EDNAFULL", atype, 0, float(o), float(e),
+    return oracle.ref_distances("BLOSUM62" if atype == 0 else "EDNAFULL", atype, dist_fn, float(o), float(e),
                                 concat, off, rows, cols)  # the transliterated reference
 
 
@@ -343,17 +343,21 @@ def _timed(stream, fn):
 
 
 def config_sets(cs, only=None, n=None):
-    """Configurations 1, 2 and 4: (name, description, sequences, matrix, open, extend, mode, type).
+    """Configurations 1, 2 and 4, and configuration 1 with the Kimura2 distance: (name, description,
+    sequences, matrix, open, extend, mode, type, distance function).
     only: the names to keep; n: the first n sequences of each (a smaller case, for profiling)."""
     from csharp_b200 import synth
     bl = cs.ScoringMatrix.Load("BLOSUM62").Scores
+    c1 = synth.config1()
     sets = [
         ("cfg1", "plain SW-Gotoh: 1,000 DNA, 20 roots of 500 nt, lengths 200-600, EDNAFULL 16/4",
-         synth.config1(), "EDNAFULL", 16, 4, cs.SWG_MPI, cs.NUCLEIC),
+         c1, "EDNAFULL", 16, 4, cs.SWG_MPI, cs.NUCLEIC, cs.PERCENT_IDENTITY),
         ("cfg2", "NW global: 10,000 DNA, lengths uniform 300-500, 100 roots, EDNAFULL 16/4",
-         synth.config2(), "EDNAFULL", 16, 4, cs.NW, cs.NUCLEIC),
+         synth.config2(), "EDNAFULL", 16, 4, cs.NW, cs.NUCLEIC, cs.PERCENT_IDENTITY),
         ("cfg4", "protein SW-Gotoh: 20,000 sequences (20 amino acids, lengths 100-1000, 500 roots), BLOSUM62 10/1",
-         synth.config4(bl), "BLOSUM62", 10, 1, cs.SWG_MPI, cs.PROTEIN),
+         synth.config4(bl), "BLOSUM62", 10, 1, cs.SWG_MPI, cs.PROTEIN, cs.PERCENT_IDENTITY),
+        ("cfg1_kimura2", "SW-Gotoh with the Kimura2 distance: the 1,000 DNA of configuration 1, EDNAFULL 16/4",
+         c1, "EDNAFULL", 16, 4, cs.SWG_MPI, cs.NUCLEIC, cs.KIMURA2),
     ]
     if only:
         sets = [s for s in sets if s[0] in only]
@@ -378,10 +382,11 @@ def run_configs(cs, device, stream, flush, sets, picks, parity):
     and the oracle's verdict on its checked pairs."""
     import torch
     out, got = {}, {}
-    for name, desc, seqs, matrix, o, e, mode, atype in sets:
+    for name, desc, seqs, matrix, o, e, mode, atype, dist_fn in sets:
         concat, off = cs.pack_sequences(seqs)
         n = len(seqs)
-        eng = with_options(cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=mode, alignment_type=atype, device=device))
+        eng = with_options(cs.Engine(cs.ScoringMatrix.Load(matrix), o, e, mode=mode, alignment_type=atype,
+                                     distance_fn=dist_fn, device=device))
         eng.upload(concat=concat, offsets=off)
         eng.use_stream(stream.cuda_stream)
         full = torch.zeros((n, n), dtype=torch.int16, device="cuda")
@@ -423,8 +428,8 @@ def main():
     ap.add_argument("--rows-per-lane", type=int, default=0, help="engine rows per lane (0 = per query)")
     ap.add_argument("--no-autotune", action="store_true", help="built-in rows-per-lane costs instead of measured ones")
     ap.add_argument("--serving-only", action="store_true", help="only the serving workload (one JSON line)")
-    ap.add_argument("--configs-only", action="store_true", help="only configurations 1, 2 and 4 (one JSON line)")
-    ap.add_argument("--only", default="", help="with --configs-only: comma-separated names (cfg1,cfg2,cfg4)")
+    ap.add_argument("--configs-only", action="store_true", help="only configurations 1, 2, 4 and 1 with Kimura2 (one JSON line)")
+    ap.add_argument("--only", default="", help="with --configs-only: comma-separated names (cfg1,cfg2,cfg4,cfg1_kimura2)")
     ap.add_argument("--config-n", type=int, default=0, help="with --configs-only: first N sequences of each")
     ap.add_argument("--serve-jobs", type=int, default=SERVE["jobs"])
     ap.add_argument("--box-reg", type=int, default=-1, choices=[-1, 0, 1],
@@ -586,13 +591,16 @@ def main():
 def start_parity(cs, sets, picks, threads):
     """Queue the oracle checks of configurations 1, 2 and 4 on all but two host cores."""
     tables = {}
-    for name, _, seqs, matrix, o, e, mode, atype in sets:
+    for name, _, seqs, matrix, o, e, mode, atype, dist_fn in sets:
         concat, off = cs.pack_sequences(seqs)
-        tables[name] = (concat, off, cs.ScoringMatrix.Load(matrix).Scores[:127, :127].copy(), o, e, atype)
+        tables[name] = (concat, off, cs.ScoringMatrix.Load(matrix).Scores[:127, :127].copy(), o, e, atype, dist_fn)
     parity = Parity(tables, threads - 2)
-    for name, _, seqs, matrix, o, e, mode, atype in sets:
+    for name, _, seqs, matrix, o, e, mode, atype, dist_fn in sets:
         ii, jj = picks[name]
-        kind = "nw" if mode == cs.NW else ("ref" if (atype == cs.PROTEIN and reference_available()) else "count")
+        if dist_fn != cs.PERCENT_IDENTITY and not reference_available():
+            raise RuntimeError(f"{name}: its checker is the transliterated reference (oracle/_ref), not built")
+        kind = "nw" if mode == cs.NW else ("ref" if ((atype == cs.PROTEIN and reference_available()) or
+                                                     dist_fn != cs.PERCENT_IDENTITY) else "count")
         parity.submit(name, kind, ii, jj)
     return parity
 
