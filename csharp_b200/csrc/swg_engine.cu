@@ -534,9 +534,14 @@ __device__ __forceinline__ void score_two(const uint32_t* __restrict__ prof, int
       const uint32_t* phb = pl + xb * plane + (NP == 3 ? mpad : 0);
       auto cell = [&](const int r, const uint32_t pl_r, const uint32_t ph_r) {
         const uint32_t F = (NP == 3) ? VOD + pl_r + ph_r : mad_hi16(ph_r, VOD + pl_r);
-        const uint32_t G = __vmaxs2(VOU, GU - E2);
-        H[r] = __vmaxs2(VOL[r], H[r] - E2);
-        const uint32_t V = __vmaxs2(__vimax3_s16x2(F, G, H[r]), bias2);
+        // G and H floored at 0 (bias), so that V = max(F, G, H) needs no floor of its own (one
+        // max fewer per cell pair).  By induction a floored G' is max(G, 0) of the unfloored G:
+        // max(VO, max(G, 0) - e, 0) = max(VO, G - e, -e, 0) = max(G_next, 0), and likewise H'; so
+        // max(F, G', H') = max(F, G, H, 0) and every V -- hence every row's best and its first
+        // column -- is unchanged.  This pass keeps no pointers: G and H are not needed otherwise.
+        const uint32_t G = __vimax3_s16x2(VOU, GU - E2, bias2);
+        H[r] = __vimax3_s16x2(VOL[r], H[r] - E2, bias2);
+        const uint32_t V = __vimax3_s16x2(F, G, H[r]);
         bool hiB, loA;
         BEST[r] = vmax2(BEST[r], V, hiB, loA);  // kept unless V is strictly greater
         bcA[r] = loA ? bcA[r] : colv;
