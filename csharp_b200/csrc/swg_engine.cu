@@ -2167,7 +2167,11 @@ class QueryRunnerImpl : public QueryRunner {
     N_ = P.nseq;
     nw_ = P.mode == kModeNw;
     third_ = P.third_pass != 0;
-    lanes16_ = !(B_.alpha > kMaxAlpha16 || P.lanes == SW_LANES_32 || B_.alpha == 0 || (P.dist_fn != 0 && !P.protein));
+    // Kimura2 / JukesCantor of SWG-MPI / SWG-MS on letters that fit three profile planes: the
+    // 16-bit kernels with two counter words (the batch planner's rule); otherwise 32-bit lanes
+    const bool kim = P.dist_fn != 0 && !P.protein;
+    kim_ = kim && (P.dist_fn == 1 || P.dist_fn == 2) && !nw_ && B_.alpha > 0 && planes_of(B_.alpha) == 3;
+    lanes16_ = !(B_.alpha > kMaxAlpha16 || P.lanes == SW_LANES_32 || B_.alpha == 0 || (kim && !kim_));
     // database chunks in length order
     for (int c0 = 0; c0 < N_; c0 += kQueryChunk) {
       const int c1 = std::min(N_, c0 + kQueryChunk);
@@ -2221,7 +2225,8 @@ class QueryRunnerImpl : public QueryRunner {
         uint32_t f = 0;
         if (x != kPadCode && c != A) {
           v = P.h_scores[x * 128 + B_.letters[c]];
-          f = P.h_flags[x * 128 + B_.letters[c]] & kFlagCount;
+          const uint32_t fl = P.h_flags[x * 128 + B_.letters[c]];
+          f = kim_ ? ((fl & kFlagCntA) ? 1u : 0u) | ((fl & kFlagCntB) ? 0x10000u : 0u) : fl & kFlagCount;
         }
         qtab[(size_t)x * A1 + c] = v + P.o;
         qflag[(size_t)x * A1 + c] = f;
@@ -2230,7 +2235,7 @@ class QueryRunnerImpl : public QueryRunner {
     if ((rc = upload_vec(&d_qflag_, qflag, msg, "query flag table"))) return rc;
     // two passes where the engine uses them (the same rule): the score-only kernels, then the box
     // step with a table row per query residue byte
-    two_ = !nw_ && std::min(P.o, P.e) >= 2 &&
+    two_ = !nw_ && !kim_ && std::min(P.o, P.e) >= 2 &&
            (P.two_pass == 2 || (P.two_pass == 1 && P.o >= 3 * max_s_ && P.e >= 3));
     if (two_) {
       std::vector<int32_t> qsc((size_t)128 * A1), qscf((size_t)128 * A1);
@@ -2248,6 +2253,9 @@ class QueryRunnerImpl : public QueryRunner {
     return SW_OK;
   }
 
+  // The 16-bit kernel kind of this runner's waves.
+  int kind() const { return nw_ ? kKindNw : kim_ ? kKindKim : two_ ? kKindScore : kKindSw; }
+
   int db_count() const override { return N_; }
 
   int64_t query_cells(int m) const override { return (int64_t)m * total_len_; }
@@ -2256,10 +2264,9 @@ class QueryRunnerImpl : public QueryRunner {
     int K = 0, passes = 0;
     bool fits = lanes16_ && (!nw_ || m <= nw_qmax_);
     if (fits) {
-      choose_k(m, 0, &K, &passes);
+      choose_k(m, 0, &K, &passes, false, nullptr, kim_ ? kKimMaxK : 16);
       // a profile beyond shared memory (queries of several thousand residues): 32-bit lanes
-      fits = engine_smem(B_.alpha, passes * 32 * K, B_.maxcol, K, nw_ ? kKindNw : two_ ? kKindScore : kKindSw) <=
-             227 * 1024;
+      fits = engine_smem(B_.alpha, passes * 32 * K, B_.maxcol, K, kind()) <= 227 * 1024;
     }
     for (size_t c = 0; c < chunk_lo_.size(); c++) {
       QueryItem it;
@@ -2323,7 +2330,7 @@ class QueryRunnerImpl : public QueryRunner {
     // per-bin launch shape and scratch (bins run concurrently, each multi-pass bin has its own;
     // two passes: each bin its own rows' bounds too)
     const int A = B_.alpha;
-    const int kind = nw_ ? kKindNw : two_ ? kKindScore : kKindSw;
+    const int kind = this->kind();
     std::vector<size_t> smem(ls.size()), scr_off(ls.size()), row_off(ls.size());
     std::vector<int> grid(ls.size());
     size_t scr_words = 0, row_words = 0;
@@ -2334,7 +2341,8 @@ class QueryRunnerImpl : public QueryRunner {
       const int occ = std::max(1, occupancy_k(ls[x].K, A, kind, smem[x]));
       grid[x] = std::min(P_.sms * occ, ls[x].count);
       scr_off[x] = scr_words;
-      if (ls[x].max_passes > 1) scr_words += (size_t)grid[x] * warps_of(ls[x].K, kind) * B_.maxcol * kScrWords;
+      if (ls[x].max_passes > 1)
+        scr_words += (size_t)grid[x] * warps_of(ls[x].K, kind) * B_.maxcol * (kim_ ? kScrWordsKim : kScrWords);
       row_off[x] = row_words;
       if (two_) row_words += (size_t)grid[x] * warps_of(ls[x].K, kind) * ls[x].mpad;
     }
@@ -2379,6 +2387,7 @@ class QueryRunnerImpl : public QueryRunner {
       J.code = B_.d_code; J.off = P_.off; J.sorted = B_.d_sorted;
       J.A = A; J.o = P_.o; J.e = P_.e; J.bias = bias_; J.thresh = thresh_;
       J.mode = P_.mode; J.ranks = 1; J.nseq = N_; J.protein = P_.protein;
+      J.dist_fn = P_.dist_fn; J.throws = P_.throws;
       J.maxcol = B_.maxcol;
       J.rerun = W.d_rerun; J.rerun_count = W.d_rerun_count; J.rerun_cap = (int)rerun_cap;
       J.stats = W.d_stats;
@@ -2616,6 +2625,7 @@ class QueryRunnerImpl : public QueryRunner {
   uint32_t* d_qflag_ = nullptr;
   bool two_ = false;          // SW-Gotoh with gap costs that suit the box step: two passes
   bool nw_ = false;           // global alignment (the NW kernels)
+  bool kim_ = false;          // Kimura2 / JukesCantor on 16-bit lanes (two counter words)
   bool third_ = true;         // two passes: the box step's give-ups on 16-bit lanes (third pass)
   int nw_qmax_ = 0;           // NW: longest query the 16-bit lanes' bias covers
   int32_t* d_qbsc_ = nullptr;   // [128 * (A+1)] box step tables (query residue byte x database code)

@@ -63,6 +63,23 @@ def test_query_batch_matches_oracle(cs, oracle_mod, opts):
     assert r["submit_s"] <= r["admit_s"] <= r["done_s"]
 
 
+@pytest.mark.parametrize("dist_fn,mode", [(1, 0), (2, 1), (1, 1)])
+def test_kimura_and_jukes_cantor_query_batch_matches_oracle(cs, oracle_mod, dist_fn, mode):
+    """Kimura2 / JukesCantor serving (16-bit lanes with two counter words per state, queries over
+    256 residues in several passes) against the oracle's block restatement, query = s1."""
+    db = _dna(240, 21, 1, 900)
+    queries = _dna(7, 22, 30, 800) + [b"", b"C", _dna(1, 23, 1300, 1300)[0]]
+    sm = cs.ScoringMatrix.Load("EDNAFULL")
+    eng = cs.Engine(sm, 16, 4, mode=mode, distance_fn=dist_fn).upload(db)
+    r = eng.wait(eng.submit(queries))
+    assert r["status"] == 0 and r["pairs"] == len(queries) * len(db)
+    concat, off = cs.pack_sequences(list(queries) + list(db))
+    nq, nd = len(queries), len(db)
+    want, _ = oracle_mod.block(concat, off, 0, nq - 1, nq, nq + nd - 1, False, mode,
+                               sm.Scores[:127, :127].astype(np.float32), 16.0, 4.0, 1, dist_fn)
+    np.testing.assert_array_equal(r["out"], want)
+
+
 def test_results_are_the_same_alone_and_in_the_mix(cs):
     db = _dna(400, 21, 20, 900)
     jobs = [_dna(k, 30 + k, 40, 1200) for k in (40, 1, 7, 3, 2, 12)]
