@@ -1596,8 +1596,10 @@ class EngineImpl : public Engine {
     Base& B = *base_;
     const bool nw = P0.mode == kModeNw;
     const bool kim = P0.dist_fn != 0 && !P0.protein;
+    // 32-bit lanes only: nothing to choose; Kimura2 / JukesCantor (at most 8 rows per lane, two
+    // counter words) keep the built-in costs
     if (B.alpha > kMaxAlpha16 || (nw && !B.nw16) || kim || P0.lanes == SW_LANES_32 || P0.nseq < 2)
-      return SW_OK;  // 32-bit lanes only: nothing to choose
+      return SW_OK;
     if ((rc = ensure_streams(msg))) return rc;
     // sample: the last R queries of the set (each aligned against every earlier sequence); each
     // K is timed on the sampled queries it serves in one pass with under 64 rows of padding
