@@ -576,9 +576,15 @@ def main():
                               "unit": "Gcell/s", "frac": round(achieved / peak_cells, 4), "traffic": traffic,
                               "peak_basis": f"measured max.s32 {peak_max / 1e12:.2f} Tops/s x {LANES_PER_OP} lanes / {OPS_PER_CELL} ops per cell",
                               "kernel_ms": round(kernel_ms, 2)}
-    if not a.skip_extras and rank == 0:
-        covered = {share_of(k) for k in range(a.warmup + a.steps)}
-        extras(a, cs, eng, stream, flush, out, concat, off, lens, N, bal, threads, result, covered)
+    if not a.skip_extras:
+        # every rank: the job end to end through the block handler; one GPU only: the CPU
+        # reference, the plain-kernel comparison, the configurations and serving
+        e2e = e2e_leg(cs, eng, concat, off, lens, N, rank, world)
+        if rank == 0:
+            result["e2e"] = e2e
+        if world == 1:
+            covered = {share_of(k) for k in range(a.warmup + a.steps)}
+            extras(a, cs, eng, stream, flush, out, concat, off, lens, N, bal, threads, result, covered)
     if rank == 0:
         print(json.dumps(result))
     if world > 1:
@@ -603,6 +609,58 @@ def start_parity(cs, sets, picks, threads):
                                                      dist_fn != cs.PERCENT_IDENTITY) else "count")
         parity.submit(name, kind, ii, jj)
     return parity
+
+
+def e2e_leg(cs, eng, concat, off, lens, N, rank, world):
+    """The reference-facing C ABI with host buffers, over the whole job split among the ranks (rank
+    r takes the 8-rank shares r, r + world, ...).  Per share: sw_upload_sequences of the set from
+    pinned host memory (same lengths and letters: the engine keeps its plans), then one
+    sw_compute_block call per block of the share, in the reference driver's order, each copying its
+    block into the share's row slab in pinned host memory.  Host wall clock per rank; the job's
+    time is the slowest rank's."""
+    import torch
+    mine = [s for s in range(SHARES) if s % world == rank]
+    pin_seq = torch.from_numpy(concat).pin_memory().numpy()
+    rows = max(b - a_ + 1 for a_, b in ranges(N, SHARES))
+    slab = torch.empty((rows, N), dtype=torch.int16).pin_memory().numpy()
+
+    def share_calls(s):
+        r0 = ranges(N, SHARES)[s][0]
+        for rs, re_, cs_, ce, diag in share_blocks(N, s):
+            eng.compute_block(rs, re_, cs_, ce, diag, out=slab[rs - r0:re_ - r0 + 1, cs_:ce + 1])
+
+    t = time.perf_counter()
+    eng.set_option("plan_only", 1)
+    for s in mine:
+        share_calls(s)
+    eng.set_option("plan_only", 0)
+    plan_s = time.perf_counter() - t
+    if mine:  # one untimed share
+        eng.upload(concat=pin_seq, offsets=off)
+        share_calls(mine[0])
+    cells, h2d, d2h = 0, 0, 0
+    t = time.perf_counter()
+    for s in mine:
+        eng.upload(concat=pin_seq, offsets=off)
+        share_calls(s)
+        cells += checkerboard_share_cells(lens, s)
+        h2d += concat.nbytes + off.nbytes
+        d2h += sum((re_ - rs + 1) * (ce - cs_ + 1) * 2 for rs, re_, cs_, ce, _ in share_blocks(N, s))
+    secs = time.perf_counter() - t
+    if world > 1:
+        import torch.distributed as dist
+        x = torch.tensor([secs, plan_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(x, op=dist.ReduceOp.MAX)
+        y = torch.tensor([cells, h2d, d2h], device="cuda", dtype=torch.float64)
+        dist.all_reduce(y, op=dist.ReduceOp.SUM)
+        secs, plan_s = float(x[0]), float(x[1])
+        cells, h2d, d2h = float(y[0]), float(y[1]), float(y[2])
+    return {"value": round(cells / secs / 1e9, 3), "unit": "GCUPS",
+            "h2d_bytes_per_step": int(h2d // SHARES), "d2h_bytes_per_step": int(d2h // SHARES),
+            "note": f"the whole job as {SHARES} 8-rank shares split over {world} GPU(s); per share: "
+                    "sw_upload_sequences from pinned host memory, then one sw_compute_block per block of the "
+                    "share (host output) in the reference driver's order; host wall clock, slowest rank",
+            "plan_s": round(plan_s, 2)}
 
 
 def extras(a, cs, eng, stream, flush, out, concat, off, lens, N, bal, threads, result, covered):
@@ -636,42 +694,6 @@ def extras(a, cs, eng, stream, flush, out, concat, off, lens, N, bal, threads, r
     got = out[torch.from_numpy(ii).cuda(), torch.from_numpy(jj).cuda()].cpu().numpy()
     result["parity"] = {"pairs_checked_vs_cpu_reference": npairs, "mismatches": int((got != d_cpu).sum()),
                         "tolerance": "exact Int16"}
-
-    # ---- e2e: the reference-facing C ABI with host buffers.  Per step: sw_upload_sequences of the
-    # set from pinned host memory (same lengths and letters: the engine keeps its plans), then one
-    # sw_compute_block call per block of the share, in the reference driver's order, each copying
-    # its block into the rank's row slab in pinned host memory
-    pin_seq = torch.from_numpy(concat).pin_memory().numpy()
-    rows = max(b - a_ + 1 for a_, b in ranges(N, SHARES))
-    slab = torch.empty((rows, N), dtype=torch.int16).pin_memory().numpy()
-    t = time.perf_counter()
-    eng.set_option("plan_only", 1)
-    for s in range(SHARES):
-        r0 = ranges(N, SHARES)[s][0]
-        for rs, re_, cs_, ce, diag in share_blocks(N, s):
-            eng.compute_block(rs, re_, cs_, ce, diag, out=slab[rs - r0:re_ - r0 + 1, cs_:ce + 1])
-    eng.set_option("plan_only", 0)
-    e2e_plan_s = time.perf_counter() - t
-    e_cells, e_s, h2d, d2h = 0, 0.0, 0, 0
-    for k in range(-1, SHARES):  # one untimed step, then the whole job
-        s = max(k, 0)
-        r0 = ranges(N, SHARES)[s][0]
-        t = time.perf_counter()
-        eng.upload(concat=pin_seq, offsets=off)
-        for rs, re_, cs_, ce, diag in share_blocks(N, s):
-            eng.compute_block(rs, re_, cs_, ce, diag, out=slab[rs - r0:re_ - r0 + 1, cs_:ce + 1])
-        dt = time.perf_counter() - t
-        if k >= 0:
-            e_s += dt
-            e_cells += checkerboard_share_cells(lens, s)
-            h2d += concat.nbytes + off.nbytes
-            d2h += sum((re_ - rs + 1) * (ce - cs_ + 1) * 2 for rs, re_, cs_, ce, _ in share_blocks(N, s))
-    result["e2e"] = {"value": round(e_cells / e_s / 1e9, 3), "unit": "GCUPS",
-                     "h2d_bytes_per_step": int(h2d // SHARES), "d2h_bytes_per_step": int(d2h // SHARES),
-                     "note": "per step (one 8-rank share): sw_upload_sequences from pinned host memory, then one "
-                             "sw_compute_block per block of the share (host output) in the reference driver's order; "
-                             "host wall clock; the 8 steps are the whole job",
-                     "plan_s": round(e2e_plan_s, 2)}
 
     # ---- the parity checks of configurations 1, 2 and 4 run on the host cores from here on
     sets = config_sets(cs)
