@@ -10,9 +10,10 @@ whole job once on one GPU.  With N GPUs (torchrun) each rank takes a different s
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 Besides the headline value (inputs resident in HBM, one engine call per share), the line carries:
-  e2e              the same shares through the reference-facing C ABI with host buffers: per step
-                   sw_upload_sequences from pinned memory, then one sw_compute_block call per block
-                   of the share in the reference driver's order, each copying its block to the host
+  e2e              the whole job through the reference-facing C ABI with host buffers, its 8 shares
+                   split among the ranks: per share sw_upload_sequences from pinned memory, then one
+                   sw_compute_block call per block in the reference driver's order, each copying its
+                   block to the host (every rank; the rest below at N = 1 only)
   roofline         the engine kernels' cell rate against the integer-pipe peak measured live
   cpu_baseline     the reference's own aligner and ComputeDistance (transliterated from its C#)
                    on the host cores, over a uniform sample of the job's pairs, with its parity
