@@ -612,6 +612,11 @@ def start_parity(cs, sets, picks, threads):
     return parity
 
 
+def e2e_shares(rank, world):
+    """The 8-rank shares the end-to-end leg of rank `rank` (of `world`) takes: r, r + world, ..."""
+    return [s for s in range(SHARES) if s % world == rank]
+
+
 def e2e_leg(cs, eng, concat, off, lens, N, rank, world):
     """The reference-facing C ABI with host buffers, over the whole job split among the ranks (rank
     r takes the 8-rank shares r, r + world, ...).  Per share: sw_upload_sequences of the set from
@@ -620,7 +625,7 @@ def e2e_leg(cs, eng, concat, off, lens, N, rank, world):
     block into the share's row slab in pinned host memory.  Host wall clock per rank; the job's
     time is the slowest rank's."""
     import torch
-    mine = [s for s in range(SHARES) if s % world == rank]
+    mine = e2e_shares(rank, world)
     pin_seq = torch.from_numpy(concat).pin_memory().numpy()
     rows = max(b - a_ + 1 for a_, b in ranges(N, SHARES))
     slab = torch.empty((rows, N), dtype=torch.int16).pin_memory().numpy()
