@@ -194,12 +194,16 @@ def _parity_task(args):
     """One chunk of a parity check: (set name, checker, pairs) -> the oracle's distances."""
     name, kind, rows, cols = args
     import oracle
-    concat, off, scores, o, e, atype, dist_fn = _PARITY_SETS[name]
+    concat, off, scores, o, e, atype, dist_fn, mode = _PARITY_SETS[name]
     if kind == "count":    # the in-DP integer checker, one counter word (pinned by the tests)
         return oracle.indp_pairs(concat, off, rows, cols, scores.astype(np.int32), o, e, atype, threads=1, fast=True)
     if kind == "nw":       # the NW traceback restatement
         return oracle.nw_pairs(concat, off, rows, cols, scores.astype(np.float32), float(o), float(e),
                                protein=atype == 0, threads=1)
+    if kind == "block":    # the oracle's block restatement, one pair at a time (any distance)
+        sc = scores.astype(np.float32)
+        return np.array([oracle.block(concat, off, int(i), int(i), int(j), int(j), False, mode, sc, float(o),
+                                      float(e), atype, dist_fn)[0][0, 0] for i, j in zip(rows, cols)], dtype=np.int16)
     return oracle.ref_distances("BLOSUM62" if atype == 0 else "EDNAFULL", atype, dist_fn, float(o), float(e),
                                 concat, off, rows, cols)  # the transliterated reference
 
@@ -411,7 +415,8 @@ def run_configs(cs, device, stream, flush, sets, picks, parity):
         out[name]["parity"] = {"pairs_checked": int(len(want)), "mismatches": int((got[name] != want).sum()),
                                "checker": {"count": "oracle in-DP integer restatement (every pair)",
                                            "nw": "oracle NW traceback restatement (uniform sample)",
-                                           "ref": "transliterated reference oracle/_ref (uniform sample)"}[kind],
+                                           "ref": "transliterated reference oracle/_ref (uniform sample)",
+                                           "block": "oracle block restatement (uniform sample)"}[kind],
                                "tolerance": "exact Int16"}
     return out
 
@@ -600,14 +605,17 @@ def start_parity(cs, sets, picks, threads):
     tables = {}
     for name, _, seqs, matrix, o, e, mode, atype, dist_fn in sets:
         concat, off = cs.pack_sequences(seqs)
-        tables[name] = (concat, off, cs.ScoringMatrix.Load(matrix).Scores[:127, :127].copy(), o, e, atype, dist_fn)
+        tables[name] = (concat, off, cs.ScoringMatrix.Load(matrix).Scores[:127, :127].copy(), o, e, atype, dist_fn,
+                        mode)
     parity = Parity(tables, threads - 2)
     for name, _, seqs, matrix, o, e, mode, atype, dist_fn in sets:
         ii, jj = picks[name]
-        if dist_fn != cs.PERCENT_IDENTITY and not reference_available():
-            raise RuntimeError(f"{name}: its checker is the transliterated reference (oracle/_ref), not built")
-        kind = "nw" if mode == cs.NW else ("ref" if ((atype == cs.PROTEIN and reference_available()) or
-                                                     dist_fn != cs.PERCENT_IDENTITY) else "count")
+        if mode == cs.NW:
+            kind = "nw"
+        elif dist_fn != cs.PERCENT_IDENTITY:
+            kind = "ref" if reference_available() else "block"
+        else:
+            kind = "ref" if (atype == cs.PROTEIN and reference_available()) else "count"
         parity.submit(name, kind, ii, jj)
     return parity
 
